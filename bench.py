@@ -1,0 +1,366 @@
+"""Benchmark of the fused thermal LBM time step on B200.
+
+Workload (default): the 3D differentially heated cubic cavity, D3Q19 MRT +
+D3Q7 thermal, 128^3 nodes on a tanh-stretched grid (factor 1.5) on every axis,
+Ra = 1e5, Pr = 0.71, Ma = 0.1, rest initial state (rho = 1, u = 0, T = 0),
+FP64 storage and arithmetic (the drop-in).  A bench "step" is `--inner` LBM
+iterations (one lbm_step call).  Inputs are synthetic: the reference ships no
+data and none is needed.
+
+value  MLUPS of the fused step kernel with the state resident in HBM, timed
+       with CUDA events on the library's stream (the state, 2 x 436 MB
+       ping-pong, is larger than the 126 MB L2, so no flush is needed);
+e2e    the same metric through the public C ABI with host buffers: every step
+       uploads the initial macroscopic fields from pinned host memory
+       (lbm_init_equilibrium), runs the iterations and reads the fields back
+       (lbm_get_macro);
+roofline  algorithmic bytes per lattice update (2*Q*b_pop + 2*b_aux: 432 B in
+       FP64 3D) x nodes / mean kernel duration, against the measured HBM copy
+       bandwidth;
+cpu_baseline  the CPU restatement of the reference (C, OpenMP) on this host's
+       cores, on a bounded sample of the same workload.
+
+`--impl reference` times the reference's CPU algorithm instead: the Fortran
+reference cannot be compiled here (no Fortran compiler, no MPI), so its C
+restatement runs on all host cores, one full-domain iteration per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (dim, nx, ny, nz, grid, stretch, Ra, Pr)
+    "cavity3d_128": (3, 128, 128, 128, "tanh", 1.5, 1e5, 0.71),
+    "cavity2d_2048": (2, 2048, 2048, 1, "tanh", 1.5, 1e6, 0.71),
+    "cavity2d_128": (2, 128, 128, 1, "tanh", 1.5, 1e4, 0.71),
+}
+BYTES_PER_VALUE = {"f64": 8, "f32": 4, "f16s": 2}
+AUX_BYTES = {"f64": 8, "f32": 4, "f16s": 4}
+
+
+def bytes_per_lup(dim: int, storage: str) -> int:
+    q = 14 if dim == 2 else 26
+    return 2 * q * BYTES_PER_VALUE[storage] + 2 * AUX_BYTES[storage]
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload: str, storage: str):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 3 and parts[0] == workload and parts[1] == storage:
+            try:
+                return float(parts[2])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str | None):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu is not None:
+            cmd += ["-i", self.gpu]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, p[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sample(wl, seconds: float = 12.0, max_steps: int = 200):
+    """Time the oracle (C restatement of the reference, OpenMP) on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    o = oracle.Oracle(dim, nx, ny, nz, grid=grid, stretch=stretch, Ra=Ra, Pr=Pr)
+    shape = o.shape
+    one, zero = np.ones(shape), np.zeros(shape)
+    o.set_macro(one, zero, zero, zero if dim == 3 else None, zero)
+    o.step(1)
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps:
+        o.step(1)
+        steps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    nn = nx * ny * nz
+    return {"value": nn * steps / dt / 1e6, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"{steps} full-domain iterations of {nx}x{ny}x{nz} (FP64, C restatement, "
+                      f"{oracle.get_threads()} OpenMP threads), {dt:.1f} s"}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    wl = WORKLOADS[args.workload]
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    o = oracle.Oracle(dim, nx, ny, nz, grid=grid, stretch=stretch, Ra=Ra, Pr=Pr)
+    shape = o.shape
+    one, zero = np.ones(shape), np.zeros(shape)
+    o.set_macro(one, zero, zero, zero if dim == 3 else None, zero)
+    for _ in range(args.warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(1)
+    dt = time.perf_counter() - t0
+    nn = nx * ny * nz
+    v = nn * args.steps / dt / 1e6
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": config_of(args, wl, inner=1),
+        "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
+                         "sample": f"{args.steps} full-domain iterations per run, one per step; the Fortran "
+                                   f"reference is not compilable here (no Fortran compiler / MPI), its C "
+                                   f"restatement runs instead"},
+        "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl, inner):
+    dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
+    return {"workload": args.workload, "lattice": "D2Q9+D2Q5" if dim == 2 else "D3Q19+D3Q7",
+            "nodes": [nx, ny, nz] if dim == 3 else [nx, ny], "grid": f"{grid} stretch {stretch}",
+            "Ra": Ra, "Pr": Pr, "Ma": 0.1, "storage": args.storage, "mode": args.mode,
+            "iterations_per_step": inner, "init": "rest (rho=1, u=0, T=0)",
+            "l2": "state larger than L2 (2 x ping-pong buffers), no flush",
+            "parallelism": f"{args.gpus} independent cavities, one per GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--inner", type=int, default=100, help="LBM iterations per bench step")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS))
+    ap.add_argument("--storage", default="f64", choices=["f64", "f32", "f16s"])
+    ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-clocks", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        # rank 0 alone times the CPU algorithm; other ranks exit without work
+        # and without a process group
+        run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_setup()
+
+    import torch
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    wl = WORKLOADS[args.workload]
+    dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
+    cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, storage=args.storage,
+                     mode=args.mode, device=local)
+    shape = cav.shape
+    # pinned host fields for the end-to-end leg
+    pin = {k: torch.zeros(shape, dtype=torch.float64, pin_memory=True) for k in ("rho", "u", "v", "w", "T")}
+    pin["rho"].fill_(1.0)
+    hostf = {k: t.numpy() for k, t in pin.items()}
+    cav.init_equilibrium(hostf["rho"], hostf["u"], hostf["v"], hostf["w"] if dim == 3 else None, hostf["T"])
+    stream = torch.cuda.ExternalStream(cav.stream_ptr(), device=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        cav.step(args.inner)
+    cav.synchronize()
+
+    clocks = None
+    sampler = None
+    if not args.no_clocks and rank == 0:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        gpu = vis.split(",")[local] if vis else str(local)
+        sampler = ClockSampler(gpu)
+        sampler.start()
+        time.sleep(0.3)
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = pkg.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        cav.step(args.inner)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = pkg.kernel_launches() - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    if sampler is not None:
+        clocks = sampler.stop()
+
+    nn = cav.nnode
+    iters = args.steps * args.inner
+    value = world * nn * iters / (ms / 1e3) / 1e6
+    bpl = bytes_per_lup(dim, args.storage)
+    peak, peak_kind = measured_peak()
+    ms_launch = ms / iters
+    achieved = bpl * nn / (ms_launch / 1e3) / 1e9
+    traffic = ncu_traffic(args.workload, args.storage)
+
+    # end-to-end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        h2d = 0
+        d2h = 0
+        pout = {k: torch.zeros(shape, dtype=torch.float64, pin_memory=True).numpy()
+                for k in ("rho", "u", "v", "w", "T")}
+        nfield = 5 if dim == 3 else 4
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            cav.init_equilibrium(hostf["rho"], hostf["u"], hostf["v"], hostf["w"] if dim == 3 else None,
+                                 hostf["T"])
+            cav.step(args.inner)
+            cav.get_macro_into(pout["rho"], pout["u"], pout["v"], pout["w"] if dim == 3 else None, pout["T"])
+        f1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1))
+        h2d = nfield * nn * 8
+        d2h = nfield * nn * 8
+        e2e = {"value": world * nn * iters / (ems / 1e3) / 1e6, "unit": "MLUPS", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "wall_s": wall,
+               "path": "lbm_init_equilibrium (pinned host fields) + lbm_step + lbm_get_macro (pinned)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(wl)
+
+    if rank == 0:
+        line = {
+            "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "f16s": "f16 storage / f32"}[args.storage],
+            "data": "synthetic", "config": config_of(args, wl, args.inner),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_lup": bpl, "kernel": "k_step3d" if dim == 3 else "k_step2d",
+                         "ms_per_launch": ms_launch, "frac_of_8TBps": achieved / 8000.0},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    cav.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

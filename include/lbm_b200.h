@@ -1,0 +1,180 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 thermal lattice-Boltzmann time step.
+ *
+ * This is the drop-in boundary for the time step of the reference Fortran
+ * solver (zzhao0930/MPI-Multi-Process-Version).  The reference has no API:
+ * its step is a chain of argument-less subroutines that share `module
+ * commondata` (natural-convection_2dim_mono.f90:1-72, 3dim_mono.f90:1-77) and
+ * are called from the `do while` loop of `program main`
+ * (2dim_mono.f90:307-330, 3dim_mono.f90:373-396).  Each entry point below
+ * replaces one or more of those subroutines; the comment on each names them.
+ * A Fortran caller binds these with `iso_c_binding`.
+ *
+ * Conventions
+ *   - every function returns an int status: LBM_OK (0) or a negative
+ *     LBM_ERR_* code; lbm_last_error() gives a one-line message;
+ *   - host arrays are in the reference's Fortran layout: scalar fields
+ *     a(nx, ny[, nz]) (x fastest), populations f(0:Q-1, nx, ny[, nz])
+ *     (population index fastest), coordinates x(0:n+1) in lattice units;
+ *   - all device work of a handle runs on the handle's own CUDA stream;
+ *     lbm_step is asynchronous, the getters and reductions synchronise;
+ *   - the library owns its device memory; the caller owns host arrays.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* status codes */
+#define LBM_OK               0
+#define LBM_ERR_PARAM       -1  /* a bad argument or parameter set */
+#define LBM_ERR_CUDA        -2  /* a CUDA runtime call failed */
+#define LBM_ERR_NONFINITE   -3  /* NaN or Inf found in a reduction */
+#define LBM_ERR_DIVERGED    -4  /* residual grew past the allowed bound */
+#define LBM_ERR_TIMEOUT     -5  /* a bounded device wait gave up */
+#define LBM_ERR_STATE       -6  /* call out of order (e.g. step before init) */
+#define LBM_ERR_NOMEM       -7  /* device allocation failed */
+#define LBM_ERR_UNSUPPORTED -8  /* option not built into this library */
+#define LBM_ERR_NODEVICE    -9  /* no CUDA device visible */
+
+/* population storage precision */
+#define LBM_STORE_F64   0  /* FP64 storage, FP64 arithmetic: the drop-in */
+#define LBM_STORE_F32   1  /* FP32 storage, FP32 arithmetic */
+#define LBM_STORE_F16S  2  /* FP16 storage of f - w*rho0 and g - w*T0, FP32 arithmetic */
+
+/* arithmetic mode (FP64 storage only) */
+#define LBM_MODE_FAST   0  /* multiply-add contraction, reciprocal constants */
+#define LBM_MODE_EXACT  1  /* the reference's operation order, no contraction:
+                              bit-identical to the CPU restatement */
+
+/* grid kinds for lbm_mesh */
+#define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */
+#define LBM_GRID_TANH    1  /* 0.5*(1 + tanh(b*(2*xi-1))/tanh(b)), b = stretch */
+#define LBM_GRID_UNIFORM 2
+
+typedef struct lbm_params {
+    int32_t dim;            /* 2 (D2Q9 + D2Q5) or 3 (D3Q19 + D3Q7) */
+    int32_t nx, ny, nz;     /* nodes per axis; nz ignored when dim == 2 */
+    double Ra, Pr, Ma;      /* Rayleigh, Prandtl, Mach: commondata 2M:9-11 */
+    double Thot, Tcold;     /* wall temperatures: 2M:12 */
+    double dt;              /* time step in lattice units from mesh(): 2M:111 */
+    double length_LB;       /* 1/dx(1) from mesh(): 2M:110 */
+    int32_t storage;        /* LBM_STORE_* */
+    int32_t mode;           /* LBM_MODE_* */
+    int32_t device;         /* CUDA device ordinal */
+    int32_t reserved;       /* must be 0 */
+} lbm_params;
+
+typedef struct lbm_handle lbm_handle;
+
+/* Version of this ABI (LBM_ABI_VERSION). */
+int lbm_abi_version(void);
+
+/* Short text for a status code, and the last error message of this thread. */
+const char *lbm_error_string(int status);
+const char *lbm_last_error(void);
+
+/* mesh(): the reference's grid construction, 2M:74-134 (3M:122-189).
+ * Fills x(0:nx+1), y(0:ny+1) and, for nz > 0, z(0:nz+1) in lattice units and
+ * returns dx0, length_LB and dt.  Host only; needs no GPU. */
+int lbm_mesh(int32_t kind, double stretch, int32_t nx, int32_t ny, int32_t nz,
+             double *x, double *y, double *z,
+             double *dx0, double *length_LB, double *dt);
+
+/* The parameter block of initial() (2M:151-162, 3M:206-229) for a parameter
+ * set: out[0..8] = viscosity_LB, kappa, gbeta, tauf, Snu, Sq, sig_k, dt,
+ * length_LB.  Host only. */
+int lbm_derived_params(const lbm_params *p, double *out9);
+
+/* Create a cavity on p->device: allocates device state, derives the
+ * parameters of initial() and the interpolation weights of interpolate()
+ * (2M:591-660) from the coordinates.  x, y, z are x(0:n+1) as mesh() leaves
+ * them; z may be NULL when dim == 2.  Replaces the allocations and the
+ * parameter block of initial() (2M:143-197). */
+int lbm_create(const lbm_params *p, const double *x, const double *y,
+               const double *z, lbm_handle **out);
+
+/* Free everything the handle owns (the deallocate block of main, 2M:347-375). */
+int lbm_destroy(lbm_handle *h);
+
+/* The reference's initial state (initial(), 2M:199-240 / 3M:256-301):
+ * rho = 1, u = v = w = 0, T the linear conduction profile between the
+ * isothermal walls, f and g at equilibrium; resets itc and the check state. */
+int lbm_init_reference(lbm_handle *h);
+
+/* Equilibrium initial state from host macroscopic fields a(nx,ny[,nz]) with
+ * the equilibrium formulas of initial() (2M:227-240, 3M:286-301).  w may be
+ * NULL (taken as 0).  Resets itc and the check state.  This is the entry
+ * point of warm starts. */
+int lbm_init_equilibrium(lbm_handle *h, const double *rho, const double *u,
+                         const double *v, const double *w, const double *T);
+
+/* Advance nsteps iterations of the reference loop body: collision_U,
+ * collision_T, update (a no-op on one domain), interpolate, bounceback_u,
+ * bounceback_T, macro_u, macro_t (2M:309-325, 3M:375-391).  Asynchronous. */
+int lbm_step(lbm_handle *h, int32_t nsteps);
+
+/* Iterations done since the last init (the reference's itc). */
+int lbm_itc(const lbm_handle *h, int64_t *itc);
+
+/* check(): 2M:755-805 (3M:1027-1082).  errU = |u - u_prev| / |u|,
+ * errT = |T - T_prev| / |T| in FP64 over all nodes; then u_prev = u,
+ * T_prev = T.  Returns LBM_ERR_NONFINITE if a sum is not finite. */
+int lbm_check(lbm_handle *h, double *errU, double *errT);
+
+/* Wall-averaged Nusselt numbers at the hot and cold isothermal walls, FP64.
+ * The reference has no such function (no counterpart to cite).
+ * Local Nu = -(L_LB-1)/(Thot-Tcold) dT/dn from the quadratic through the
+ * wall (dt/2 outside the first node) and the first two nodes; averaged with
+ * node cell widths. */
+int lbm_nusselt(lbm_handle *h, double *nu_hot, double *nu_cold);
+
+/* Mass sum(rho*dV) and energy sum(T*dV) in FP64 (no counterpart). */
+int lbm_sums(lbm_handle *h, double *mass, double *energy);
+
+/* Copy the macroscopic fields to host arrays a(nx,ny[,nz]); any pointer may
+ * be NULL; w is ignored in 2D.  Replaces gather_data (2M:807-816). */
+int lbm_get_macro(lbm_handle *h, double *rho, double *u, double *v,
+                  double *w, double *T);
+
+/* Overwrite the macroscopic fields (an exact restart is set_populations
+ * followed by set_macro with the saved fields).  NULL pointers keep the
+ * current field. */
+int lbm_set_macro(lbm_handle *h, const double *rho, const double *u,
+                  const double *v, const double *w, const double *T);
+
+/* Populations after the last completed iteration (post-streaming, post
+ * boundary, pre-collision: the reference's f and g arrays) in the Fortran
+ * layout f(0:Q-1,nx,ny[,nz]), g(0:QT-1,nx,ny[,nz]).  Either may be NULL. */
+int lbm_get_populations(lbm_handle *h, double *f, double *g);
+
+/* Load populations (same layout).  The macroscopic fields are recomputed
+ * from them (rho = sum f, T = sum g, u from the momentum with half the
+ * buoyancy force of the loaded state); call lbm_set_macro afterwards to
+ * restore the exact carried state of a checkpoint. */
+int lbm_set_populations(lbm_handle *h, const double *f, const double *g);
+
+/* Wait for all work of the handle. */
+int lbm_synchronize(lbm_handle *h);
+
+/* The handle's CUDA stream as an opaque pointer (cudaStream_t). */
+int lbm_stream(const lbm_handle *h, void **stream);
+
+/* Device bytes the handle holds. */
+int lbm_device_bytes(const lbm_handle *h, int64_t *bytes);
+
+/* Number of kernels this library launched since load (all handles). */
+int64_t lbm_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

@@ -1,0 +1,641 @@
+// C ABI of the B200 thermal LBM step (declared in include/lbm_b200.h).
+//
+// Host side of the drop-in boundary: parameter derivation and mesh as in the
+// reference's mesh() / initial() (natural-convection_2dim_mono.f90:74-281,
+// natural-convection_3dim_mono.f90:122-345), the interpolation weight tables
+// of interpolate() (2M:591-660), and the run state of the time loop
+// (2M:307-330).  Host arithmetic is compiled without multiply-add contraction
+// so the derived parameters and weights are the reference's to the bit.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_internal.h"
+
+using namespace lbm;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string t_last_error;
+
+static int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+static int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
+#define CU(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,   \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+extern "C" int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+
+extern "C" const char *lbm_error_string(int status)
+{
+    switch (status) {
+    case LBM_OK: return "ok";
+    case LBM_ERR_PARAM: return "bad parameter";
+    case LBM_ERR_CUDA: return "CUDA error";
+    case LBM_ERR_NONFINITE: return "non-finite value";
+    case LBM_ERR_DIVERGED: return "residual diverged";
+    case LBM_ERR_TIMEOUT: return "device wait timed out";
+    case LBM_ERR_STATE: return "call out of order";
+    case LBM_ERR_NOMEM: return "out of device memory";
+    case LBM_ERR_UNSUPPORTED: return "unsupported option";
+    case LBM_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char *lbm_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" int64_t lbm_kernel_launches(void) { return g_launches; }
+
+// ---------------------------------------------------------------------------
+// mesh() and initial() host arithmetic
+// ---------------------------------------------------------------------------
+static void grid_raw(int kind, int n, double stretch, double *xr)
+{
+    // 2M:86-88 (erf, constA = stretch); tanh and uniform variants
+    for (int i = 0; i <= n + 1; ++i) {
+        double xi = (double)i / (double)(n + 1);
+        if (kind == LBM_GRID_ERF)
+            xr[i] = 0.5 * (erf(stretch * ((double)i / (double)(n + 1) - 0.5)) / erf(0.5 * stretch) + 1.0);
+        else if (kind == LBM_GRID_TANH)
+            xr[i] = 0.5 * (tanh(stretch * (2.0 * xi - 1.0)) / tanh(stretch) + 1.0);
+        else
+            xr[i] = xi;
+    }
+}
+
+extern "C" int lbm_mesh(int32_t kind, double stretch, int32_t nx, int32_t ny, int32_t nz, double *x, double *y,
+                        double *z, double *dx0_out, double *length_LB_out, double *dt_out)
+{
+    if (kind < 0 || kind > 2) return fail(LBM_ERR_PARAM, "lbm_mesh: unknown grid kind %d", kind);
+    if (nx < 3 || ny < 3 || (z && nz < 3)) return fail(LBM_ERR_PARAM, "lbm_mesh: need >= 3 nodes per axis");
+    if (!x || !y) return fail(LBM_ERR_PARAM, "lbm_mesh: x and y are required");
+    if (kind != LBM_GRID_UNIFORM && !(stretch > 0.0))
+        return fail(LBM_ERR_PARAM, "lbm_mesh: stretch must be > 0");
+    grid_raw(kind, nx, stretch, x);
+    grid_raw(kind, ny, stretch, y);
+    if (z) grid_raw(kind, nz, stretch, z);
+    // 2M:94-116: spacing of the first x cell sets the lattice unit
+    const double dx1 = x[1] - x[0];
+    const double dx0 = dx1, dt0 = dx0;
+    const double length_LB = 1.0 / dx1;
+    const double dt = dt0 * length_LB;
+    for (int i = 1; i <= nx; ++i) x[i] = x[i] - dx0 / 2.0;
+    for (int j = 1; j <= ny; ++j) y[j] = y[j] - dx0 / 2.0;
+    if (z) for (int k = 1; k <= nz; ++k) z[k] = z[k] - dx0 / 2.0;
+    for (int i = 0; i <= nx + 1; ++i) x[i] = x[i] * length_LB;
+    for (int j = 0; j <= ny + 1; ++j) y[j] = y[j] * length_LB;
+    if (z) for (int k = 0; k <= nz + 1; ++k) z[k] = z[k] * length_LB;
+    if (dx0_out) *dx0_out = dx0;
+    if (length_LB_out) *length_LB_out = length_LB;
+    if (dt_out) *dt_out = dt;
+    return LBM_OK;
+}
+
+struct Derived {
+    double viscosity_LB, kappa, gbeta, tauf, Snu, Sq, sig_k;
+};
+
+static Derived derive(const lbm_params &p)
+{
+    // 2M:152-162 and 3M:207-229
+    Derived d;
+    d.viscosity_LB = (p.Ma * (p.length_LB - 1.0) * sqrt(p.Pr)) / sqrt(3.0 * p.Ra);
+    d.kappa = d.viscosity_LB / p.Pr;
+    const double L1 = p.length_LB - 1.0;
+    d.gbeta = p.Ra * d.viscosity_LB * d.kappa / ((L1 * L1) * L1);
+    d.tauf = d.viscosity_LB * 3.0 + 0.5;
+    d.Snu = 1.0 / d.tauf;
+    d.Sq = 8.0 * (2.0 - d.Snu) / (8.0 - d.Snu);
+    if (p.dim == 2)
+        d.sig_k = 1.0 / (0.5 + 4.0 * (1.0 / d.Snu - 0.5) / (3.0 * p.Pr));
+    else
+        d.sig_k = 1.0 / (0.5 + (1.0 / d.Snu - 0.5) / (0.5 * p.Pr));
+    return d;
+}
+
+static int validate(const lbm_params *p)
+{
+    if (!p) return fail(LBM_ERR_PARAM, "params is NULL");
+    if (p->dim != 2 && p->dim != 3) return fail(LBM_ERR_PARAM, "dim must be 2 or 3 (got %d)", p->dim);
+    if (p->nx < 3 || p->ny < 3 || (p->dim == 3 && p->nz < 3))
+        return fail(LBM_ERR_PARAM, "need >= 3 nodes per axis (got %d x %d x %d)", p->nx, p->ny, p->nz);
+    const double lim = 1 << 24;
+    if (p->nx > lim || p->ny > lim || (p->dim == 3 && p->nz > lim))
+        return fail(LBM_ERR_PARAM, "axis too long");
+    if (!(p->Ra > 0) || !(p->Pr > 0) || !(p->Ma > 0)) return fail(LBM_ERR_PARAM, "Ra, Pr, Ma must be > 0");
+    if (!(p->dt > 0) || !isfinite(p->dt)) return fail(LBM_ERR_PARAM, "dt must be finite and > 0");
+    if (!(p->length_LB > 1.0) || !isfinite(p->length_LB)) return fail(LBM_ERR_PARAM, "length_LB must be > 1");
+    if (!isfinite(p->Thot) || !isfinite(p->Tcold) || p->Thot == p->Tcold)
+        return fail(LBM_ERR_PARAM, "Thot and Tcold must be finite and differ");
+    if (p->storage < LBM_STORE_F64 || p->storage > LBM_STORE_F16S)
+        return fail(LBM_ERR_PARAM, "unknown storage %d", p->storage);
+    if (p->mode != LBM_MODE_FAST && p->mode != LBM_MODE_EXACT) return fail(LBM_ERR_PARAM, "unknown mode %d", p->mode);
+    if (p->mode == LBM_MODE_EXACT && p->storage != LBM_STORE_F64)
+        return fail(LBM_ERR_UNSUPPORTED, "exact mode needs FP64 storage");
+    if (p->reserved != 0) return fail(LBM_ERR_PARAM, "reserved field must be 0");
+    return LBM_OK;
+}
+
+extern "C" int lbm_derived_params(const lbm_params *p, double *out9)
+{
+    int st = validate(p);
+    if (st) return st;
+    if (!out9) return fail(LBM_ERR_PARAM, "out is NULL");
+    Derived d = derive(*p);
+    out9[0] = d.viscosity_LB; out9[1] = d.kappa; out9[2] = d.gbeta; out9[3] = d.tauf;
+    out9[4] = d.Snu; out9[5] = d.Sq; out9[6] = d.sig_k; out9[7] = p->dt; out9[8] = p->length_LB;
+    return LBM_OK;
+}
+
+// Interpolation weights of interpolateF (2M:649-660) for every node of one
+// axis and both shift signs, in the stencil order of inter_x (2B:246-296):
+// tab[(i-1)*6 + s*3 + c], s = 0 for a +dt shift, 1 for -dt.
+static void axis_weights(const double *c, int n, double dt, double *tab)
+{
+    for (int i = 1; i <= n; ++i) {
+        int a, m = i, b;
+        if (i == 1) { a = i + 1; b = i + 2; }
+        else if (i == n) { a = i - 1; b = i - 2; }
+        else { a = i - 1; b = i + 1; }
+        for (int s = 0; s < 2; ++s) {
+            const double delta = (s == 0 ? 1.0 : -1.0) * dt;
+            const double x0 = c[a] + delta, x1 = c[m] + delta, x2 = c[b] + delta, x = c[m];
+            double *w = tab + (int64_t)(i - 1) * 6 + s * 3;
+            w[0] = ((x - x1) * (x - x2)) / ((x0 - x1) * (x0 - x2));
+            w[1] = ((x - x0) * (x - x2)) / ((x1 - x0) * (x1 - x2));
+            w[2] = ((x - x0) * (x - x1)) / ((x2 - x0) * (x2 - x1));
+        }
+    }
+}
+
+// cell widths of nodes 1..n: the wall lies dt/2 outside the end nodes
+static void cell_widths(const double *c, int n, double dt, double *wd)
+{
+    const double lo = c[1] - 0.5 * dt, hi = c[n] + 0.5 * dt;
+    for (int i = 1; i <= n; ++i) {
+        const double a = (i == 1) ? lo : 0.5 * (c[i - 1] + c[i]);
+        const double b = (i == n) ? hi : 0.5 * (c[i] + c[i + 1]);
+        wd[i - 1] = b - a;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct lbm_handle {
+    lbm_params p;
+    Derived d;
+    int Q, QT;
+    int device;
+    size_t esize, csize;      // storage / compute element size
+    Geo geo;
+    Bufs bufs;
+    std::vector<double> coord[3];
+    double *d_wgt[3] = {nullptr, nullptr, nullptr};
+    double *d_coord[3] = {nullptr, nullptr, nullptr};
+    double *d_cellw[3] = {nullptr, nullptr, nullptr};
+    void *staging = nullptr;     // population planes for stream-only output
+    double *aos = nullptr;       // Fortran-layout staging
+    cudaStream_t stream = nullptr;
+    int cur = 0;                 // buffer holding the newest populations
+    int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
+    int64_t itc = 0;
+    int64_t bytes = 0;
+};
+
+static int set_device(const lbm_handle *h)
+{
+    CU(cudaSetDevice(h->device));
+    return LBM_OK;
+}
+
+template <class T>
+static int dalloc(lbm_handle *h, T **ptr, size_t bytes)
+{
+    cudaError_t e = cudaMalloc((void **)ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        return fail(e == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA, "cudaMalloc(%zu): %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    h->bytes += (int64_t)bytes;
+    return LBM_OK;
+}
+
+static void free_all(lbm_handle *h)
+{
+    void *ptrs[] = {h->bufs.pop[0], h->bufs.pop[1], h->bufs.F[0], h->bufs.F[1], h->bufs.rho, h->bufs.u,
+                    h->bufs.v, h->bufs.w, h->bufs.T, h->bufs.up, h->bufs.vp, h->bufs.wp, h->bufs.Tp,
+                    h->bufs.partials, h->bufs.scal, h->d_wgt[0], h->d_wgt[1], h->d_wgt[2], h->d_coord[0],
+                    h->d_coord[1], h->d_coord[2], h->d_cellw[0], h->d_cellw[1], h->d_cellw[2], h->staging,
+                    h->aos};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+extern "C" int lbm_destroy(lbm_handle *h)
+{
+    if (!h) return LBM_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return LBM_OK;
+}
+
+extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y, const double *z, lbm_handle **out)
+{
+    if (!out) return fail(LBM_ERR_PARAM, "out is NULL");
+    *out = nullptr;
+    int st = validate(p);
+    if (st) return st;
+    if (!x || !y || (p->dim == 3 && !z)) return fail(LBM_ERR_PARAM, "coordinates missing");
+    const int n[3] = {p->nx, p->ny, p->dim == 3 ? p->nz : 1};
+    const double *c[3] = {x, y, z};
+    for (int a = 0; a < p->dim; ++a) {
+        for (int i = 0; i <= n[a] + 1; ++i)
+            if (!isfinite(c[a][i])) return fail(LBM_ERR_PARAM, "axis %d: coordinate %d not finite", a, i);
+        for (int i = 1; i < n[a]; ++i)
+            if (!(c[a][i + 1] > c[a][i])) return fail(LBM_ERR_PARAM, "axis %d: nodes not increasing at %d", a, i);
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(LBM_ERR_NODEVICE, "no CUDA device");
+    if (p->device < 0 || p->device >= ndev) return fail(LBM_ERR_PARAM, "device %d out of range", p->device);
+
+    lbm_handle *h = new lbm_handle();
+    h->p = *p;
+    if (p->dim == 2) h->p.nz = 1;
+    h->d = derive(h->p);
+    h->device = p->device;
+    h->Q = p->dim == 2 ? 9 : 19;
+    h->QT = p->dim == 2 ? 5 : 7;
+    h->esize = p->storage == LBM_STORE_F64 ? 8 : (p->storage == LBM_STORE_F32 ? 4 : 2);
+    h->csize = p->storage == LBM_STORE_F64 ? 8 : 4;
+
+    auto bail = [&](int code) {
+        free_all(h);
+        delete h;
+        return code;
+    };
+    if ((st = set_device(h))) return bail(st);
+    {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(fail(LBM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
+    }
+
+    Geo &g = h->geo;
+    memset(&g, 0, sizeof g);
+    g.dim = p->dim;
+    g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
+    g.pitch = g.nx;
+    g.slab = g.pitch * g.ny;
+    const int64_t cells = g.slab * g.nz;
+    g.plane = (cells + 127) / 128 * 128;
+    g.nnode = (int64_t)g.nx * g.ny * g.nz;
+    g.Snu = h->d.Snu; g.Sq = h->d.Sq; g.sig_k = h->d.sig_k; g.gbeta = h->d.gbeta;
+    g.dt = p->dt; g.Thot = p->Thot; g.Tcold = p->Tcold; g.T0 = 0.5 * (p->Thot + p->Tcold);
+    g.length_LB = p->length_LB;
+
+    // coordinates, weights, cell widths
+    for (int a = 0; a < 3; ++a) {
+        const int na = n[a];
+        h->coord[a].assign(na + 2, 0.0);
+        if (a < p->dim) memcpy(h->coord[a].data(), c[a], sizeof(double) * (na + 2));
+        std::vector<double> wt((size_t)na * 6, 0.0), cw((size_t)na, 1.0);
+        if (a < p->dim) {
+            axis_weights(h->coord[a].data(), na, p->dt, wt.data());
+            cell_widths(h->coord[a].data(), na, p->dt, cw.data());
+        }
+        if ((st = dalloc(h, &h->d_wgt[a], wt.size() * 8))) return bail(st);
+        if ((st = dalloc(h, &h->d_coord[a], h->coord[a].size() * 8))) return bail(st);
+        if ((st = dalloc(h, &h->d_cellw[a], cw.size() * 8))) return bail(st);
+        if (cudaMemcpy(h->d_wgt[a], wt.data(), wt.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_coord[a], h->coord[a].data(), h->coord[a].size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_cellw[a], cw.data(), cw.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(LBM_ERR_CUDA, "upload of axis tables failed"));
+        g.wgt[a] = h->d_wgt[a];
+        g.coord[a] = h->d_coord[a];
+        g.cellw[a] = h->d_cellw[a];
+    }
+
+    // state
+    Bufs &b = h->bufs;
+    memset(&b, 0, sizeof b);
+    const size_t popb = (size_t)(h->Q + h->QT) * (size_t)g.plane * h->esize;
+    const size_t fb = (size_t)g.plane * h->csize;
+    const size_t mb = (size_t)g.nnode * 8;
+    if ((st = dalloc(h, &b.pop[0], popb)) || (st = dalloc(h, &b.pop[1], popb)) ||
+        (st = dalloc(h, &b.F[0], fb)) || (st = dalloc(h, &b.F[1], fb)) || (st = dalloc(h, &b.rho, mb)) ||
+        (st = dalloc(h, &b.u, mb)) || (st = dalloc(h, &b.v, mb)) || (st = dalloc(h, &b.w, mb)) ||
+        (st = dalloc(h, &b.T, mb)) || (st = dalloc(h, &b.up, mb)) || (st = dalloc(h, &b.vp, mb)) ||
+        (st = dalloc(h, &b.wp, mb)) || (st = dalloc(h, &b.Tp, mb)) ||
+        (st = dalloc(h, &b.partials, 592 * 4 * 8)) || (st = dalloc(h, &b.scal, 16 * 8)))
+        return bail(st);
+    if (cudaMemset(b.F[0], 0, fb) != cudaSuccess || cudaMemset(b.F[1], 0, fb) != cudaSuccess ||
+        cudaMemset(b.w, 0, mb) != cudaSuccess || cudaMemset(b.wp, 0, mb) != cudaSuccess)
+        return bail(fail(LBM_ERR_CUDA, "memset failed"));
+    h->phase = 0;
+    *out = h;
+    return LBM_OK;
+}
+
+#define CHECK_H(h)                                                        \
+    do {                                                                  \
+        if (!(h)) return fail(LBM_ERR_PARAM, "handle is NULL");           \
+        int st_ = set_device(h);                                          \
+        if (st_) return st_;                                              \
+    } while (0)
+
+static cudaError_t launch_equilibrium(lbm_handle *h, void *pop)
+{
+    return h->p.mode == LBM_MODE_EXACT ? exact::equilibrium(h->geo, h->p.storage, pop, h->bufs, h->stream)
+                                       : fast::equilibrium(h->geo, h->p.storage, pop, h->bufs, h->stream);
+}
+
+static int reset_run(lbm_handle *h)
+{
+    const size_t mb = (size_t)h->geo.nnode * 8;
+    CU(cudaMemsetAsync(h->bufs.up, 0, mb, h->stream));
+    CU(cudaMemsetAsync(h->bufs.vp, 0, mb, h->stream));
+    CU(cudaMemsetAsync(h->bufs.wp, 0, mb, h->stream));
+    CU(cudaMemsetAsync(h->bufs.Tp, 0, mb, h->stream));
+    h->itc = 0;
+    return LBM_OK;
+}
+
+static int upload_macro(lbm_handle *h, const double *rho, const double *u, const double *v, const double *w,
+                        const double *T)
+{
+    const size_t mb = (size_t)h->geo.nnode * 8;
+    if (rho) CU(cudaMemcpyAsync(h->bufs.rho, rho, mb, cudaMemcpyHostToDevice, h->stream));
+    if (u) CU(cudaMemcpyAsync(h->bufs.u, u, mb, cudaMemcpyHostToDevice, h->stream));
+    if (v) CU(cudaMemcpyAsync(h->bufs.v, v, mb, cudaMemcpyHostToDevice, h->stream));
+    if (w && h->p.dim == 3) CU(cudaMemcpyAsync(h->bufs.w, w, mb, cudaMemcpyHostToDevice, h->stream));
+    if (T) CU(cudaMemcpyAsync(h->bufs.T, T, mb, cudaMemcpyHostToDevice, h->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_init_reference(lbm_handle *h)
+{
+    CHECK_H(h);
+    // initial(): rho = rho0, u = v = 0, T linear between the isothermal
+    // walls (2M:200-212 in x; 3M:257-271 in y)
+    const lbm_params &p = h->p;
+    const int64_t N = h->geo.nnode;
+    std::vector<double> rho((size_t)N, 1.0), zero((size_t)N, 0.0), T((size_t)N);
+    for (int k = 0; k < p.nz; ++k)
+        for (int j = 1; j <= p.ny; ++j)
+            for (int i = 1; i <= p.nx; ++i) {
+                const int64_t id = ((int64_t)k * p.ny + (j - 1)) * p.nx + (i - 1);
+                if (p.dim == 2)
+                    T[id] = (double)(i - 1) / (double)(p.nx - 1) * (p.Tcold - p.Thot) + p.Thot;
+                else
+                    T[id] = (double)(j - 1) / (double)(p.ny - 1) * (p.Tcold - p.Thot) + p.Thot;
+            }
+    int st = upload_macro(h, rho.data(), zero.data(), zero.data(), zero.data(), T.data());
+    if (st) return st;
+    CU(launch_equilibrium(h, h->bufs.pop[h->cur]));
+    if ((st = reset_run(h))) return st;
+    CU(cudaStreamSynchronize(h->stream));
+    h->phase = 1;
+    return LBM_OK;
+}
+
+extern "C" int lbm_init_equilibrium(lbm_handle *h, const double *rho, const double *u, const double *v,
+                                    const double *w, const double *T)
+{
+    CHECK_H(h);
+    if (!rho || !u || !v || !T) return fail(LBM_ERR_PARAM, "rho, u, v and T are required");
+    const int64_t N = h->geo.nnode;
+    std::vector<double> zero;
+    if (h->p.dim == 3 && !w) {
+        zero.assign((size_t)N, 0.0);
+        w = zero.data();
+    }
+    int st = upload_macro(h, rho, u, v, w, T);
+    if (st) return st;
+    CU(launch_equilibrium(h, h->bufs.pop[h->cur]));
+    if ((st = reset_run(h))) return st;
+    CU(cudaStreamSynchronize(h->stream));
+    h->phase = 1;
+    return LBM_OK;
+}
+
+extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
+{
+    CHECK_H(h);
+    if (nsteps < 0) return fail(LBM_ERR_PARAM, "nsteps < 0");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_step before an init call");
+    if (nsteps == 0) return LBM_OK;
+    const bool ex = h->p.mode == LBM_MODE_EXACT;
+    Bufs &b = h->bufs;
+    if (h->phase == 1) {
+        // first collision of the run, from the pre-collision state
+        const int nxt = 1 - h->cur;
+        CU(ex ? exact::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream)
+              : fast::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream));
+        h->cur = nxt;
+        h->phase = 2;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        const int nxt = 1 - h->cur;
+        const int wm = (s == nsteps - 1);
+        CU(ex ? exact::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm, h->stream)
+              : fast::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm, h->stream));
+        h->cur = nxt;
+    }
+    h->itc += nsteps;
+    return LBM_OK;
+}
+
+extern "C" int lbm_itc(const lbm_handle *h, int64_t *itc)
+{
+    if (!h || !itc) return fail(LBM_ERR_PARAM, "NULL argument");
+    *itc = h->itc;
+    return LBM_OK;
+}
+
+static int read_scal(lbm_handle *h, int first, int count, double *out)
+{
+    CU(cudaMemcpyAsync(out, h->bufs.scal + first, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_check(lbm_handle *h, double *errU, double *errT)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_check before an init call");
+    CU(reduce_check(h->geo, h->bufs, h->stream));
+    double s[4];
+    int st = read_scal(h, 0, 4, s);
+    if (st) return st;
+    // errorU = sqrt(error1_all)/sqrt(error2_all) (2M:784), errorT likewise (2M:798)
+    if (errU) *errU = sqrt(s[0]) / sqrt(s[1]);
+    if (errT) *errT = sqrt(s[2]) / sqrt(s[3]);
+    for (double v : s)
+        if (!isfinite(v)) return fail(LBM_ERR_NONFINITE, "check: non-finite residual sum");
+    return LBM_OK;
+}
+
+extern "C" int lbm_nusselt(lbm_handle *h, double *nu_hot, double *nu_cold)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_nusselt before an init call");
+    CU(reduce_nusselt(h->geo, h->bufs, h->stream));
+    double s[3];
+    int st = read_scal(h, 4, 3, s);
+    if (st) return st;
+    if (nu_hot) *nu_hot = s[0] / s[2];
+    if (nu_cold) *nu_cold = s[1] / s[2];
+    if (!isfinite(s[0]) || !isfinite(s[1])) return fail(LBM_ERR_NONFINITE, "nusselt: non-finite");
+    return LBM_OK;
+}
+
+extern "C" int lbm_sums(lbm_handle *h, double *mass, double *energy)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_sums before an init call");
+    CU(reduce_sums(h->geo, h->bufs, h->stream));
+    double s[2];
+    int st = read_scal(h, 7, 2, s);
+    if (st) return st;
+    if (mass) *mass = s[0];
+    if (energy) *energy = s[1];
+    if (!isfinite(s[0]) || !isfinite(s[1])) return fail(LBM_ERR_NONFINITE, "sums: non-finite");
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_macro(lbm_handle *h, double *rho, double *u, double *v, double *w, double *T)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_get_macro before an init call");
+    const size_t mb = (size_t)h->geo.nnode * 8;
+    if (rho) CU(cudaMemcpyAsync(rho, h->bufs.rho, mb, cudaMemcpyDeviceToHost, h->stream));
+    if (u) CU(cudaMemcpyAsync(u, h->bufs.u, mb, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CU(cudaMemcpyAsync(v, h->bufs.v, mb, cudaMemcpyDeviceToHost, h->stream));
+    if (w && h->p.dim == 3) CU(cudaMemcpyAsync(w, h->bufs.w, mb, cudaMemcpyDeviceToHost, h->stream));
+    if (T) CU(cudaMemcpyAsync(T, h->bufs.T, mb, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_macro(lbm_handle *h, const double *rho, const double *u, const double *v, const double *w,
+                             const double *T)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_set_macro before an init call");
+    if (h->phase == 2)
+        return fail(LBM_ERR_STATE, "lbm_set_macro after lbm_step: load populations first (lbm_set_populations)");
+    int st = upload_macro(h, rho, u, v, w, T);
+    if (st) return st;
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+static int ensure_staging(lbm_handle *h)
+{
+    if (!h->staging) {
+        int st = dalloc(h, &h->staging, (size_t)(h->Q + h->QT) * (size_t)h->geo.plane * h->esize);
+        if (st) return st;
+    }
+    if (!h->aos) {
+        int st = dalloc(h, &h->aos, (size_t)h->geo.nnode * h->Q * 8);
+        if (st) return st;
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_get_populations(lbm_handle *h, double *f, double *g)
+{
+    CHECK_H(h);
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_get_populations before an init call");
+    int st = ensure_staging(h);
+    if (st) return st;
+    const void *src = h->bufs.pop[h->cur];
+    if (h->phase == 2) {
+        // the newest buffer is one collision ahead; stream the previous one
+        const int prv = 1 - h->cur;
+        Bufs b = h->bufs;
+        CU(h->p.mode == LBM_MODE_EXACT
+               ? exact::stream_only(h->geo, h->p.storage, b.pop[prv], b.F[prv], h->staging, b, h->stream)
+               : fast::stream_only(h->geo, h->p.storage, b.pop[prv], b.F[prv], h->staging, b, h->stream));
+        src = h->staging;
+    }
+    const int64_t N = h->geo.nnode;
+    if (f) {
+        CU(planes_to_aos(h->geo, h->p.storage, 0, h->Q, src, h->aos, h->stream));
+        CU(cudaMemcpyAsync(f, h->aos, (size_t)N * h->Q * 8, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    if (g) {
+        CU(planes_to_aos(h->geo, h->p.storage, h->Q, h->QT, src, h->aos, h->stream));
+        CU(cudaMemcpyAsync(g, h->aos, (size_t)N * h->QT * 8, cudaMemcpyDeviceToHost, h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_set_populations(lbm_handle *h, const double *f, const double *g)
+{
+    CHECK_H(h);
+    if (!f || !g) return fail(LBM_ERR_PARAM, "f and g are required");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_set_populations before an init call");
+    int st = ensure_staging(h);
+    if (st) return st;
+    const int64_t N = h->geo.nnode;
+    void *dst = h->bufs.pop[h->cur];
+    CU(cudaMemcpyAsync(h->aos, f, (size_t)N * h->Q * 8, cudaMemcpyHostToDevice, h->stream));
+    CU(aos_to_planes(h->geo, h->p.storage, 0, h->Q, h->aos, dst, h->stream));
+    CU(cudaMemcpyAsync(h->aos, g, (size_t)N * h->QT * 8, cudaMemcpyHostToDevice, h->stream));
+    CU(aos_to_planes(h->geo, h->p.storage, h->Q, h->QT, h->aos, dst, h->stream));
+    CU(macro_from_pops(h->geo, h->p.storage, dst, h->bufs, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    h->phase = 1;
+    return LBM_OK;
+}
+
+extern "C" int lbm_synchronize(lbm_handle *h)
+{
+    CHECK_H(h);
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_stream(const lbm_handle *h, void **stream)
+{
+    if (!h || !stream) return fail(LBM_ERR_PARAM, "NULL argument");
+    *stream = (void *)h->stream;
+    return LBM_OK;
+}
+
+extern "C" int lbm_device_bytes(const lbm_handle *h, int64_t *bytes)
+{
+    if (!h || !bytes) return fail(LBM_ERR_PARAM, "NULL argument");
+    *bytes = h->bytes;
+    return LBM_OK;
+}

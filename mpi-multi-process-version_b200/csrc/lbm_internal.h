@@ -1,0 +1,69 @@
+// Internal interface between the C ABI (lbm_capi.cu) and the kernels
+// (lbm_kernels.cu, compiled once per arithmetic mode).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lbm {
+
+// Geometry and physics constants a kernel needs, passed by value.
+struct Geo {
+    int dim, nx, ny, nz;
+    int64_t pitch;   // elements between rows of a population plane
+    int64_t slab;    // elements between z-planes (pitch * ny)
+    int64_t plane;   // elements between population planes
+    int64_t nnode;   // nx*ny*nz: packed macro arrays, x fastest
+    double Snu, Sq, sig_k, gbeta, dt, Thot, Tcold, T0, length_LB;
+    const double *wgt[3];    // per axis: weights [n][2 signs][3], sign 0 = +1, 1 = -1
+    const double *coord[3];  // per axis: coordinates c(0:n+1)
+    const double *cellw[3];  // per axis: cell widths of nodes 1..n
+};
+
+// Device buffers of one cavity.
+struct Bufs {
+    void *pop[2];          // ping-pong population buffers, (Q+QT) planes each
+    void *F[2];            // carried buoyancy force, one value per node
+    double *rho, *u, *v, *w, *T;   // macroscopic fields, packed
+    double *up, *vp, *wp, *Tp;     // fields at the previous check
+    double *partials;      // reduction partials
+    double *scal;          // reduction results
+};
+
+enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
+
+// kernel launchers; one set per arithmetic mode
+#define LBM_DECLARE_LAUNCHERS(NS)                                                             \
+    namespace NS {                                                                            \
+    /* init: equilibrium populations from the macroscopic fields into pop */                  \
+    cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, cudaStream_t s); \
+    /* first collision of a run: pre-collision pop_in -> post-collision pop_out, F_out */     \
+    cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out,           \
+                        void *F_out, const Bufs &b, cudaStream_t s);                          \
+    /* fused step: stream + walls + macro + collide.  write_macro != 0 also stores rho,u,T */ \
+    cudaError_t step(const Geo &g, int store, const void *pop_in, const void *F_in,           \
+                     void *pop_out, void *F_out, const Bufs &b, int write_macro,              \
+                     cudaStream_t s);                                                         \
+    /* stream + walls + macro only: pre-collision populations into pop_out, macro fields */  \
+    cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in,    \
+                            void *pop_out, const Bufs &b, cudaStream_t s);                    \
+    }
+
+LBM_DECLARE_LAUNCHERS(fast)
+LBM_DECLARE_LAUNCHERS(exact)
+
+// mode-independent kernels (lbm_reduce.cu)
+cudaError_t reduce_check(const Geo &g, const Bufs &b, cudaStream_t s);      // scal[0..3]
+cudaError_t reduce_nusselt(const Geo &g, const Bufs &b, cudaStream_t s);    // scal[4..6]
+cudaError_t reduce_sums(const Geo &g, const Bufs &b, cudaStream_t s);       // scal[7..8]
+// AoS (Fortran f(0:Q-1,nodes)) <-> SoA planes, for FP64/FP32/FP16S storage
+cudaError_t aos_to_planes(const Geo &g, int store, int q0, int nq, const double *aos,
+                          void *pop, cudaStream_t s);
+cudaError_t planes_to_aos(const Geo &g, int store, int q0, int nq, const void *pop,
+                          double *aos, cudaStream_t s);
+// macro fields from populations (used by set_populations)
+cudaError_t macro_from_pops(const Geo &g, int store, const void *pop, const Bufs &b,
+                            cudaStream_t s);
+
+extern int64_t g_launches;  // kernels launched by this library
+
+}  // namespace lbm

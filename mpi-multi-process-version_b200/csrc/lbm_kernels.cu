@@ -1,0 +1,782 @@
+// Thermal LBM time-step kernels for sm_100a.
+//
+// This file is compiled twice:
+//   LBM_NS=fast                      multiply-add contraction on, constant
+//                                    divisions turned into reciprocal products;
+//   LBM_NS=exact, LBM_EXACT=1, --fmad=false
+//                                    every expression in the reference's operand
+//                                    order with its divisions, no contraction:
+//                                    FP64 results are bit-identical to the CPU
+//                                    restatement of the reference.
+//
+// One fused kernel per time step replaces the reference's chain of sweeps
+// collision_U -> collision_T -> update -> interpolate -> bounceback_u ->
+// bounceback_T -> macro_u -> macro_t (natural-convection_2dim_mono.f90:309-325,
+// natural-convection_3dim_mono.f90:375-391) with a pull formulation:
+//   read post-collision populations of the previous step around the node,
+//   interpolate (ISLBM streaming, 2M:591-660 / 3M:751-876),
+//   apply the wall rules of the node (2B:731-801 / 3B:1053-1197),
+//   form rho, u, T (2M:726-753 / 3M:988-1025) with the buoyancy force carried
+//   from the previous collision,
+//   collide (2M:431-569 / 3M:445-730) and write the new post-collision
+//   populations and force.
+// Populations live in structure-of-arrays planes: plane q holds population q of
+// every node, rows of `pitch` elements, z-planes of `slab` elements.  Planes
+// 0..Q-1 are f, Q..Q+QT-1 are g.
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+#include "lbm_internal.h"
+
+#ifndef LBM_EXACT
+#define LBM_EXACT 0
+#endif
+
+namespace lbm {
+namespace LBM_NS {
+
+// ---------------------------------------------------------------------------
+// storage traits
+// ---------------------------------------------------------------------------
+template <int ST> struct Tr;
+template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false; };
+template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = false; };
+template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true; };
+
+__device__ __forceinline__ double tocomp(double x) { return x; }
+__device__ __forceinline__ float tocomp(float x) { return x; }
+__device__ __forceinline__ float tocomp(__half x) { return __half2float(x); }
+
+template <class S> __device__ __forceinline__ S fromcomp(double x);
+template <> __device__ __forceinline__ double fromcomp<double>(double x) { return x; }
+template <class S> __device__ __forceinline__ S fromcompf(float x);
+template <> __device__ __forceinline__ float fromcompf<float>(float x) { return x; }
+template <> __device__ __forceinline__ __half fromcompf<__half>(float x) { return __float2half_rn(x); }
+
+template <class S, class C> __device__ __forceinline__ S tostore(C x);
+template <> __device__ __forceinline__ double tostore<double, double>(double x) { return x; }
+template <> __device__ __forceinline__ float tostore<float, float>(float x) { return x; }
+template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x); }
+
+// lattice weights used as storage shifts (f - w*rho0, g - w*T0), rho0 = 1
+__device__ __forceinline__ float wU2(int q) { return q == 0 ? 4.0f / 9.0f : (q < 5 ? 1.0f / 9.0f : 1.0f / 36.0f); }
+__device__ __forceinline__ float wT2(int q) { return q == 0 ? 0.5f : 0.125f; }
+__device__ __forceinline__ float wU3(int q) { return q == 0 ? 1.0f / 3.0f : (q < 7 ? 1.0f / 18.0f : 1.0f / 36.0f); }
+__device__ __forceinline__ float wT3(int q) { return q == 0 ? 0.5f : 1.0f / 12.0f; }
+
+// division by a literal: a true division in the exact build, a product with
+// the folded reciprocal in the fast build
+#if LBM_EXACT
+#define DV(a, c) ((a) / C(c))
+#else
+#define DV(a, c) ((a) * (C(1.0) / C(c)))
+#endif
+
+// three-point Lagrange interpolation with precomputed weights, in the operand
+// order of interpolateF (2M:655-657): (w0*f0 + w1*f1) + w2*f2
+template <class C>
+__device__ __forceinline__ C ip(const C w[3], C a, C m, C b) { return w[0] * a + w[1] * m + w[2] * b; }
+
+template <class C>
+__device__ __forceinline__ void load_w(const double *__restrict__ tab, int n, C wp[3], C wm[3])
+{
+    const double *t = tab + (int64_t)n * 6;
+    wp[0] = C(__ldg(t + 0)); wp[1] = C(__ldg(t + 1)); wp[2] = C(__ldg(t + 2));
+    wm[0] = C(__ldg(t + 3)); wm[1] = C(__ldg(t + 4)); wm[2] = C(__ldg(t + 5));
+}
+
+// stencil offsets (in nodes) of inter_x(i,1) and inter_x(i,3) relative to i:
+// (i+1, i+2) at the first node, (i-1, i-2) at the last, (i-1, i+1) inside
+// (2B:246-296)
+__device__ __forceinline__ int off_a(int i, int n) { (void)n; return i == 0 ? 1 : -1; }
+__device__ __forceinline__ int off_b(int i, int n) { return i == 0 ? 2 : (i == n - 1 ? -2 : 1); }
+
+// ---------------------------------------------------------------------------
+// 2D: D2Q9 MRT + D2Q5
+// ---------------------------------------------------------------------------
+
+// collision_U (2M:431-520) and collision_T (2M:522-569) at one node.
+template <class C>
+__device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C u, C v, C T,
+                                          const Geo &G, C fp[9], C gp[5], C &Fy)
+{
+    const C Snu = C(G.Snu), Sq = C(G.Sq), dt = C(G.dt), gbeta = C(G.gbeta), sig_k = C(G.sig_k);
+    C m[9], meq[9], mp[9];
+    m[0] = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+    m[1] = -C(4.0)*f[0]-f[1]-f[2]-f[3]-f[4]+C(2.0)*(f[5]+f[6]+f[7]+f[8]);
+    m[2] = C(4.0)*f[0]-C(2.0)*(f[1]+f[2]+f[3]+f[4])+f[5]+f[6]+f[7]+f[8];
+    m[3] = f[1]-f[3]+f[5]-f[6]-f[7]+f[8];
+    m[4] = -C(2.0)*f[1]+C(2.0)*f[3]+f[5]-f[6]-f[7]+f[8];
+    m[5] = f[2]-f[4]+f[5]+f[6]-f[7]-f[8];
+    m[6] = -C(2.0)*f[2]+C(2.0)*f[4]+f[5]+f[6]-f[7]-f[8];
+    m[7] = f[1]-f[2]+f[3]-f[4];
+    m[8] = f[5]-f[6]+f[7]-f[8];
+
+    meq[0] = rho;
+    meq[1] = rho*( -C(2.0)+C(3.0)*(u*u+v*v) );
+    meq[2] = rho*( C(1.0)-C(3.0)*(u*u+v*v) );
+    meq[3] = rho*u;
+    meq[4] = -rho*u;
+    meq[5] = rho*v;
+    meq[6] = -rho*v;
+    meq[7] = rho*(u*u-v*v);
+    meq[8] = rho*(u*v);
+
+    Fy = gbeta*T*rho;
+#if LBM_EXACT
+    // the reference's source terms with Fx = 0 kept (2M:475-486)
+    const C Fx = C(0.0);
+    const C s1 = Snu, s2 = Snu, s4 = Sq, s6 = Sq, s7 = Snu, s8 = Snu;
+    C src[9];
+    src[0] = C(0.0);
+    src[1] = (C(6.0)-C(3.0)*s1)*(u*Fx+v*Fy);
+    src[2] = -(C(6.0)-C(3.0)*s2)*(u*Fx+v*Fy);
+    src[3] = Fx;
+    src[4] = -(C(1.0)-C(0.5)*s4)*Fx;
+    src[5] = Fy;
+    src[6] = -(C(1.0)-C(0.5)*s6)*Fy;
+    src[7] = (C(2.0)-s7)*(u*Fx-v*Fy);
+    src[8] = (C(1.0)-C(0.5)*s8)*(v*Fx+u*Fy);
+    const C sv[9] = {C(0.0), Snu, Snu, C(0.0), Sq, C(0.0), Sq, Snu, Snu};
+#pragma unroll
+    for (int a = 0; a < 9; ++a) mp[a] = m[a]-sv[a]*(m[a]-meq[a])+src[a]*dt;
+#else
+    // Fx = 0: the Fx terms vanish
+    const C vF = v*Fy, uF = u*Fy;
+    mp[0] = m[0];
+    mp[1] = m[1]-Snu*(m[1]-meq[1])+(C(6.0)-C(3.0)*Snu)*vF*dt;
+    mp[2] = m[2]-Snu*(m[2]-meq[2])-(C(6.0)-C(3.0)*Snu)*vF*dt;
+    mp[3] = m[3];
+    mp[4] = m[4]-Sq*(m[4]-meq[4]);
+    mp[5] = m[5]+Fy*dt;
+    mp[6] = m[6]-Sq*(m[6]-meq[6])-(C(1.0)-C(0.5)*Sq)*Fy*dt;
+    mp[7] = m[7]-Snu*(m[7]-meq[7])-(C(2.0)-Snu)*vF*dt;
+    mp[8] = m[8]-Snu*(m[8]-meq[8])+(C(1.0)-C(0.5)*Snu)*uF*dt;
+#endif
+
+    fp[0] = DV( mp[0]-mp[1]+mp[2] , 9.0);
+    fp[1] = DV(mp[0],9.0)-DV(mp[1],36.0)-DV(mp[2],18.0)+DV(mp[3],6.0)-DV(mp[4],6.0)+mp[7]*C(0.25);
+    fp[2] = DV(mp[0],9.0)-DV(mp[1],36.0)-DV(mp[2],18.0)+DV(mp[5],6.0)-DV(mp[6],6.0)-mp[7]*C(0.25);
+    fp[3] = DV(mp[0],9.0)-DV(mp[1],36.0)-DV(mp[2],18.0)-DV(mp[3],6.0)+DV(mp[4],6.0)+mp[7]*C(0.25);
+    fp[4] = DV(mp[0],9.0)-DV(mp[1],36.0)-DV(mp[2],18.0)-DV(mp[5],6.0)+DV(mp[6],6.0)-mp[7]*C(0.25);
+    fp[5] = DV(mp[0],9.0)+DV(mp[1],18.0)+DV(mp[2],36.0)+DV(mp[3],6.0)+DV(mp[4],12.0)
+            +DV(mp[5],6.0)+DV(mp[6],12.0)+mp[8]*C(0.25);
+    fp[6] = DV(mp[0],9.0)+DV(mp[1],18.0)+DV(mp[2],36.0)-DV(mp[3],6.0)-DV(mp[4],12.0)
+            +DV(mp[5],6.0)+DV(mp[6],12.0)-mp[8]*C(0.25);
+    fp[7] = DV(mp[0],9.0)+DV(mp[1],18.0)+DV(mp[2],36.0)-DV(mp[3],6.0)-DV(mp[4],12.0)
+            -DV(mp[5],6.0)-DV(mp[6],12.0)+mp[8]*C(0.25);
+    fp[8] = DV(mp[0],9.0)+DV(mp[1],18.0)+DV(mp[2],36.0)+DV(mp[3],6.0)+DV(mp[4],12.0)
+            -DV(mp[5],6.0)-DV(mp[6],12.0)-mp[8]*C(0.25);
+
+    // thermal D2Q5
+    C n[5], np[5];
+    n[0] = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+    n[1] = gg[1]-gg[3];
+    n[2] = gg[2]-gg[4];
+    n[3] = gg[1]+gg[2]+gg[3]+gg[4];
+    n[4] = gg[1]-gg[2]+gg[3]-gg[4];
+#if LBM_EXACT
+    const C Qr[5] = {C(1.0), sig_k, sig_k, C(1.9), C(1.9)};
+    const C neq[5] = {T, T*u, T*v, T*C(0.5), C(0.0)};
+#pragma unroll
+    for (int a = 0; a < 5; ++a) np[a] = n[a]-Qr[a]*(n[a]-neq[a]);
+#else
+    np[0] = T;  // n(0) - 1*(n(0) - T)
+    np[1] = n[1]-sig_k*(n[1]-T*u);
+    np[2] = n[2]-sig_k*(n[2]-T*v);
+    np[3] = n[3]-C(1.9)*(n[3]-T*C(0.5));
+    np[4] = n[4]-C(1.9)*n[4];
+#endif
+    gp[0] = np[0]-np[3];
+    gp[1] = DV(np[1],2.0)+DV(np[3],4.0)+DV(np[4],4.0);
+    gp[2] = DV(np[2],2.0)+DV(np[3],4.0)-DV(np[4],4.0);
+    gp[3] = -DV(np[1],2.0)+DV(np[3],4.0)+DV(np[4],4.0);
+    gp[4] = -DV(np[2],2.0)+DV(np[3],4.0)-DV(np[4],4.0);
+}
+
+// KIND 0: fused step; KIND 1: stream + walls + macro only
+template <int ST, int KIND>
+__global__ void __launch_bounds__(256)
+k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename Tr<ST>::C *__restrict__ Fin,
+         typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+         int write_macro)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= G.nx || j >= G.ny) return;
+    const int64_t P = G.plane;
+    const int64_t id = (int64_t)j * G.pitch + i;
+    const int xa = off_a(i, G.nx), xb = off_b(i, G.nx);
+    const int64_t ya = (int64_t)off_a(j, G.ny) * G.pitch, yb = (int64_t)off_b(j, G.ny) * G.pitch;
+    C xp[3], xm[3], yp[3], ym[3];
+    load_w(G.wgt[0], i, xp, xm);
+    load_w(G.wgt[1], j, yp, ym);
+
+    auto LD = [&](int q, int64_t off) -> C {
+        C val = tocomp(__ldg(src + q * P + id + off));
+        if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        return val;
+    };
+    // y-interpolation of plane q on the column at x-offset c
+    auto YI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + ya), LD(q, c), LD(q, c + yb)); };
+
+    C f[9], gg[5];
+    f[0] = LD(0, 0);
+    f[1] = ip(xp, LD(1, xa), LD(1, 0), LD(1, xb));
+    f[2] = ip(yp, LD(2, ya), LD(2, 0), LD(2, yb));
+    f[3] = ip(xm, LD(3, xa), LD(3, 0), LD(3, xb));
+    f[4] = ip(ym, LD(4, ya), LD(4, 0), LD(4, yb));
+    f[5] = ip(xp, YI(5, yp, xa), YI(5, yp, 0), YI(5, yp, xb));
+    f[6] = ip(xm, YI(6, yp, xa), YI(6, yp, 0), YI(6, yp, xb));
+    f[7] = ip(xm, YI(7, ym, xa), YI(7, ym, 0), YI(7, ym, xb));
+    f[8] = ip(xp, YI(8, ym, xa), YI(8, ym, 0), YI(8, ym, xb));
+    gg[0] = LD(9, 0);
+    gg[1] = ip(xp, LD(10, xa), LD(10, 0), LD(10, xb));
+    gg[2] = ip(yp, LD(11, ya), LD(11, 0), LD(11, yb));
+    gg[3] = ip(xm, LD(12, xa), LD(12, 0), LD(12, xb));
+    gg[4] = ip(ym, LD(13, ya), LD(13, 0), LD(13, yb));
+
+    // walls: bounceback_u (2B:731-768), bounceback_T (2B:770-801)
+    const C two_wT = C(2.0) * C(0.125);
+    if (i == 0) {
+        f[1] = LD(3, 0); f[5] = LD(7, 0); f[8] = LD(6, 0);
+        gg[1] = -LD(12, 0) + two_wT * C(G.Thot);
+    }
+    if (i == G.nx - 1) {
+        f[3] = LD(1, 0); f[6] = LD(8, 0); f[7] = LD(5, 0);
+        gg[3] = -LD(10, 0) + two_wT * C(G.Tcold);
+    }
+    if (j == G.ny - 1) {
+        f[4] = LD(2, 0); f[7] = LD(5, 0); f[8] = LD(6, 0);
+        gg[4] = LD(11, 0);
+    }
+    if (j == 0) {
+        f[2] = LD(4, 0); f[5] = LD(7, 0); f[6] = LD(8, 0);
+        gg[2] = LD(13, 0);
+    }
+
+    // macro_u / macro_t (2M:726-753); the force is the one of the collision
+    // that produced src
+    const C Fy0 = Fin[id];
+    const C dt = C(G.dt);
+    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+#if LBM_EXACT
+    const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
+    const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
+#else
+    const C rinv = C(1.0) / rho;
+    const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
+    const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
+#endif
+    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+
+    if (write_macro || KIND == 1) {
+        const int64_t mid = (int64_t)j * G.nx + i;
+        B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
+    }
+
+    auto ST_ = [&](int q, C val) {
+        if (Tr<ST>::kShift) val -= (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        dst[q * P + id] = tostore<S, C>(val);
+    };
+    if (KIND == 1) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) ST_(q, f[q]);
+#pragma unroll
+        for (int q = 0; q < 5; ++q) ST_(9 + q, gg[q]);
+        return;
+    }
+
+    C fp[9], gp[5], Fy;
+    collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    Fout[id] = Fy;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) ST_(q, fp[q]);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) ST_(9 + q, gp[q]);
+}
+
+// ---------------------------------------------------------------------------
+// 3D: D3Q19 MRT + D3Q7
+// ---------------------------------------------------------------------------
+
+// collision_U (3M:445-669) and collision_T (3M:671-730) at one node.
+template <class C>
+__device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C u, C v, C w, C T,
+                                          const Geo &G, C fp[19], C gp[7], C &Fz)
+{
+    const C Snu = C(G.Snu), Sq = C(G.Sq), dt = C(G.dt), gbeta = C(G.gbeta), sig_k = C(G.sig_k);
+    const C Vsquare = u*u+v*v+w*w;
+    C m[19], meq[19], mp[19];
+    m[0]=f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
+    m[1]=-C(30.0)*f[0]-C(11.0)*(f[1]+f[2]+f[3]+f[4]+f[5]+f[6])+C(8.0)*(f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18]);
+    m[2]=C(12.0)*f[0]-C(4.0)*(f[1]+f[2]+f[3]+f[4]+f[5]+f[6])+(f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18]);
+    m[3]=f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14];
+    m[4]=C(4.0)*(-f[1]+f[2])+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14];
+    m[5]=f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18];
+    m[6]=-C(4.0)*(f[3]-f[4])+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18];
+    m[7]=f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18];
+    m[8]=-C(4.0)*(f[5]-f[6])+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18];
+    m[9]=C(2.0)*(f[1]+f[2])-(f[3]+f[4]+f[5]+f[6])+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]-C(2.0)*(f[15]+f[16]+f[17]+f[18]);
+    m[10]=-C(4.0)*(f[1]+f[2])+C(2.0)*(f[3]+f[4]+f[5]+f[6])+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]-C(2.0)*(f[15]+f[16]+f[17]+f[18]);
+    m[11]=f[3]+f[4]-f[5]-f[6]+f[7]+f[8]+f[9]+f[10]-f[11]-f[12]-f[13]-f[14];
+    m[12]=-C(2.0)*(f[3]+f[4]-f[5]-f[6])+f[7]+f[8]+f[9]+f[10]-f[11]-f[12]-f[13]-f[14];
+    m[13]=f[7]-f[8]-f[9]+f[10];
+    m[14]=f[15]-f[16]-f[17]+f[18];
+    m[15]=f[11]-f[12]-f[13]+f[14];
+    m[16]=f[7]-f[8]+f[9]-f[10]-f[11]+f[12]-f[13]+f[14];
+    m[17]=-f[7]-f[8]+f[9]+f[10]+f[15]-f[16]+f[17]-f[18];
+    m[18]=f[11]+f[12]-f[13]-f[14]-f[15]-f[16]+f[17]+f[18];
+
+    meq[0]=rho;
+    meq[1]=-C(11.0)*rho+C(19.0)*rho*Vsquare;
+    meq[2]=C(3.0)*rho-C(5.5)*rho*Vsquare;
+    meq[3]=rho*u;
+    meq[4]=DV(-C(2.0)*rho*u, 3.0);
+    meq[5]=rho*v;
+    meq[6]=DV(-C(2.0)*rho*v, 3.0);
+    meq[7]=rho*w;
+    meq[8]=DV(-C(2.0)*rho*w, 3.0);
+    meq[9]=C(3.0)*rho*(u*u)-rho*Vsquare;
+    meq[10]=-C(0.5)*(C(3.0)*rho*(u*u)-rho*Vsquare);
+    meq[11]=rho*((v*v)-(w*w));
+    meq[12]=-C(0.5)*rho*((v*v)-(w*w));
+    meq[13]=rho*u*v;
+    meq[14]=rho*v*w;
+    meq[15]=rho*u*w;
+
+    Fz = gbeta*T*rho;
+#if LBM_EXACT
+    const C sv[19] = {C(0.0), Snu, Snu, C(0.0), Sq, C(0.0), Sq, C(0.0), Sq, Snu, Snu, Snu, Snu, Snu, Snu, Snu, Sq, Sq, Sq};
+    meq[16]=C(0.0); meq[17]=C(0.0); meq[18]=C(0.0);
+    C src[19];
+    src[0] = C(0.0);
+    src[1] = (C(38.0)-C(19.0)*sv[1])*w*Fz;
+    src[2] = -(C(11.0)-C(5.5)*sv[2])*w*Fz;
+    src[3] = C(0.0); src[4] = C(0.0); src[5] = C(0.0); src[6] = C(0.0);
+    src[7] = (C(1.0)-C(0.5)*sv[7])*Fz;
+    src[8] = -C(2.0)*(C(1.0)-C(0.5)*sv[8])*Fz/C(3.0);
+    src[9] = (-C(2.0)+sv[9])*w*Fz;
+    src[10] = (C(1.0)-C(0.5)*sv[10])*w*Fz;
+    src[11] = -(C(2.0)-sv[11])*w*Fz;
+    src[12] = (C(1.0)-C(0.5)*sv[12])*w*Fz;
+    src[13] = C(0.0);
+    src[14] = (C(1.0)-C(0.5)*sv[14])*v*Fz;
+    src[15] = (C(1.0)-C(0.5)*sv[15])*u*Fz;
+    src[16] = C(0.0); src[17] = C(0.0); src[18] = C(0.0);
+#pragma unroll
+    for (int a = 0; a < 19; ++a) mp[a] = m[a]-sv[a]*(m[a]-meq[a])+src[a]*dt;
+#else
+    const C wF = w*Fz*dt;
+    const C hNu = C(1.0)-C(0.5)*Snu;
+    mp[0] = m[0];
+    mp[1] = m[1]-Snu*(m[1]-meq[1])+(C(38.0)-C(19.0)*Snu)*wF;
+    mp[2] = m[2]-Snu*(m[2]-meq[2])-(C(11.0)-C(5.5)*Snu)*wF;
+    mp[3] = m[3];
+    mp[4] = m[4]-Sq*(m[4]-meq[4]);
+    mp[5] = m[5];
+    mp[6] = m[6]-Sq*(m[6]-meq[6]);
+    mp[7] = m[7]+Fz*dt;
+    mp[8] = m[8]-Sq*(m[8]-meq[8])-DV(C(2.0)*(C(1.0)-C(0.5)*Sq)*Fz*dt, 3.0);
+    mp[9] = m[9]-Snu*(m[9]-meq[9])+(-C(2.0)+Snu)*wF;
+    mp[10] = m[10]-Snu*(m[10]-meq[10])+hNu*wF;
+    mp[11] = m[11]-Snu*(m[11]-meq[11])-(C(2.0)-Snu)*wF;
+    mp[12] = m[12]-Snu*(m[12]-meq[12])+hNu*wF;
+    mp[13] = m[13]-Snu*(m[13]-meq[13]);
+    mp[14] = m[14]-Snu*(m[14]-meq[14])+hNu*v*Fz*dt;
+    mp[15] = m[15]-Snu*(m[15]-meq[15])+hNu*u*Fz*dt;
+    mp[16] = m[16]-Sq*m[16];
+    mp[17] = m[17]-Sq*m[17];
+    mp[18] = m[18]-Sq*m[18];
+#endif
+
+    fp[0]=DV(mp[0],19.0)-DV(C(5.0)*mp[1],399.0)+DV(mp[2],21.0);
+    fp[1]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)+DV(mp[3],10.0)-DV(mp[4],10.0)+DV(mp[9],18.0)-DV(mp[10],18.0);
+    fp[2]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)-DV(mp[3],10.0)+DV(mp[4],10.0)+DV(mp[9],18.0)-DV(mp[10],18.0);
+    fp[3]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)+DV(mp[5],10.0)-DV(mp[6],10.0)-DV(mp[9],36.0)+DV(mp[10],36.0)+DV(mp[11],12.0)-DV(mp[12],12.0);
+    fp[4]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)-DV(mp[5],10.0)+DV(mp[6],10.0)-DV(mp[9],36.0)+DV(mp[10],36.0)+DV(mp[11],12.0)-DV(mp[12],12.0);
+    fp[5]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)+DV(mp[7],10.0)-DV(mp[8],10.0)-DV(mp[9],36.0)+DV(mp[10],36.0)-DV(mp[11],12.0)+DV(mp[12],12.0);
+    fp[6]=DV(mp[0],19.0)-DV(C(11.0)*mp[1],2394.0)-DV(mp[2],63.0)-DV(mp[7],10.0)+DV(mp[8],10.0)-DV(mp[9],36.0)+DV(mp[10],36.0)-DV(mp[11],12.0)+DV(mp[12],12.0);
+    fp[7]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[3],10.0)+DV(mp[4],40.0)+DV(mp[5],10.0)+DV(mp[6],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          +DV(mp[11],12.0)+DV(mp[12],24.0)+DV(mp[13],4.0)+DV(mp[16],8.0)-DV(mp[17],8.0);
+    fp[8]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[3],10.0)-DV(mp[4],40.0)+DV(mp[5],10.0)+DV(mp[6],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          +DV(mp[11],12.0)+DV(mp[12],24.0)-DV(mp[13],4.0)-DV(mp[16],8.0)-DV(mp[17],8.0);
+    fp[9]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[3],10.0)+DV(mp[4],40.0)-DV(mp[5],10.0)-DV(mp[6],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          +DV(mp[11],12.0)+DV(mp[12],24.0)-DV(mp[13],4.0)+DV(mp[16],8.0)+DV(mp[17],8.0);
+    fp[10]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[3],10.0)-DV(mp[4],40.0)-DV(mp[5],10.0)-DV(mp[6],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          +DV(mp[11],12.0)+DV(mp[12],24.0)+DV(mp[13],4.0)-DV(mp[16],8.0)+DV(mp[17],8.0);
+    fp[11]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[3],10.0)+DV(mp[4],40.0)+DV(mp[7],10.0)+DV(mp[8],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          -DV(mp[11],12.0)-DV(mp[12],24.0)+DV(mp[15],4.0)-DV(mp[16],8.0)+DV(mp[18],8.0);
+    fp[12]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[3],10.0)-DV(mp[4],40.0)+DV(mp[7],10.0)+DV(mp[8],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          -DV(mp[11],12.0)-DV(mp[12],24.0)-DV(mp[15],4.0)+DV(mp[16],8.0)+DV(mp[18],8.0);
+    fp[13]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[3],10.0)+DV(mp[4],40.0)-DV(mp[7],10.0)-DV(mp[8],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          -DV(mp[11],12.0)-DV(mp[12],24.0)-DV(mp[15],4.0)-DV(mp[16],8.0)-DV(mp[18],8.0);
+    fp[14]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[3],10.0)-DV(mp[4],40.0)-DV(mp[7],10.0)-DV(mp[8],40.0)+DV(mp[9],36.0)+DV(mp[10],72.0)
+          -DV(mp[11],12.0)-DV(mp[12],24.0)+DV(mp[15],4.0)+DV(mp[16],8.0)-DV(mp[18],8.0);
+    fp[15]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[5],10.0)+DV(mp[6],40.0)+DV(mp[7],10.0)+DV(mp[8],40.0)-DV(mp[9],18.0)-DV(mp[10],36.0)
+          +DV(mp[14],4.0)+DV(mp[17],8.0)-DV(mp[18],8.0);
+    fp[16]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[5],10.0)-DV(mp[6],40.0)+DV(mp[7],10.0)+DV(mp[8],40.0)-DV(mp[9],18.0)-DV(mp[10],36.0)
+          -DV(mp[14],4.0)-DV(mp[17],8.0)-DV(mp[18],8.0);
+    fp[17]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)+DV(mp[5],10.0)+DV(mp[6],40.0)-DV(mp[7],10.0)-DV(mp[8],40.0)-DV(mp[9],18.0)-DV(mp[10],36.0)
+          -DV(mp[14],4.0)+DV(mp[17],8.0)+DV(mp[18],8.0);
+    fp[18]=DV(mp[0],19.0)+DV(C(4.0)*mp[1],1197.0)+DV(mp[2],252.0)-DV(mp[5],10.0)-DV(mp[6],40.0)-DV(mp[7],10.0)-DV(mp[8],40.0)-DV(mp[9],18.0)-DV(mp[10],36.0)
+          +DV(mp[14],4.0)-DV(mp[17],8.0)+DV(mp[18],8.0);
+
+    // thermal D3Q7
+    C n[7], np[7];
+    n[0] = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+    n[1] = gg[1]-gg[2];
+    n[2] = gg[3]-gg[4];
+    n[3] = gg[5]-gg[6];
+    n[4] = gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+    n[5] = gg[1]+gg[2]-gg[3]-gg[4];
+    n[6] = gg[1]+gg[2]-gg[5]-gg[6];
+#if LBM_EXACT
+    const C Qr[7] = {C(1.0), sig_k, sig_k, sig_k, C(1.2), C(1.2), C(1.2)};
+    const C neq[7] = {T, T*u, T*v, T*w, T*C(0.5), C(0.0), C(0.0)};
+#pragma unroll
+    for (int a = 0; a < 7; ++a) np[a] = n[a]-Qr[a]*(n[a]-neq[a]);
+#else
+    np[0] = T;
+    np[1] = n[1]-sig_k*(n[1]-T*u);
+    np[2] = n[2]-sig_k*(n[2]-T*v);
+    np[3] = n[3]-sig_k*(n[3]-T*w);
+    np[4] = n[4]-C(1.2)*(n[4]-T*C(0.5));
+    np[5] = n[5]-C(1.2)*n[5];
+    np[6] = n[6]-C(1.2)*n[6];
+#endif
+    gp[0] = np[0]-np[4];
+    gp[1] = DV(np[1],2.0)+DV(np[4],6.0)+DV(np[5],6.0)+DV(np[6],6.0);
+    gp[2] = -DV(np[1],2.0)+DV(np[4],6.0)+DV(np[5],6.0)+DV(np[6],6.0);
+    gp[3] = DV(np[2],2.0)+DV(np[4],6.0)-DV(np[5],3.0)+DV(np[6],6.0);
+    gp[4] = -DV(np[2],2.0)+DV(np[4],6.0)-DV(np[5],3.0)+DV(np[6],6.0);
+    gp[5] = DV(np[3],2.0)+DV(np[4],6.0)+DV(np[5],6.0)-DV(np[6],3.0);
+    gp[6] = -DV(np[3],2.0)+DV(np[4],6.0)+DV(np[5],6.0)-DV(np[6],3.0);
+}
+
+template <int ST, int KIND>
+__global__ void __launch_bounds__(256)
+k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename Tr<ST>::C *__restrict__ Fin,
+         typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+         int write_macro)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= G.nx || j >= G.ny) return;
+    const int64_t P = G.plane;
+    const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
+    const int64_t xa = off_a(i, G.nx), xb = off_b(i, G.nx);
+    const int64_t ya = (int64_t)off_a(j, G.ny) * G.pitch, yb = (int64_t)off_b(j, G.ny) * G.pitch;
+    const int64_t za = (int64_t)off_a(k, G.nz) * G.slab, zb = (int64_t)off_b(k, G.nz) * G.slab;
+    C xp[3], xm[3], yp[3], ym[3], zp[3], zm[3];
+    load_w(G.wgt[0], i, xp, xm);
+    load_w(G.wgt[1], j, yp, ym);
+    load_w(G.wgt[2], k, zp, zm);
+
+    auto LD = [&](int q, int64_t off) -> C {
+        C val = tocomp(__ldg(src + q * P + id + off));
+        if (Tr<ST>::kShift) val += (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+        return val;
+    };
+    auto YI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + ya), LD(q, c), LD(q, c + yb)); };
+    auto ZI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + za), LD(q, c), LD(q, c + zb)); };
+
+    C f[19], gg[7];
+    f[0] = LD(0, 0);
+    // axis directions: one-dimensional interpolation (the zero-shift axis
+    // weights of the reference's in-plane scheme are exactly (0, 1, 0))
+    f[1] = ip(xp, LD(1, xa), LD(1, 0), LD(1, xb));
+    f[2] = ip(xm, LD(2, xa), LD(2, 0), LD(2, xb));
+    f[3] = ip(yp, LD(3, ya), LD(3, 0), LD(3, yb));
+    f[4] = ip(ym, LD(4, ya), LD(4, 0), LD(4, yb));
+    f[5] = ip(zp, LD(5, za), LD(5, 0), LD(5, zb));
+    f[6] = ip(zm, LD(6, za), LD(6, 0), LD(6, zb));
+    // xoy plane (3M:807-824): y-interpolation on three x-columns, then x
+    f[7] = ip(xp, YI(7, yp, xa), YI(7, yp, 0), YI(7, yp, xb));
+    f[8] = ip(xm, YI(8, yp, xa), YI(8, yp, 0), YI(8, yp, xb));
+    f[9] = ip(xp, YI(9, ym, xa), YI(9, ym, 0), YI(9, ym, xb));
+    f[10] = ip(xm, YI(10, ym, xa), YI(10, ym, 0), YI(10, ym, xb));
+    // xoz plane (3M:787-804): z-interpolation on three x-columns, then x
+    f[11] = ip(xp, ZI(11, zp, xa), ZI(11, zp, 0), ZI(11, zp, xb));
+    f[12] = ip(xm, ZI(12, zp, xa), ZI(12, zp, 0), ZI(12, zp, xb));
+    f[13] = ip(xp, ZI(13, zm, xa), ZI(13, zm, 0), ZI(13, zm, xb));
+    f[14] = ip(xm, ZI(14, zm, xa), ZI(14, zm, 0), ZI(14, zm, xb));
+    // yoz plane (3M:767-784): z-interpolation on three y-rows, then y
+    f[15] = ip(yp, ZI(15, zp, ya), ZI(15, zp, 0), ZI(15, zp, yb));
+    f[16] = ip(ym, ZI(16, zp, ya), ZI(16, zp, 0), ZI(16, zp, yb));
+    f[17] = ip(yp, ZI(17, zm, ya), ZI(17, zm, 0), ZI(17, zm, yb));
+    f[18] = ip(ym, ZI(18, zm, ya), ZI(18, zm, 0), ZI(18, zm, yb));
+    // D3Q7 (3M:831-859)
+    gg[0] = LD(19, 0);
+    gg[1] = ip(xp, LD(20, xa), LD(20, 0), LD(20, xb));
+    gg[2] = ip(xm, LD(21, xa), LD(21, 0), LD(21, xb));
+    gg[3] = ip(yp, LD(22, ya), LD(22, 0), LD(22, yb));
+    gg[4] = ip(ym, LD(23, ya), LD(23, 0), LD(23, yb));
+    gg[5] = ip(zp, LD(24, za), LD(24, 0), LD(24, zb));
+    gg[6] = ip(zm, LD(25, za), LD(25, 0), LD(25, zb));
+
+    // walls: bounceback_u (3B:1053-1136), bounceback_T (3B:1138-1197)
+    const C two_wT = C(2.0) * (C(1.0) / C(12.0));
+    if (j == 0) {
+        f[3] = LD(4, 0); f[7] = LD(10, 0); f[8] = LD(9, 0); f[15] = LD(18, 0); f[17] = LD(16, 0);
+        gg[3] = -LD(23, 0) + two_wT * C(G.Thot);
+    }
+    if (j == G.ny - 1) {
+        f[4] = LD(3, 0); f[9] = LD(8, 0); f[10] = LD(7, 0); f[16] = LD(17, 0); f[18] = LD(15, 0);
+        gg[4] = -LD(22, 0) + two_wT * C(G.Tcold);
+    }
+    if (i == 0) {
+        f[1] = LD(2, 0); f[9] = LD(8, 0); f[7] = LD(10, 0); f[13] = LD(12, 0); f[11] = LD(14, 0);
+        gg[1] = LD(21, 0);
+    }
+    if (i == G.nx - 1) {
+        f[2] = LD(1, 0); f[8] = LD(9, 0); f[10] = LD(7, 0); f[12] = LD(13, 0); f[14] = LD(11, 0);
+        gg[2] = LD(20, 0);
+    }
+    if (k == 0) {
+        f[5] = LD(6, 0); f[11] = LD(14, 0); f[12] = LD(13, 0); f[15] = LD(18, 0); f[16] = LD(17, 0);
+        gg[5] = LD(25, 0);
+    }
+    if (k == G.nz - 1) {
+        f[6] = LD(5, 0); f[13] = LD(12, 0); f[14] = LD(11, 0); f[17] = LD(16, 0); f[18] = LD(15, 0);
+        gg[6] = LD(24, 0);
+    }
+
+    // macro_u / macro_t (3M:988-1025)
+    const C Fz0 = Fin[id];
+    const C dt = C(G.dt);
+    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
+#if LBM_EXACT
+    const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
+    const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
+    const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)/rho;
+#else
+    const C rinv = C(1.0) / rho;
+    const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])*rinv;
+    const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
+    const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
+#endif
+    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+
+    if (write_macro || KIND == 1) {
+        const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
+        B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
+        B.w[mid] = double(w); B.T[mid] = double(T);
+    }
+    auto ST_ = [&](int q, C val) {
+        if (Tr<ST>::kShift) val -= (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+        dst[q * P + id] = tostore<S, C>(val);
+    };
+    if (KIND == 1) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) ST_(q, f[q]);
+#pragma unroll
+        for (int q = 0; q < 7; ++q) ST_(19 + q, gg[q]);
+        return;
+    }
+    C fp[19], gp[7], Fz;
+    collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+    Fout[id] = Fz;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) ST_(q, fp[q]);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) ST_(19 + q, gp[q]);
+}
+
+// ---------------------------------------------------------------------------
+// initial equilibrium (2M:227-240, 3M:286-301) and the first collision
+// ---------------------------------------------------------------------------
+template <int ST>
+__global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop, const Bufs B)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= G.nnode) return;
+    const int i = int(n % G.nx);
+    const int j = int((n / G.nx) % G.ny);
+    const int k = int(n / ((int64_t)G.nx * G.ny));
+    const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
+    const int64_t P = G.plane;
+    // FP64 here in every storage mode: the initial state is formed once
+    const double rho = B.rho[n], u = B.u[n], v = B.v[n], T = B.T[n];
+    const double w = G.dim == 3 ? B.w[n] : 0.0;
+    if (G.dim == 2) {
+        const int ex[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+        const int ey[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+        const double wU[9] = {4.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0};
+        const double wT[5] = {1.0/2.0, 1.0/8.0, 1.0/8.0, 1.0/8.0, 1.0/8.0};
+        const double velocitySquare = u*u+v*v;
+        for (int a = 0; a < 9; ++a) {
+            const double un = u*ex[a]+v*ey[a];
+            double fa = rho*wU[a]*(1.0+3.0*un+4.5*un*un-1.5*velocitySquare);
+            if (Tr<ST>::kShift) fa -= wU[a];
+            pop[a * P + id] = tostore<S, C>(C(fa));
+        }
+        for (int a = 0; a < 5; ++a) {
+            const double un = u*ex[a]+v*ey[a];
+            double ga = wT[a]*T*(1.0+4.0*un);
+            if (Tr<ST>::kShift) ga -= wT[a] * G.T0;
+            pop[(9 + a) * P + id] = tostore<S, C>(C(ga));
+        }
+    } else {
+        const int ex[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+        const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+        const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+        const double us2 = u*u+v*v+w*w;
+        for (int a = 0; a < 19; ++a) {
+            const double wa = a == 0 ? 1.0/3.0 : (a < 7 ? 1.0/18.0 : 1.0/36.0);
+            const double un = u*ex[a]+v*ey[a]+w*ez[a];
+            double fa = wa*rho*(1.0+3.0*un+4.5*un*un-1.5*us2);
+            if (Tr<ST>::kShift) fa -= wa;
+            pop[a * P + id] = tostore<S, C>(C(fa));
+        }
+        for (int a = 0; a < 7; ++a) {
+            const double wa = a == 0 ? 1.0/2.0 : 1.0/12.0;
+            const double un = u*ex[a]+v*ey[a]+w*ez[a];
+            double ga = wa*T*(1.0+6.0*un);
+            if (Tr<ST>::kShift) ga -= wa * G.T0;
+            pop[(19 + a) * P + id] = tostore<S, C>(C(ga));
+        }
+    }
+}
+
+// The first collision of a run, from pre-collision populations and the
+// macroscopic fields held in B (what the reference's loop starts from).
+template <int ST>
+__global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in,
+                          typename Tr<ST>::S *__restrict__ out, typename Tr<ST>::C *__restrict__ Fout,
+                          const Bufs B)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= G.nnode) return;
+    const int i = int(n % G.nx);
+    const int j = int((n / G.nx) % G.ny);
+    const int k = int(n / ((int64_t)G.nx * G.ny));
+    const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
+    const int64_t P = G.plane;
+    const int Q = G.dim == 2 ? 9 : 19, QT = G.dim == 2 ? 5 : 7;
+    auto shift = [&](int q) -> C {
+        if (!Tr<ST>::kShift) return C(0);
+        if (G.dim == 2) return q < 9 ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        return q < 19 ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+    };
+    C f[19], gg[7], fp[19], gp[7], F;
+    for (int q = 0; q < Q; ++q) f[q] = tocomp(in[q * P + id]) + shift(q);
+    for (int q = 0; q < QT; ++q) gg[q] = tocomp(in[(Q + q) * P + id]) + shift(Q + q);
+    const C rho = C(B.rho[n]), u = C(B.u[n]), v = C(B.v[n]), T = C(B.T[n]);
+    if (G.dim == 2) {
+        collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, F);
+    } else {
+        const C w = C(B.w[n]);
+        collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, F);
+    }
+    Fout[id] = F;
+    for (int q = 0; q < Q; ++q) out[q * P + id] = tostore<S, C>(fp[q] - shift(q));
+    for (int q = 0; q < QT; ++q) out[(Q + q) * P + id] = tostore<S, C>(gp[q] - shift(Q + q));
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <int ST>
+static cudaError_t launch_step(const Geo &g, const void *pin, const void *Fin, void *pout, void *Fout,
+                               const Bufs &b, int wm, int kind, cudaStream_t s)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    dim3 blk(32, 8, 1);
+    if (g.dim == 2) {
+        dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, 1);
+        if (kind == 0)
+            k_step2d<ST, 0><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
+        else
+            k_step2d<ST, 1><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
+    } else {
+        dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+        if (kind == 0)
+            k_step3d<ST, 0><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
+        else
+            k_step3d<ST, 1><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
+    }
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+#if LBM_EXACT
+#define LBM_DISPATCH(store, CALL)                          \
+    switch (store) {                                       \
+    case kF64: return CALL(kF64);                          \
+    default: return cudaErrorNotSupported;                 \
+    }
+#else
+#define LBM_DISPATCH(store, CALL)                          \
+    switch (store) {                                       \
+    case kF64: return CALL(kF64);                          \
+    case kF32: return CALL(kF32);                          \
+    case kF16S: return CALL(kF16S);                        \
+    default: return cudaErrorNotSupported;                 \
+    }
+#endif
+
+cudaError_t step(const Geo &g, int store, const void *pop_in, const void *F_in, void *pop_out, void *F_out,
+                 const Bufs &b, int write_macro, cudaStream_t s)
+{
+#define CALL(ST) launch_step<ST>(g, pop_in, F_in, pop_out, F_out, b, write_macro, 0, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in, void *pop_out,
+                        const Bufs &b, cudaStream_t s)
+{
+#define CALL(ST) launch_step<ST>(g, pop_in, F_in, pop_out, nullptr, b, 1, 1, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+template <int ST>
+static cudaError_t launch_eq(const Geo &g, void *pop, const Bufs &b, cudaStream_t s)
+{
+    const int64_t n = g.nnode;
+    k_equilibrium<ST><<<unsigned((n + 255) / 256), 256, 0, s>>>(g, (typename Tr<ST>::S *)pop, b);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, cudaStream_t s)
+{
+#define CALL(ST) launch_eq<ST>(g, pop, b, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+template <int ST>
+static cudaError_t launch_collide(const Geo &g, const void *in, void *out, void *Fout, const Bufs &b,
+                                  cudaStream_t s)
+{
+    const int64_t n = g.nnode;
+    k_collide<ST><<<unsigned((n + 127) / 128), 128, 0, s>>>(g, (const typename Tr<ST>::S *)in,
+                                                          (typename Tr<ST>::S *)out,
+                                                          (typename Tr<ST>::C *)Fout, b);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out, void *F_out, const Bufs &b,
+                    cudaStream_t s)
+{
+#define CALL(ST) launch_collide<ST>(g, pop_in, pop_out, F_out, b, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+}  // namespace LBM_NS
+}  // namespace lbm

@@ -1,0 +1,340 @@
+"""Python host mirror of the reference's time-step interface over the C ABI.
+
+The reference (zzhao0930/MPI-Multi-Process-Version) drives its step from
+`program main` (natural-convection_2dim_mono.f90:283-380): mesh(), initial(),
+then a `do while` loop over collision/streaming/boundary/macro subroutines with
+check() every 2000 iterations, an MLUPS print and a Tecplot ASCII dump.  This
+module keeps those names and meanings (`mesh`, `Cavity.initial`,
+`Cavity.step`, `Cavity.check`, `run_main`, `output_ascii`) and calls the CUDA
+library liblbm_b200.so through ctypes.  There is no CPU fallback: if the
+library or a CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbm_b200.so")
+
+LBM_OK = 0
+STORE = {"f64": 0, "f32": 1, "f16s": 2}
+MODE = {"fast": 0, "exact": 1}
+GRID = {"erf": 0, "tanh": 1, "uniform": 2}
+
+# every symbol include/lbm_b200.h declares
+EXPORTS = [
+    "lbm_abi_version", "lbm_error_string", "lbm_last_error", "lbm_mesh", "lbm_derived_params",
+    "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_itc",
+    "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
+    "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
+]
+
+
+class LBMError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+class lbm_params(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("Ra", ctypes.c_double), ("Pr", ctypes.c_double), ("Ma", ctypes.c_double),
+        ("Thot", ctypes.c_double), ("Tcold", ctypes.c_double),
+        ("dt", ctypes.c_double), ("length_LB", ctypes.c_double),
+        ("storage", ctypes.c_int32), ("mode", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_lib = None
+
+
+def lib():
+    """Load liblbm_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run build.py (the CUDA path has no fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.lbm_error_string.restype = ctypes.c_char_p
+        L.lbm_last_error.restype = ctypes.c_char_p
+        L.lbm_mesh.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                               _dp, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_derived_params.argtypes = [ctypes.POINTER(lbm_params), _dp]
+        L.lbm_create.argtypes = [ctypes.POINTER(lbm_params), _dp, _dp, _dp, ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_destroy.argtypes = [ctypes.c_void_p]
+        L.lbm_init_reference.argtypes = [ctypes.c_void_p]
+        L.lbm_init_equilibrium.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_step.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.lbm_itc.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_check.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_nusselt.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_sums.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_get_macro.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_set_macro.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_get_populations.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_set_populations.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_synchronize.argtypes = [ctypes.c_void_p]
+        L.lbm_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_kernel_launches.restype = ctypes.c_int64
+        _lib = L
+    return _lib
+
+
+def _chk(status: int, where: str):
+    if status != LBM_OK:
+        raise LBMError(status, where, lib().lbm_last_error().decode())
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous, "need contiguous float64"
+    return a.ctypes.data_as(_dp)
+
+
+def kernel_launches() -> int:
+    return int(lib().lbm_kernel_launches())
+
+
+# ---------------------------------------------------------------------------
+# mesh(): 2M:74-134 / 3M:122-189
+# ---------------------------------------------------------------------------
+@dataclass
+class Mesh:
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray | None
+    dx0: float
+    length_LB: float
+    dt: float
+
+
+def mesh(nx: int, ny: int, nz: int = 0, grid: str = "erf", stretch: float = 3.2) -> Mesh:
+    """The reference's grid: erf-stretched (constA = 3.2) by default; tanh and
+    uniform grids go through the same shift/scale (2M:94-116)."""
+    x, y = np.zeros(nx + 2), np.zeros(ny + 2)
+    z = np.zeros(nz + 2) if nz else None
+    out = np.zeros(3)
+    _chk(lib().lbm_mesh(GRID[grid], float(stretch), nx, ny, nz, _p(x), _p(y), _p(z),
+                        _p(out[0:1]), _p(out[1:2]), _p(out[2:3])), "lbm_mesh")
+    return Mesh(x, y, z, float(out[0]), float(out[1]), float(out[2]))
+
+
+# ---------------------------------------------------------------------------
+# one cavity
+# ---------------------------------------------------------------------------
+class Cavity:
+    """A differentially heated cavity on one GPU.
+
+    dim=2: D2Q9 MRT + D2Q5 (hot wall x = 1, cold wall x = nx, gravity along y);
+    dim=3: D3Q19 MRT + D3Q7 (hot wall y = 1, cold wall y = ny, gravity along z),
+    as in the reference.  Fields come back in the Fortran layout a(nx, ny[, nz])
+    as numpy arrays of shape (ny, nx) / (nz, ny, nx) (C order, x fastest)."""
+
+    def __init__(self, dim: int, nx: int, ny: int, nz: int = 1, Ra: float = 1e5, Pr: float = 0.71,
+                 Ma: float = 0.1, Thot: float = 1.0, Tcold: float = 0.0, grid: str = "erf",
+                 stretch: float = 3.2, storage: str = "f64", mode: str = "fast", device: int = 0,
+                 coords: Mesh | None = None):
+        if dim == 2:
+            nz = 1
+        m = coords or mesh(nx, ny, nz if dim == 3 else 0, grid, stretch)
+        self.mesh = m
+        self.dim, self.nx, self.ny, self.nz = dim, nx, ny, nz
+        self.Q, self.QT = (9, 5) if dim == 2 else (19, 7)
+        self.params = lbm_params(dim, nx, ny, nz, float(Ra), float(Pr), float(Ma), float(Thot), float(Tcold),
+                                 m.dt, m.length_LB, STORE[storage], MODE[mode], int(device), 0)
+        self.storage, self.mode = storage, mode
+        h = ctypes.c_void_p()
+        self._x = np.ascontiguousarray(m.x)
+        self._y = np.ascontiguousarray(m.y)
+        self._z = np.ascontiguousarray(m.z) if m.z is not None else None
+        _chk(lib().lbm_create(ctypes.byref(self.params), _p(self._x), _p(self._y), _p(self._z), ctypes.byref(h)),
+             "lbm_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().lbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.ny, self.nx) if self.dim == 2 else (self.nz, self.ny, self.nx)
+
+    @property
+    def nnode(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    def derived(self) -> dict:
+        out = np.zeros(9)
+        _chk(lib().lbm_derived_params(ctypes.byref(self.params), _p(out)), "lbm_derived_params")
+        keys = ["viscosity_LB", "kappa", "gbeta", "tauf", "Snu", "Sq", "sig_k", "dt", "length_LB"]
+        return dict(zip(keys, out.tolist()))
+
+    # initial(): 2M:136-281
+    def initial(self):
+        _chk(lib().lbm_init_reference(self.h), "lbm_init_reference")
+        return self
+
+    def init_equilibrium(self, rho, u, v, w, T):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, w, T)]
+        _chk(lib().lbm_init_equilibrium(self.h, *[_p(a) for a in arrs]), "lbm_init_equilibrium")
+        return self
+
+    def step(self, n: int = 1):
+        _chk(lib().lbm_step(self.h, int(n)), "lbm_step")
+
+    @property
+    def itc(self) -> int:
+        v = ctypes.c_int64()
+        _chk(lib().lbm_itc(self.h, ctypes.byref(v)), "lbm_itc")
+        return int(v.value)
+
+    def check(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _chk(lib().lbm_check(self.h, ctypes.byref(a), ctypes.byref(b)), "lbm_check")
+        return a.value, b.value
+
+    def nusselt(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _chk(lib().lbm_nusselt(self.h, ctypes.byref(a), ctypes.byref(b)), "lbm_nusselt")
+        return a.value, b.value
+
+    def sums(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _chk(lib().lbm_sums(self.h, ctypes.byref(a), ctypes.byref(b)), "lbm_sums")
+        return a.value, b.value
+
+    def macro(self) -> dict:
+        out = {k: np.zeros(self.shape) for k in ("rho", "u", "v", "w", "T")}
+        _chk(lib().lbm_get_macro(self.h, *[_p(out[k]) for k in ("rho", "u", "v", "w", "T")]), "lbm_get_macro")
+        if self.dim == 2:
+            del out["w"]
+        return out
+
+    def get_macro_into(self, rho=None, u=None, v=None, w=None, T=None):
+        """Copy the macroscopic fields into caller-owned float64 arrays (e.g. pinned)."""
+        _chk(lib().lbm_get_macro(self.h, _p(rho), _p(u), _p(v), _p(w), _p(T)), "lbm_get_macro")
+
+    def set_macro(self, rho=None, u=None, v=None, w=None, T=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, w, T)]
+        _chk(lib().lbm_set_macro(self.h, *[_p(a) for a in arrs]), "lbm_set_macro")
+
+    def populations(self):
+        f = np.zeros(self.shape + (self.Q,))
+        g = np.zeros(self.shape + (self.QT,))
+        _chk(lib().lbm_get_populations(self.h, _p(f), _p(g)), "lbm_get_populations")
+        return f, g
+
+    def set_populations(self, f, g):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        assert f.size == self.nnode * self.Q and g.size == self.nnode * self.QT
+        _chk(lib().lbm_set_populations(self.h, _p(f), _p(g)), "lbm_set_populations")
+
+    def synchronize(self):
+        _chk(lib().lbm_synchronize(self.h), "lbm_synchronize")
+
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        _chk(lib().lbm_stream(self.h, ctypes.byref(s)), "lbm_stream")
+        return int(s.value or 0)
+
+    def device_bytes(self) -> int:
+        v = ctypes.c_int64()
+        _chk(lib().lbm_device_bytes(self.h, ctypes.byref(v)), "lbm_device_bytes")
+        return int(v.value)
+
+
+# ---------------------------------------------------------------------------
+# program main (2M:283-380): loop with check every 2000 iterations
+# ---------------------------------------------------------------------------
+def run_main(cav: Cavity, itc_max: int = 20000, eps: float = float(np.float32(1e-6)),
+             check_every: int = 2000, log=print):
+    """The reference's driver loop: iterate while (errorU > epsU or errorT > epsT)
+    and itc < itc_max, calling check() every `check_every` iterations and
+    printing `itc errorU errorT` (2M:307-330, 800-802).  epsU = 1e-6 is a
+    single-precision literal in the reference (2M:35), hence float32(1e-6).
+    Returns (itc, errorU, errorT, seconds, MLUPS)."""
+    errU = errT = 100.0
+    itc = cav.itc
+    t0 = time.perf_counter()
+    while (errU > eps or errT > eps) and itc < itc_max:
+        n = min(check_every - itc % check_every, itc_max - itc)
+        cav.step(n)
+        itc += n
+        if itc % check_every == 0:
+            errU, errT = cav.check()
+            if log:
+                log(f"{itc:12d}   {errU:.15E}   {errT:.15E}")
+    cav.synchronize()
+    dt = time.perf_counter() - t0
+    mlups = cav.nnode / 1e6 * itc / dt if dt > 0 else float("nan")
+    return itc, errU, errT, dt, mlups
+
+
+def fortran_e(v: float, w: int, d: int) -> str:
+    """Fortran `Ew.d` edit descriptor: 0.ddddE+xx right-justified in w columns."""
+    v = float(v)
+    if v == 0.0:
+        s = "0." + "0" * d + "E+00"
+    else:
+        mant, ex = f"{abs(v):.{d - 1}E}".split("E")
+        exp = int(ex) + 1
+        s = "0." + mant.replace(".", "") + f"E{'+' if exp >= 0 else '-'}{abs(exp):02d}"
+        if v < 0:
+            s = "-" + s
+    return s.rjust(w)
+
+
+def output_ascii(cav: Cavity, path: str):
+    """Tecplot POINT file in the reference's format: output_ASCII
+    (2M:818-843: X Y U V T rho; 3M:1097-1121: X Y Z U V W RHO T), Fortran
+    formats (1x,2(e11.4,' '),10(e13.6,' '))."""
+    m = cav.macro()
+    x, y = cav.mesh.x, cav.mesh.y
+
+    e = fortran_e
+    with open(path, "w") as fh:
+        if cav.dim == 2:
+            fh.write(' TITLE="thermal convective flows"\n')
+            fh.write(' VARIABLES="X" "Y" "U" "V" "T" "rho"\n')
+            fh.write(f"ZONE I= {cav.nx:5d}  J= {cav.ny:5d} F=POINT\n")
+            for j in range(cav.ny):
+                for i in range(cav.nx):
+                    vals = [m["u"][j, i], m["v"][j, i], m["T"][j, i], m["rho"][j, i]]
+                    fh.write(" " + e(x[i + 1], 11, 4) + " " + e(y[j + 1], 11, 4) + " "
+                             + " ".join(e(v, 13, 6) for v in vals) + " \n")
+        else:
+            z = cav.mesh.z
+            fh.write(' TITLE="side-heated convection "\n')
+            fh.write(' VARIABLES="X" "Y" "Z" "U" "V" "W" "RHO" "T" \n')
+            fh.write(f"ZONE I= {cav.nx:5d}  J= {cav.ny:5d} K= {cav.nz:5d} F=POINT\n")
+            for k in range(cav.nz):
+                for j in range(cav.ny):
+                    for i in range(cav.nx):
+                        vals = [z[k + 1], m["u"][k, j, i], m["v"][k, j, i], m["w"][k, j, i],
+                                m["rho"][k, j, i], m["T"][k, j, i]]
+                        fh.write(" " + e(x[i + 1], 11, 4) + " " + e(y[j + 1], 11, 4) + " "
+                                 + " ".join(e(v, 13, 6) for v in vals) + " \n")

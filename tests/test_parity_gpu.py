@@ -1,0 +1,194 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the CPU
+oracle on the same grids and parameters.
+
+exact mode   FP64, the reference's operation order, no contraction: populations
+             and macroscopic fields bit-identical to the oracle;
+fast mode    FP64 with multiply-add contraction: <= 1e-12 relative in the
+             populations after 1000 steps, <= 1e-10 in the average Nusselt
+             number (the drop-in tolerance);
+f32 / f16s   reduced storage: errors against the FP64 oracle stay within the
+             bounds written in each test.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(pkg, ora, dim, nx, ny, nz=1, grid="erf", stretch=3.2, Ra=1e5, Pr=0.71, mode="fast", storage="f64"):
+    cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, mode=mode, storage=storage)
+    o = ora.Oracle(dim, nx, ny, nz, x=cav.mesh.x, y=cav.mesh.y, z=cav.mesh.z, dt=cav.mesh.dt,
+                   length_LB=cav.mesh.length_LB, Ra=Ra, Pr=Pr)
+    cav.initial()
+    return cav, o
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+FIELDS2 = ("rho", "u", "v", "T")
+FIELDS3 = ("rho", "u", "v", "w", "T")
+
+
+@pytest.mark.parametrize("case", [
+    dict(dim=2, nx=32, ny=32, grid="erf", stretch=3.2, steps=150),
+    dict(dim=2, nx=40, ny=24, grid="tanh", stretch=1.5, steps=120),
+    dict(dim=3, nx=14, ny=12, nz=10, grid="erf", stretch=3.2, steps=40),
+    dict(dim=3, nx=16, ny=16, nz=16, grid="tanh", stretch=1.5, steps=30),
+])
+def test_exact_mode_bit_identical(pkg, ora, case):
+    c = dict(case)
+    steps = c.pop("steps")
+    cav, o = pair(pkg, ora, mode="exact", **c)
+    cav.step(steps)
+    o.step(steps)
+    m = cav.macro()
+    for k in (FIELDS2 if c["dim"] == 2 else FIELDS3):
+        assert np.array_equal(m[k], o.field(k)), f"{k}: max diff {np.abs(m[k] - o.field(k)).max():.3e}"
+    f, g = cav.populations()
+    assert np.array_equal(f, o.pops("f"))
+    assert np.array_equal(g, o.pops("g"))
+    cav.close()
+
+
+@pytest.mark.parametrize("case", [
+    dict(dim=2, nx=48, ny=48, grid="tanh", stretch=1.5, Ra=1e4),
+    dict(dim=2, nx=33, ny=33, grid="erf", stretch=3.2, Ra=1e5),
+    dict(dim=3, nx=20, ny=20, nz=20, grid="tanh", stretch=1.5, Ra=1e5),
+])
+def test_fast_fp64_within_1e12_after_1000_steps(pkg, ora, case):
+    cav, o = pair(pkg, ora, mode="fast", **case)
+    cav.step(1000)
+    o.step(1000)
+    f, g = cav.populations()
+    assert rel_err(f, o.pops("f")) <= 1e-12
+    assert rel_err(g, o.pops("g")) <= 1e-12
+    nh, nc = cav.nusselt()
+    onh, onc = o.nusselt()
+    assert abs(nh - onh) <= 1e-10 * abs(onh)
+    assert abs(nc - onc) <= 1e-10 * abs(onc)
+    cav.close()
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_check_nusselt_sums_match_oracle(pkg, ora, mode):
+    cav, o = pair(pkg, ora, 2, 36, 36, grid="erf", Ra=1e5, mode=mode)
+    tol = 1e-13 if mode == "exact" else 1e-10
+    for _ in range(3):
+        cav.step(40)
+        o.step(40)
+        eu, et = cav.check()
+        ou, ot = o.check()
+        assert eu == pytest.approx(ou, rel=tol) and et == pytest.approx(ot, rel=tol)
+    for a, b in zip(cav.nusselt(), o.nusselt()):
+        assert a == pytest.approx(b, rel=tol)
+    for a, b in zip(cav.sums(), o.sums()):
+        assert a == pytest.approx(b, rel=tol)
+    assert cav.itc == 120
+    cav.close()
+
+
+def test_check_nusselt_sums_3d(pkg, ora):
+    cav, o = pair(pkg, ora, 3, 14, 14, 14, grid="tanh", stretch=1.5, Ra=1e5, mode="exact")
+    cav.step(25)
+    o.step(25)
+    for a, b in zip(cav.check(), o.check()):
+        assert a == pytest.approx(b, rel=1e-13)
+    for a, b in zip(cav.nusselt(), o.nusselt()):
+        assert a == pytest.approx(b, rel=1e-13)
+    for a, b in zip(cav.sums(), o.sums()):
+        assert a == pytest.approx(b, rel=1e-13)
+    cav.close()
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_checkpoint_restart_is_exact(pkg, ora, dim):
+    n = (30, 30, 1) if dim == 2 else (12, 12, 12)
+    a, _ = pair(pkg, ora, dim, *n, mode="exact")
+    b, _ = pair(pkg, ora, dim, *n, mode="exact")
+    a.step(37)
+    f, g = a.populations()
+    mac = a.macro()
+    a.step(23)
+    b.step(5)  # some other state, then restore the checkpoint
+    b.set_populations(f, g)
+    b.set_macro(**mac)
+    b.step(23)
+    ma, mb = a.macro(), b.macro()
+    for k in ma:
+        assert np.array_equal(ma[k], mb[k]), k
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("storage,tol_u,tol_T", [("f32", 2e-4, 1e-5), ("f16s", 5e-2, 5e-3)])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_reduced_precision_storage(pkg, ora, storage, tol_u, tol_T, dim):
+    n = (48, 48, 1) if dim == 2 else (16, 16, 16)
+    cav, o = pair(pkg, ora, dim, *n, grid="tanh", stretch=1.5, Ra=1e5, storage=storage)
+    cav.step(500)
+    o.step(500)
+    m = cav.macro()
+    umax = max(np.abs(o.field(k)).max() for k in ("u", "v"))
+    du = max(np.abs(m[k] - o.field(k)).max() for k in ("u", "v"))
+    dT = np.abs(m["T"] - o.field("T")).max()
+    print(f"{storage} {dim}D: |du|/umax = {du / umax:.3e}, |dT| = {dT:.3e}")
+    assert du / umax <= tol_u
+    assert dT <= tol_T
+    cav.close()
+
+
+def test_step_before_init_is_a_state_error(pkg):
+    cav = pkg.Cavity(2, 16, 16)
+    with pytest.raises(pkg.LBMError) as e:
+        cav.step(1)
+    assert e.value.status == -6
+    cav.initial()
+    cav.step(1)
+    cav.close()
+
+
+def test_init_equilibrium_rest_state(pkg, ora):
+    # BASELINE's rest initial state (rho = 1, u = 0, T = 0) through the
+    # equilibrium entry point, against the oracle's set_macro
+    cav = pkg.Cavity(2, 40, 40, grid="tanh", stretch=1.5, Ra=1e4, mode="exact")
+    o = ora.Oracle(2, 40, 40, x=cav.mesh.x, y=cav.mesh.y, dt=cav.mesh.dt, length_LB=cav.mesh.length_LB, Ra=1e4)
+    one, zero = np.ones(cav.shape), np.zeros(cav.shape)
+    rng = np.random.default_rng(7)
+    T = rng.uniform(-1e-4, 1e-4, cav.shape)
+    cav.init_equilibrium(one, zero, zero, None, T)
+    o.set_macro(one, zero, zero, None, T)
+    cav.step(60)
+    o.step(60)
+    m = cav.macro()
+    for k in FIELDS2:
+        assert np.array_equal(m[k], o.field(k)), k
+    cav.close()
+
+
+@pytest.mark.parametrize("dim,n,steps", [(3, 128, 3), (2, 2048, 2)])
+def test_full_size_against_oracle(pkg, ora, dim, n, steps):
+    # the benchmark sizes (128^3 D3Q19+D3Q7, 2048^2 D2Q9+D2Q5) for a few steps
+    ns = (n, n, n) if dim == 3 else (n, n, 1)
+    cav, o = pair(pkg, ora, dim, *ns, grid="tanh", stretch=1.5, Ra=1e5, mode="fast")
+    cav.step(steps)
+    o.step(steps)
+    m = cav.macro()
+    for k in (FIELDS2 if dim == 2 else FIELDS3):
+        ref = o.field(k)
+        assert np.abs(m[k] - ref).max() <= 1e-12 * max(np.abs(ref).max(), 1e-30) + 1e-300, k
+    cav.close()
+
+
+def test_runs_are_deterministic(pkg):
+    out = []
+    for _ in range(2):
+        cav = pkg.Cavity(3, 64, 64, 64, grid="tanh", stretch=1.5, Ra=1e5)
+        cav.initial()
+        cav.step(50)
+        out.append((cav.macro(), cav.check(), cav.nusselt()))
+        cav.close()
+    for k in out[0][0]:
+        assert np.array_equal(out[0][0][k], out[1][0][k])
+    assert out[0][1] == out[1][1] and out[0][2] == out[1][2]

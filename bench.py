@@ -232,6 +232,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "march"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -249,7 +250,7 @@ def main():
     wl = WORKLOADS[args.workload]
     dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
     cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, storage=args.storage,
-                     mode=args.mode, device=local)
+                     mode=args.mode, device=local, kernel=args.kernel)
     shape = cav.shape
     # pinned host fields for the end-to-end leg
     pin = {k: torch.zeros(shape, dtype=torch.float64, pin_memory=True) for k in ("rho", "u", "v", "w", "T")}
@@ -350,7 +351,8 @@ def main():
             "data": "synthetic", "config": config_of(args, wl, args.inner),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "bytes_per_lup": bpl, "kernel": "k_step3d" if dim == 3 else "k_step2d",
+                         "bytes_per_lup": bpl,
+                         "kernel": ("k_march" if cav.kernel == "march" else "k_step") + ("3d" if dim == 3 else "2d"),
                          "ms_per_launch": ms_launch, "frac_of_8TBps": achieved / 8000.0},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         }

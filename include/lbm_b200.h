@@ -54,6 +54,10 @@ extern "C" {
 #define LBM_MODE_EXACT  1  /* the reference's operation order, no contraction:
                               bit-identical to the CPU restatement */
 
+/* options for lbm_set_option / lbm_get_option */
+#define LBM_OPT_KERNEL   1  /* step kernel: 0 automatic, 1 direct-load, 2 TMA march */
+#define LBM_OPT_NBLOCKS  2  /* persistent blocks of the march kernel (0 = one wave) */
+
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */
 #define LBM_GRID_TANH    1  /* 0.5*(1 + tanh(b*(2*xi-1))/tanh(b)), b = stretch */
@@ -161,7 +165,14 @@ int lbm_get_populations(lbm_handle *h, double *f, double *g);
  * restore the exact carried state of a checkpoint. */
 int lbm_set_populations(lbm_handle *h, const double *f, const double *g);
 
-/* Wait for all work of the handle. */
+/* Tuning options of a handle (no counterpart in the reference): see
+ * LBM_OPT_*.  lbm_get_option reports the value in effect (the kernel the
+ * automatic choice picked, the block count used). */
+int lbm_set_option(lbm_handle *h, int32_t option, int64_t value);
+int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *value);
+
+/* Wait for all work of the handle; reports LBM_ERR_TIMEOUT if a kernel's
+ * bounded wait gave up since the last synchronisation. */
 int lbm_synchronize(lbm_handle *h);
 
 /* The handle's CUDA stream as an opaque pointer (cudaStream_t). */

@@ -220,6 +220,12 @@ struct lbm_handle {
     void *staging = nullptr;     // population planes for stream-only output
     double *aos = nullptr;       // Fortran-layout staging
     cudaStream_t stream = nullptr;
+    TmapSet tmaps[2];            // TMA descriptors of pop[0] and pop[1]
+    bool march_ok = false;       // tile shape and descriptors usable
+    int kernel_opt = 0;          // LBM_OPT_KERNEL as set
+    int use_march = 0;           // resolved choice
+    int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
+    int nblocks = 0;             // resolved persistent grid
     int cur = 0;                 // buffer holding the newest populations
     int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
     int64_t itc = 0;
@@ -251,7 +257,7 @@ static void free_all(lbm_handle *h)
                     h->bufs.v, h->bufs.w, h->bufs.T, h->bufs.up, h->bufs.vp, h->bufs.wp, h->bufs.Tp,
                     h->bufs.partials, h->bufs.scal, h->d_wgt[0], h->d_wgt[1], h->d_wgt[2], h->d_coord[0],
                     h->d_coord[1], h->d_coord[2], h->d_cellw[0], h->d_cellw[1], h->d_cellw[2], h->staging,
-                    h->aos};
+                    h->aos, h->bufs.err};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -264,6 +270,101 @@ extern "C" int lbm_destroy(lbm_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_all(h);
     delete h;
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// TMA descriptors for the march kernels
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Describe a population buffer as a (x, y, [z,] plane) tensor; one descriptor
+// per box class of the march kernel.  Returns false if TMA cannot be used.
+static bool encode_maps(lbm_handle *h)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    const Geo &g = h->geo;
+    const MarchShape ms = march_shape(g.dim, h->p.storage);
+    const CUtensorMapDataType dtype = h->p.storage == LBM_STORE_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                      : h->p.storage == LBM_STORE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const cuuint64_t es = h->esize;
+    const int nplanes = h->Q + h->QT;
+    for (int buf = 0; buf < 2; ++buf) {
+        for (int c = 0; c < 4; ++c) {
+            CUtensorMap *m = &h->tmaps[buf].m[c];
+            CUresult r;
+            if (g.dim == 3) {
+                const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nplanes};
+                const cuuint64_t strides[3] = {(cuuint64_t)g.pitch * es, (cuuint64_t)g.slab * es,
+                                               (cuuint64_t)g.plane * es};
+                const cuuint32_t box[4] = {(cuuint32_t)ms.bx[c], (cuuint32_t)ms.by[c], 1, 1};
+                const cuuint32_t estr[4] = {1, 1, 1, 1};
+                r = enc(m, dtype, 4, h->bufs.pop[buf], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            } else {
+                const int cc = c & 1;
+                const cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
+                const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * es, (cuuint64_t)g.plane * es};
+                const cuuint32_t box[3] = {(cuuint32_t)ms.bx[cc], 1, 1};
+                const cuuint32_t estr[3] = {1, 1, 1};
+                r = enc(m, dtype, 3, h->bufs.pop[buf], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            }
+            if (r != CUDA_SUCCESS) return false;
+        }
+    }
+    return true;
+}
+
+// The march kernel handles every size except, in 3D, a last tile row holding
+// a single y-row (its one-sided stencil would reach two rows below the box).
+static bool march_supported(const lbm_handle *h)
+{
+    if (!h->march_ok) return false;
+    const MarchShape ms = march_shape(h->geo.dim, h->p.storage);
+    if (h->geo.dim == 3 && h->geo.ny % ms.TY == 1) return false;
+    return true;
+}
+
+static int resolve_path(lbm_handle *h)
+{
+    const bool ok = march_supported(h);
+    if (h->kernel_opt == 2 && !ok)
+        return fail(LBM_ERR_UNSUPPORTED, "march kernel not available for this shape / device");
+    h->use_march = h->kernel_opt == 2 || (h->kernel_opt == 0 && ok && h->geo.nnode >= (1 << 15));
+    if (h->use_march) {
+        const int bps = h->p.mode == LBM_MODE_EXACT ? exact::march_blocks_per_sm(h->geo, h->p.storage)
+                                                   : fast::march_blocks_per_sm(h->geo, h->p.storage);
+        if (bps <= 0) {
+            if (h->kernel_opt == 2) return fail(LBM_ERR_UNSUPPORTED, "march kernel cannot be resident");
+            h->use_march = 0;
+            return LBM_OK;
+        }
+        int sms = 0;
+        CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        h->nblocks = h->nblocks_opt > 0 ? h->nblocks_opt : bps * sms;
+    }
     return LBM_OK;
 }
 
@@ -311,7 +412,8 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
     memset(&g, 0, sizeof g);
     g.dim = p->dim;
     g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
-    g.pitch = g.nx;
+    // rows padded to 16 bytes for every storage type (TMA stride rule)
+    g.pitch = (g.nx + 7) / 8 * 8;
     g.slab = g.pitch * g.ny;
     const int64_t cells = g.slab * g.nz;
     g.plane = (cells + 127) / 128 * 128;
@@ -355,9 +457,14 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
         (st = dalloc(h, &b.wp, mb)) || (st = dalloc(h, &b.Tp, mb)) ||
         (st = dalloc(h, &b.partials, 592 * 4 * 8)) || (st = dalloc(h, &b.scal, 16 * 8)))
         return bail(st);
+    if ((st = dalloc(h, &b.err, 16))) return bail(st);
     if (cudaMemset(b.F[0], 0, fb) != cudaSuccess || cudaMemset(b.F[1], 0, fb) != cudaSuccess ||
-        cudaMemset(b.w, 0, mb) != cudaSuccess || cudaMemset(b.wp, 0, mb) != cudaSuccess)
+        cudaMemset(b.w, 0, mb) != cudaSuccess || cudaMemset(b.wp, 0, mb) != cudaSuccess ||
+        cudaMemset(b.err, 0, 16) != cudaSuccess || cudaMemset(b.pop[0], 0, popb) != cudaSuccess ||
+        cudaMemset(b.pop[1], 0, popb) != cudaSuccess)
         return bail(fail(LBM_ERR_CUDA, "memset failed"));
+    h->march_ok = encode_maps(h);
+    if ((st = resolve_path(h))) return bail(st);
     h->phase = 0;
     *out = h;
     return LBM_OK;
@@ -464,8 +571,16 @@ extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
     for (int s = 0; s < nsteps; ++s) {
         const int nxt = 1 - h->cur;
         const int wm = (s == nsteps - 1);
-        CU(ex ? exact::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm, h->stream)
-              : fast::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm, h->stream));
+        if (h->use_march)
+            CU(ex ? exact::march(h->geo, h->p.storage, h->tmaps[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
+                                 h->nblocks, h->stream)
+                  : fast::march(h->geo, h->p.storage, h->tmaps[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
+                                h->nblocks, h->stream));
+        else
+            CU(ex ? exact::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
+                                h->stream)
+                  : fast::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
+                               h->stream));
         h->cur = nxt;
     }
     h->itc += nsteps;
@@ -479,11 +594,24 @@ extern "C" int lbm_itc(const lbm_handle *h, int64_t *itc)
     return LBM_OK;
 }
 
+// Synchronise the handle's stream and report a kernel's bounded wait that gave up.
+static int sync_and_check(lbm_handle *h)
+{
+    int flag = 0;
+    CU(cudaMemcpyAsync(&flag, h->bufs.err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    if (flag) {
+        CU(cudaMemsetAsync(h->bufs.err, 0, sizeof(int), h->stream));
+        CU(cudaStreamSynchronize(h->stream));
+        return fail(LBM_ERR_TIMEOUT, "a step kernel's bounded wait for its TMA copies gave up (code %d)", flag);
+    }
+    return LBM_OK;
+}
+
 static int read_scal(lbm_handle *h, int first, int count, double *out)
 {
     CU(cudaMemcpyAsync(out, h->bufs.scal + first, sizeof(double) * count, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    return LBM_OK;
+    return sync_and_check(h);
 }
 
 extern "C" int lbm_check(lbm_handle *h, double *errU, double *errT)
@@ -540,8 +668,7 @@ extern "C" int lbm_get_macro(lbm_handle *h, double *rho, double *u, double *v, d
     if (v) CU(cudaMemcpyAsync(v, h->bufs.v, mb, cudaMemcpyDeviceToHost, h->stream));
     if (w && h->p.dim == 3) CU(cudaMemcpyAsync(w, h->bufs.w, mb, cudaMemcpyDeviceToHost, h->stream));
     if (T) CU(cudaMemcpyAsync(T, h->bufs.T, mb, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    return LBM_OK;
+    return sync_and_check(h);
 }
 
 extern "C" int lbm_set_macro(lbm_handle *h, const double *rho, const double *u, const double *v, const double *w,
@@ -622,8 +749,42 @@ extern "C" int lbm_set_populations(lbm_handle *h, const double *f, const double 
 extern "C" int lbm_synchronize(lbm_handle *h)
 {
     CHECK_H(h);
-    CU(cudaStreamSynchronize(h->stream));
-    return LBM_OK;
+    return sync_and_check(h);
+}
+
+extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
+{
+    CHECK_H(h);
+    switch (option) {
+    case LBM_OPT_KERNEL: {
+        if (value < 0 || value > 2) return fail(LBM_ERR_PARAM, "kernel option must be 0, 1 or 2");
+        const int old = h->kernel_opt;
+        h->kernel_opt = (int)value;
+        int st = resolve_path(h);
+        if (st) {
+            h->kernel_opt = old;
+            resolve_path(h);
+            return st;
+        }
+        return LBM_OK;
+    }
+    case LBM_OPT_NBLOCKS:
+        if (value < 0 || value > (1 << 20)) return fail(LBM_ERR_PARAM, "nblocks out of range");
+        h->nblocks_opt = (int)value;
+        return resolve_path(h);
+    default:
+        return fail(LBM_ERR_PARAM, "unknown option %d", option);
+    }
+}
+
+extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *value)
+{
+    if (!h || !value) return fail(LBM_ERR_PARAM, "NULL argument");
+    switch (option) {
+    case LBM_OPT_KERNEL: *value = h->use_march ? 2 : 1; return LBM_OK;
+    case LBM_OPT_NBLOCKS: *value = h->use_march ? h->nblocks : 0; return LBM_OK;
+    default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
+    }
 }
 
 extern "C" int lbm_stream(const lbm_handle *h, void **stream)

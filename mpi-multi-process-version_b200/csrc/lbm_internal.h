@@ -1,6 +1,7 @@
 // Internal interface between the C ABI (lbm_capi.cu) and the kernels
 // (lbm_kernels.cu, compiled once per arithmetic mode).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -27,6 +28,18 @@ struct Bufs {
     double *up, *vp, *wp, *Tp;     // fields at the previous check
     double *partials;      // reduction partials
     double *scal;          // reduction results
+    int *err;              // device error flag (bounded waits that gave up)
+};
+
+// TMA descriptors of one population buffer, one per box class
+struct alignas(64) TmapSet {
+    CUtensorMap m[4];
+};
+
+// shape of the march kernels' tiles for a lattice and storage (host side)
+struct MarchShape {
+    int TX, TY, HX, threads, smem;
+    int bx[4], by[4];
 };
 
 enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
@@ -46,6 +59,12 @@ enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
     /* stream + walls + macro only: pre-collision populations into pop_out, macro fields */  \
     cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in,    \
                             void *pop_out, const Bufs &b, cudaStream_t s);                    \
+    /* fused step through the TMA-fed persistent march kernel */                              \
+    cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in,          \
+                      void *pop_out, void *F_out, const Bufs &b, int write_macro, int nblocks,\
+                      cudaStream_t s);                                                        \
+    /* resident blocks per SM of the march kernel (0 if it cannot launch) */                  \
+    int march_blocks_per_sm(const Geo &g, int store);                                         \
     }
 
 LBM_DECLARE_LAUNCHERS(fast)
@@ -65,5 +84,8 @@ cudaError_t macro_from_pops(const Geo &g, int store, const void *pop, const Bufs
                             cudaStream_t s);
 
 extern int64_t g_launches;  // kernels launched by this library
+
+// tile shape of the march kernels (identical in both arithmetic modes)
+MarchShape march_shape(int dim, int store);
 
 }  // namespace lbm

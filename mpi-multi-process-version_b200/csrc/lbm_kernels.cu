@@ -23,6 +23,7 @@
 // Populations live in structure-of-arrays planes: plane q holds population q of
 // every node, rows of `pitch` elements, z-planes of `slab` elements.  Planes
 // 0..Q-1 are f, Q..Q+QT-1 are g.
+#include <cuda.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
 
@@ -683,6 +684,8 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
     for (int q = 0; q < QT; ++q) out[(Q + q) * P + id] = tostore<S, C>(gp[q] - shift(Q + q));
 }
 
+#include "lbm_march.cuh"
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -778,5 +781,113 @@ cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out, 
 #undef CALL
 }
 
+template <int ST>
+static cudaError_t prepare_march(const Geo &g)
+{
+    static bool done3 = false, done2 = false;
+    if (g.dim == 3 && !done3) {
+        cudaError_t e = cudaFuncSetAttribute(k_march3d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L3<ST>::smem());
+        if (e != cudaSuccess) return e;
+        done3 = true;
+    }
+    if (g.dim == 2 && !done2) {
+        cudaError_t e = cudaFuncSetAttribute(k_march2d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L2<ST>::smem());
+        if (e != cudaSuccess) return e;
+        done2 = true;
+    }
+    return cudaSuccess;
+}
+
+template <int ST>
+static int mbps(const Geo &g)
+{
+    if (prepare_march<ST>(g) != cudaSuccess) return 0;
+    int n = 0;
+    cudaError_t e = g.dim == 3
+                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d<ST>, L3<ST>::NT, L3<ST>::smem())
+                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2<ST>::NT, L2<ST>::smem());
+    return e == cudaSuccess ? n : 0;
+}
+
+int march_blocks_per_sm(const Geo &g, int store)
+{
+#define CALL(ST) mbps<ST>(g)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+template <int ST>
+static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
+                                const Bufs &b, int wm, int nblocks, cudaStream_t s)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    cudaError_t e = prepare_march<ST>(g);
+    if (e != cudaSuccess) return e;
+    if (g.dim == 3) {
+        using L = L3<ST>;
+        const int64_t ntiles = (int64_t)((g.nx + L::TX - 1) / L::TX) * ((g.ny + L::TY - 1) / L::TY);
+        const int64_t total = ntiles * g.nz;
+        const int nb = int(nblocks < total ? nblocks : total);
+        k_march3d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
+    } else {
+        using L = L2<ST>;
+        const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
+        const int nb = int(nblocks < total ? nblocks : total);
+        k_march2d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
+    }
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in, void *pop_out, void *F_out,
+                  const Bufs &b, int write_macro, int nblocks, cudaStream_t s)
+{
+#define CALL(ST) launch_march<ST>(g, src, F_in, pop_out, F_out, b, write_macro, nblocks, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
 }  // namespace LBM_NS
+
+#if !LBM_EXACT
+// tile shapes of the march kernels, for the host's tensor-map encoding
+MarchShape march_shape(int dim, int store)
+{
+    MarchShape m{};
+    auto fill = [&](auto layout, int dims) {
+        using L = decltype(layout);
+        m.TX = L::TX;
+        m.TY = dims == 3 ? fast::L3<kF64>::TY : 1;
+        m.HX = L::HX;
+        m.threads = L::NT;
+        m.smem = L::smem();
+    };
+    if (dim == 3) {
+        switch (store) {
+        case kF64: fill(fast::L3<kF64>{}, 3); break;
+        case kF32: fill(fast::L3<kF32>{}, 3); break;
+        default: fill(fast::L3<kF16S>{}, 3); break;
+        }
+        for (int c = 0; c < 4; ++c) {
+            m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);
+            m.by[c] = m.TY + ((c & 2) ? 2 : 0);
+        }
+    } else {
+        switch (store) {
+        case kF64: fill(fast::L2<kF64>{}, 2); break;
+        case kF32: fill(fast::L2<kF32>{}, 2); break;
+        default: fill(fast::L2<kF16S>{}, 2); break;
+        }
+        for (int c = 0; c < 4; ++c) {
+            m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);
+            m.by[c] = 1;
+        }
+    }
+    return m;
+}
+#endif
+
 }  // namespace lbm

@@ -1,0 +1,668 @@
+// TMA-fed persistent "march" kernels for the fused time step.
+//
+// Included by lbm_kernels.cu inside namespace lbm::LBM_NS, so the arithmetic
+// (ip, collide2d / collide3d, DV) is the same code as the direct-load kernels
+// and is compiled in both the fast and the exact mode.
+//
+// Scheme (3D; 2D is the same one dimension down):
+//   * the domain is cut into cross-section tiles of TX x TY nodes (x, y); a
+//     work item is a tile at one z-slice, and each persistent CTA takes a
+//     contiguous, equal share of the (tile-major, z-minor) work items, so it
+//     marches along z through at most a few tile columns;
+//   * for every slice the CTA fetches one TMA box per population plane into
+//     shared memory: a box covers the tile plus the in-plane halo the plane's
+//     interpolation stencil needs (x +-HX columns, y +-1 rows);
+//   * planes whose stencil reaches along z (D3Q19 5,6,11-18; D3Q7 5,6) live in
+//     a 4-slot ring indexed by slice, fetched two slices ahead, so each slice
+//     is read once per tile column and serves the steps k-1, k, k+1 (and the
+//     one-sided stencils at the walls); the other planes use a 2-slot ring;
+//   * one thread issues the copies (cp.async.bulk.tensor with an mbarrier
+//     transaction count), every thread waits on the slot barriers it needs,
+//     computes its node from shared memory and stores the new post-collision
+//     populations straight to global memory; a __syncthreads ends each step
+//     and frees the slots the next copies reuse;
+//   * every wait is bounded (kWaitCycles): on timeout the kernel records an
+//     error code in *err, stops issuing, lets outstanding copies drain (also
+//     bounded) and returns; the host reports LBM_ERR_TIMEOUT.
+// No copy uses cluster multicast; every copy reads this GPU's own buffers.
+
+static constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ uint32_t mbar_test(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok;
+}
+
+// bounded wait for the phase of parity `parity`; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity)
+{
+    if (mbar_test(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test(b, parity))
+        if (clock64() - t0 > kWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load4(void *dst, const CUtensorMap *m, uint64_t *bar, int c0, int c1, int c2,
+                                          int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(saddr(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, uint64_t *bar, int c0, int c1, int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(saddr(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(saddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// ring bookkeeping shared by the 2D and 3D kernels
+// ---------------------------------------------------------------------------
+// Slices needed at step k along a marching axis of n nodes: k-1..k+1, plus the
+// far point of the one-sided stencils at the walls (k+2 at k = 0, k-2 at
+// k = n-1): off_a / off_b give exactly these.
+__device__ __forceinline__ int need_lo(int k, int n) { return k == n - 1 ? k - 2 : (k == 0 ? 0 : k - 1); }
+__device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k == n - 1 ? k : k + 1); }
+
+// ---------------------------------------------------------------------------
+// 3D layout
+// ---------------------------------------------------------------------------
+// box classes: 0 tile only, 1 +-HX columns, 2 +-1 rows, 3 both
+template <int ST>
+struct L3 {
+    using S = typename Tr<ST>::S;
+    static constexpr int ES = sizeof(S);
+    static constexpr int TX = 32, TY = 8, NT = TX * TY;
+    static constexpr int HX = 16 / ES;
+    __host__ __device__ static constexpr int bx(int c) { return TX + ((c & 1) ? 2 * HX : 0); }
+    __host__ __device__ static constexpr int by(int c) { return TY + ((c & 2) ? 2 : 0); }
+    __host__ __device__ static constexpr int bytes(int c) { return bx(c) * by(c) * ES; }
+    __host__ __device__ static constexpr int padded(int c) { return (bytes(c) + 127) / 128 * 128; }
+    // z-ring planes: 5 6 | 11 12 13 14 | 15 16 17 18 | 24 25
+    __host__ __device__ static constexpr int zq(int zi)
+    {
+        return zi < 2 ? 5 + zi : (zi < 10 ? 9 + zi : 14 + zi);
+    }
+    __host__ __device__ static constexpr int zc(int zi) { return zi < 2 ? 0 : (zi < 6 ? 1 : (zi < 10 ? 2 : 0)); }
+    __host__ __device__ static constexpr int zoff(int zi)
+    {
+        int o = 0;
+        for (int a = 0; a < zi; ++a) o += padded(zc(a));
+        return o;
+    }
+    __host__ __device__ static constexpr int zslot() { return zoff(12); }
+    __host__ __device__ static constexpr int ztx()
+    {
+        int b = 0;
+        for (int a = 0; a < 12; ++a) b += bytes(zc(a));
+        return b;
+    }
+    // n-ring planes: 0 | 1 2 | 3 4 | 7 8 9 10 | 19 | 20 21 | 22 23
+    __host__ __device__ static constexpr int nq(int ni)
+    {
+        return ni < 5 ? ni : (ni < 9 ? ni + 2 : ni + 10);
+    }
+    __host__ __device__ static constexpr int nc(int ni)
+    {
+        return ni == 0 ? 0 : (ni < 3 ? 1 : (ni < 5 ? 2 : (ni < 9 ? 3 : (ni == 9 ? 0 : (ni < 12 ? 1 : 2)))));
+    }
+    __host__ __device__ static constexpr int noff(int ni)
+    {
+        int o = 0;
+        for (int a = 0; a < ni; ++a) o += padded(nc(a));
+        return o;
+    }
+    __host__ __device__ static constexpr int nslot() { return noff(14); }
+    __host__ __device__ static constexpr int ntx()
+    {
+        int b = 0;
+        for (int a = 0; a < 14; ++a) b += bytes(nc(a));
+        return b;
+    }
+    // ring slots, 6 barriers and the abort flag, and slack for 128-byte alignment
+    __host__ __device__ static constexpr int smem() { return 4 * zslot() + 2 * nslot() + 64 + 128; }
+};
+
+// ---------------------------------------------------------------------------
+// 3D march kernel
+// ---------------------------------------------------------------------------
+template <int ST>
+__global__ void __launch_bounds__(256, 1)
+k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
+          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+          int write_macro, int64_t total, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    using L = L3<ST>;
+    constexpr int TX = L::TX, TY = L::TY, HX = L::HX;
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
+    uint64_t *zbar = (uint64_t *)(sm + 4 * L::zslot() + 2 * L::nslot());
+    uint64_t *nbar = zbar + 4;
+    volatile int &s_abort = *(volatile int *)(nbar + 2);
+
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const int nz = G.nz;
+    const int ntx = (G.nx + TX - 1) / TX;
+    if (tid == 0) {
+        for (int s = 0; s < 4; ++s) mbar_init(&zbar[s], 1);
+        for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
+        fence_barrier_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    uint32_t znext = 0, nnext = 0;  // per-slot parity of the next copy
+    int i0 = 0, j0 = 0;
+
+    auto issue_z = [&](int s) {
+        const int slot = s & 3;
+        if (tid == 0) {
+            uint64_t *bar = &zbar[slot];
+            mbar_arrive_tx(bar, L::ztx());
+            unsigned char *base = sm + slot * L::zslot();
+#pragma unroll
+            for (int zi = 0; zi < 12; ++zi) {
+                const int c = L::zc(zi);
+                tma_load4(base + L::zoff(zi), &maps.m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
+                          s, L::zq(zi));
+            }
+        }
+        znext ^= 1u << slot;
+    };
+    auto issue_n = [&](int s) {
+        const int slot = s & 1;
+        if (tid == 0) {
+            uint64_t *bar = &nbar[slot];
+            mbar_arrive_tx(bar, L::ntx());
+            unsigned char *base = sm + 4 * L::zslot() + slot * L::nslot();
+#pragma unroll
+            for (int ni = 0; ni < 14; ++ni) {
+                const int c = L::nc(ni);
+                tma_load4(base + L::noff(ni), &maps.m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
+                          s, L::nq(ni));
+            }
+        }
+        nnext ^= 1u << slot;
+    };
+    auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u); };
+    auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
+
+    const int64_t G_ = gridDim.x;
+    const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
+    const int64_t P = G.plane;
+    bool aborted = false;
+
+    for (int64_t u = ubeg; u < uend && !aborted;) {
+        const int64_t t = u / nz;
+        const int ka = int(u % nz);
+        const int kb = int(ka + ((uend - u) < (nz - ka) ? (uend - u) : (nz - ka)));
+        i0 = int(t % ntx) * TX;
+        j0 = int(t / ntx) * TY;
+        // the segment's z-slices: the first step's needs, then one slice per step
+        const int pre_lo = need_lo(ka, nz), pre_hi = need_hi(ka, nz);
+        const int seg_hi = need_hi(kb - 1, nz) > pre_hi ? need_hi(kb - 1, nz) : pre_hi;
+        for (int s = pre_lo; s <= pre_hi; ++s) issue_z(s);
+        issue_n(ka);
+        int zissued = pre_hi;
+
+        const int i = i0 + tx, j = j0 + ty;
+        const bool active = i < G.nx && j < G.ny;
+        C xp[3], xm[3], yp[3], ym[3];
+        int xa = 0, xb = 0, ya = 0, yb = 0;
+        if (active) {
+            load_w(G.wgt[0], i, xp, xm);
+            load_w(G.wgt[1], j, yp, ym);
+            xa = off_a(i, G.nx); xb = off_b(i, G.nx);
+            ya = off_a(j, G.ny); yb = off_b(j, G.ny);
+        }
+
+        for (int k = ka; k < kb; ++k) {
+            // prefetch: z-slice k+2 (its slot held k-2, done last step), plane slice k+1
+            if (zissued < seg_hi && k + 2 <= seg_hi && k + 2 > zissued) {
+                issue_z(k + 2);
+                zissued = k + 2;
+            }
+            if (k + 1 < kb) issue_n(k + 1);
+
+            const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
+            C Fz0 = C(0);
+            if (active) Fz0 = Fin[id];
+            bool ok = true;
+            for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
+            ok = ok && wait_n(k);
+            if (!ok) {
+                atomicExch(err, 1);
+                s_abort = 1;
+            }
+            if (active && ok) {
+                const int ka_ = k + off_a(k, nz), kb_ = k + off_b(k, nz);
+                C zp[3], zm[3];
+                load_w(G.wgt[2], k, zp, zm);
+                auto SV = [&](const unsigned char *box, int idx, int q) -> C {
+                    C val = tocomp(((const S *)box)[idx]);
+                    if (Tr<ST>::kShift) val += (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+                    return val;
+                };
+                auto ZB = [&](int zi, int s) -> const unsigned char * { return sm + (s & 3) * L::zslot() + L::zoff(zi); };
+                auto NB = [&](int ni) -> const unsigned char * {
+                    return sm + 4 * L::zslot() + (k & 1) * L::nslot() + L::noff(ni);
+                };
+                // element index of the thread's node in a box of class c, shifted by (dx, dy)
+                auto ix = [&](int c, int dx, int dy) -> int {
+                    return (ty + ((c & 2) ? 1 : 0) + dy) * L::bx(c) + tx + ((c & 1) ? HX : 0) + dx;
+                };
+                C f[19], gg[7];
+                // in-plane planes (slice k)
+                f[0] = SV(NB(0), ix(0, 0, 0), 0);
+                f[1] = ip(xp, SV(NB(1), ix(1, xa, 0), 1), SV(NB(1), ix(1, 0, 0), 1), SV(NB(1), ix(1, xb, 0), 1));
+                f[2] = ip(xm, SV(NB(2), ix(1, xa, 0), 2), SV(NB(2), ix(1, 0, 0), 2), SV(NB(2), ix(1, xb, 0), 2));
+                f[3] = ip(yp, SV(NB(3), ix(2, 0, ya), 3), SV(NB(3), ix(2, 0, 0), 3), SV(NB(3), ix(2, 0, yb), 3));
+                f[4] = ip(ym, SV(NB(4), ix(2, 0, ya), 4), SV(NB(4), ix(2, 0, 0), 4), SV(NB(4), ix(2, 0, yb), 4));
+                // xoy (3M:807-824): y-interpolation on three x-columns, then x
+                auto XY = [&](int ni, int q, const C *wx, const C *wy) -> C {
+                    const unsigned char *b = NB(ni);
+                    auto Y = [&](int dx) -> C {
+                        return ip(wy, SV(b, ix(3, dx, ya), q), SV(b, ix(3, dx, 0), q), SV(b, ix(3, dx, yb), q));
+                    };
+                    return ip(wx, Y(xa), Y(0), Y(xb));
+                };
+                f[7] = XY(5, 7, xp, yp);
+                f[8] = XY(6, 8, xm, yp);
+                f[9] = XY(7, 9, xp, ym);
+                f[10] = XY(8, 10, xm, ym);
+                gg[0] = SV(NB(9), ix(0, 0, 0), 19);
+                gg[1] = ip(xp, SV(NB(10), ix(1, xa, 0), 20), SV(NB(10), ix(1, 0, 0), 20), SV(NB(10), ix(1, xb, 0), 20));
+                gg[2] = ip(xm, SV(NB(11), ix(1, xa, 0), 21), SV(NB(11), ix(1, 0, 0), 21), SV(NB(11), ix(1, xb, 0), 21));
+                gg[3] = ip(yp, SV(NB(12), ix(2, 0, ya), 22), SV(NB(12), ix(2, 0, 0), 22), SV(NB(12), ix(2, 0, yb), 22));
+                gg[4] = ip(ym, SV(NB(13), ix(2, 0, ya), 23), SV(NB(13), ix(2, 0, 0), 23), SV(NB(13), ix(2, 0, yb), 23));
+                // z-reaching planes (slices ka_, k, kb_)
+                auto Zc = [&](int zi, int q, const C *wz, int c, int dx, int dy) -> C {
+                    const int e = ix(c, dx, dy);
+                    return ip(wz, SV(ZB(zi, ka_), e, q), SV(ZB(zi, k), e, q), SV(ZB(zi, kb_), e, q));
+                };
+                f[5] = Zc(0, 5, zp, 0, 0, 0);
+                f[6] = Zc(1, 6, zm, 0, 0, 0);
+                // xoz (3M:787-804): z-interpolation on three x-columns, then x
+                f[11] = ip(xp, Zc(2, 11, zp, 1, xa, 0), Zc(2, 11, zp, 1, 0, 0), Zc(2, 11, zp, 1, xb, 0));
+                f[12] = ip(xm, Zc(3, 12, zp, 1, xa, 0), Zc(3, 12, zp, 1, 0, 0), Zc(3, 12, zp, 1, xb, 0));
+                f[13] = ip(xp, Zc(4, 13, zm, 1, xa, 0), Zc(4, 13, zm, 1, 0, 0), Zc(4, 13, zm, 1, xb, 0));
+                f[14] = ip(xm, Zc(5, 14, zm, 1, xa, 0), Zc(5, 14, zm, 1, 0, 0), Zc(5, 14, zm, 1, xb, 0));
+                // yoz (3M:767-784): z-interpolation on three y-rows, then y
+                f[15] = ip(yp, Zc(6, 15, zp, 2, 0, ya), Zc(6, 15, zp, 2, 0, 0), Zc(6, 15, zp, 2, 0, yb));
+                f[16] = ip(ym, Zc(7, 16, zp, 2, 0, ya), Zc(7, 16, zp, 2, 0, 0), Zc(7, 16, zp, 2, 0, yb));
+                f[17] = ip(yp, Zc(8, 17, zm, 2, 0, ya), Zc(8, 17, zm, 2, 0, 0), Zc(8, 17, zm, 2, 0, yb));
+                f[18] = ip(ym, Zc(9, 18, zm, 2, 0, ya), Zc(9, 18, zm, 2, 0, 0), Zc(9, 18, zm, 2, 0, yb));
+                gg[5] = Zc(10, 24, zp, 0, 0, 0);
+                gg[6] = Zc(11, 25, zm, 0, 0, 0);
+
+                // walls: bounceback_u / bounceback_T (3B:1053-1197), centre values of slice k
+                auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0, 0), q); };
+                auto CZ = [&](int zi, int q) -> C { return SV(ZB(zi, k), ix(L::zc(zi), 0, 0), q); };
+                const C two_wT = C(2.0) * (C(1.0) / C(12.0));
+                if (j == 0) {
+                    f[3] = CN(4, 4); f[7] = CN(8, 10); f[8] = CN(7, 9); f[15] = CZ(9, 18); f[17] = CZ(7, 16);
+                    gg[3] = -CN(13, 23) + two_wT * C(G.Thot);
+                }
+                if (j == G.ny - 1) {
+                    f[4] = CN(3, 3); f[9] = CN(6, 8); f[10] = CN(5, 7); f[16] = CZ(8, 17); f[18] = CZ(6, 15);
+                    gg[4] = -CN(12, 22) + two_wT * C(G.Tcold);
+                }
+                if (i == 0) {
+                    f[1] = CN(2, 2); f[9] = CN(6, 8); f[7] = CN(8, 10); f[13] = CZ(3, 12); f[11] = CZ(5, 14);
+                    gg[1] = CN(11, 21);
+                }
+                if (i == G.nx - 1) {
+                    f[2] = CN(1, 1); f[8] = CN(7, 9); f[10] = CN(5, 7); f[12] = CZ(4, 13); f[14] = CZ(2, 11);
+                    gg[2] = CN(10, 20);
+                }
+                if (k == 0) {
+                    f[5] = CZ(1, 6); f[11] = CZ(5, 14); f[12] = CZ(4, 13); f[15] = CZ(9, 18); f[16] = CZ(8, 17);
+                    gg[5] = CZ(11, 25);
+                }
+                if (k == nz - 1) {
+                    f[6] = CZ(0, 5); f[13] = CZ(3, 12); f[14] = CZ(2, 11); f[17] = CZ(7, 16); f[18] = CZ(6, 15);
+                    gg[6] = CZ(10, 24);
+                }
+
+                // macro_u / macro_t (3M:988-1025)
+                const C dt = C(G.dt);
+                const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
+#if LBM_EXACT
+                const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
+                const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
+                const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)/rho;
+#else
+                const C rinv = C(1.0) / rho;
+                const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])*rinv;
+                const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
+                const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
+#endif
+                const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+                if (write_macro) {
+                    const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
+                    B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
+                    B.w[mid] = double(w); B.T[mid] = double(T);
+                }
+                C fp[19], gp[7], Fz;
+                collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+                Fout[id] = Fz;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    C val = fp[q];
+                    if (Tr<ST>::kShift) val -= C(wU3(q));
+                    dst[q * P + id] = tostore<S, C>(val);
+                }
+#pragma unroll
+                for (int q = 0; q < 7; ++q) {
+                    C val = gp[q];
+                    if (Tr<ST>::kShift) val -= C(wT3(q)) * C(G.T0);
+                    dst[(19 + q) * P + id] = tostore<S, C>(val);
+                }
+            }
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
+        }
+        u += kb - ka;
+    }
+    if (aborted && tid == 0) {
+        // let copies still in flight land before the CTA's shared memory is released
+        for (int s = 0; s < 4; ++s) mbar_wait(&zbar[s], ((znext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2D layout: a tile is TX nodes of one row; the march runs along y
+// ---------------------------------------------------------------------------
+template <int ST>
+struct L2 {
+    using S = typename Tr<ST>::S;
+    static constexpr int ES = sizeof(S);
+    static constexpr int TX = 128, NT = TX;
+    static constexpr int HX = 16 / ES;
+    __host__ __device__ static constexpr int bx(int c) { return TX + (c ? 2 * HX : 0); }
+    __host__ __device__ static constexpr int bytes(int c) { return bx(c) * ES; }
+    __host__ __device__ static constexpr int padded(int c) { return (bytes(c) + 127) / 128 * 128; }
+    // y-ring planes: 2 4 | 5 6 7 8 | 11 13 ; classes 0 0 | 1 1 1 1 | 0 0
+    __host__ __device__ static constexpr int yq(int yi)
+    {
+        return yi == 0 ? 2 : (yi == 1 ? 4 : (yi < 6 ? yi + 3 : (yi == 6 ? 11 : 13)));
+    }
+    __host__ __device__ static constexpr int yc(int yi) { return (yi >= 2 && yi < 6) ? 1 : 0; }
+    __host__ __device__ static constexpr int yoff(int yi)
+    {
+        int o = 0;
+        for (int a = 0; a < yi; ++a) o += padded(yc(a));
+        return o;
+    }
+    __host__ __device__ static constexpr int yslot() { return yoff(8); }
+    __host__ __device__ static constexpr int ytx()
+    {
+        int b = 0;
+        for (int a = 0; a < 8; ++a) b += bytes(yc(a));
+        return b;
+    }
+    // row planes: 0 1 3 9 10 12 ; classes 0 1 1 0 1 1
+    __host__ __device__ static constexpr int nq(int ni)
+    {
+        return ni == 0 ? 0 : (ni == 1 ? 1 : (ni == 2 ? 3 : (ni == 3 ? 9 : (ni == 4 ? 10 : 12))));
+    }
+    __host__ __device__ static constexpr int nc(int ni) { return (ni == 0 || ni == 3) ? 0 : 1; }
+    __host__ __device__ static constexpr int noff(int ni)
+    {
+        int o = 0;
+        for (int a = 0; a < ni; ++a) o += padded(nc(a));
+        return o;
+    }
+    __host__ __device__ static constexpr int nslot() { return noff(6); }
+    __host__ __device__ static constexpr int ntx()
+    {
+        int b = 0;
+        for (int a = 0; a < 6; ++a) b += bytes(nc(a));
+        return b;
+    }
+    __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + 128; }
+};
+
+template <int ST>
+__global__ void __launch_bounds__(128, 4)
+k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
+          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+          int write_macro, int64_t total, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    using L = L2<ST>;
+    constexpr int TX = L::TX, HX = L::HX;
+    extern __shared__ unsigned char sm_raw[];
+    unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
+    uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
+    uint64_t *nbar = ybar + 4;
+    volatile int &s_abort = *(volatile int *)(nbar + 2);
+
+    const int tid = threadIdx.x;
+    const int tx = tid;
+    const int ny = G.ny;
+    const int ntx = (G.nx + TX - 1) / TX;
+    if (tid == 0) {
+        for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
+        for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
+        fence_barrier_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    uint32_t ynext = 0, nnext = 0;
+    int i0 = 0;
+    auto issue_y = [&](int s) {
+        const int slot = s & 3;
+        if (tid == 0) {
+            uint64_t *bar = &ybar[slot];
+            mbar_arrive_tx(bar, L::ytx());
+            unsigned char *base = sm + slot * L::yslot();
+#pragma unroll
+            for (int yi = 0; yi < 8; ++yi) {
+                const int c = L::yc(yi);
+                tma_load3(base + L::yoff(yi), &maps.m[c], bar, i0 - (c ? HX : 0), s, L::yq(yi));
+            }
+        }
+        ynext ^= 1u << slot;
+    };
+    auto issue_n = [&](int s) {
+        const int slot = s & 1;
+        if (tid == 0) {
+            uint64_t *bar = &nbar[slot];
+            mbar_arrive_tx(bar, L::ntx());
+            unsigned char *base = sm + 4 * L::yslot() + slot * L::nslot();
+#pragma unroll
+            for (int ni = 0; ni < 6; ++ni) {
+                const int c = L::nc(ni);
+                tma_load3(base + L::noff(ni), &maps.m[c], bar, i0 - (c ? HX : 0), s, L::nq(ni));
+            }
+        }
+        nnext ^= 1u << slot;
+    };
+    auto wait_y = [&](int s) -> bool { return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u); };
+    auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
+
+    const int64_t G_ = gridDim.x;
+    const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
+    const int64_t P = G.plane;
+    bool aborted = false;
+
+    for (int64_t u = ubeg; u < uend && !aborted;) {
+        const int64_t t = u / ny;
+        const int ja = int(u % ny);
+        const int jb = int(ja + ((uend - u) < (ny - ja) ? (uend - u) : (ny - ja)));
+        i0 = int(t) * TX;
+        const int pre_lo = need_lo(ja, ny), pre_hi = need_hi(ja, ny);
+        const int seg_hi = need_hi(jb - 1, ny) > pre_hi ? need_hi(jb - 1, ny) : pre_hi;
+        for (int s = pre_lo; s <= pre_hi; ++s) issue_y(s);
+        issue_n(ja);
+        int yissued = pre_hi;
+
+        const int i = i0 + tx;
+        const bool active = i < G.nx;
+        C xp[3], xm[3];
+        int xa = 0, xb = 0;
+        if (active) {
+            load_w(G.wgt[0], i, xp, xm);
+            xa = off_a(i, G.nx); xb = off_b(i, G.nx);
+        }
+        for (int j = ja; j < jb; ++j) {
+            if (yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued) {
+                issue_y(j + 2);
+                yissued = j + 2;
+            }
+            if (j + 1 < jb) issue_n(j + 1);
+
+            const int64_t id = (int64_t)j * G.pitch + i;
+            C Fy0 = C(0);
+            if (active) Fy0 = Fin[id];
+            bool ok = true;
+            for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
+            ok = ok && wait_n(j);
+            if (!ok) {
+                atomicExch(err, 1);
+                s_abort = 1;
+            }
+            if (active && ok) {
+                const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
+                C yp[3], ym[3];
+                load_w(G.wgt[1], j, yp, ym);
+                auto SV = [&](const unsigned char *box, int idx, int q) -> C {
+                    C val = tocomp(((const S *)box)[idx]);
+                    if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+                    return val;
+                };
+                auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
+                auto NB = [&](int ni) -> const unsigned char * {
+                    return sm + 4 * L::yslot() + (j & 1) * L::nslot() + L::noff(ni);
+                };
+                auto ix = [&](int c, int dx) -> int { return tx + (c ? HX : 0) + dx; };
+                // y-interpolation of a y-ring plane at x-offset dx
+                auto YI = [&](int yi, int q, const C *w, int dx) -> C {
+                    const int c = L::yc(yi);
+                    const int e = ix(c, dx);
+                    return ip(w, SV(YB(yi, ja_), e, q), SV(YB(yi, j), e, q), SV(YB(yi, jb_), e, q));
+                };
+                C f[9], gg[5];
+                f[0] = SV(NB(0), ix(0, 0), 0);
+                f[1] = ip(xp, SV(NB(1), ix(1, xa), 1), SV(NB(1), ix(1, 0), 1), SV(NB(1), ix(1, xb), 1));
+                f[2] = YI(0, 2, yp, 0);
+                f[3] = ip(xm, SV(NB(2), ix(1, xa), 3), SV(NB(2), ix(1, 0), 3), SV(NB(2), ix(1, xb), 3));
+                f[4] = YI(1, 4, ym, 0);
+                f[5] = ip(xp, YI(2, 5, yp, xa), YI(2, 5, yp, 0), YI(2, 5, yp, xb));
+                f[6] = ip(xm, YI(3, 6, yp, xa), YI(3, 6, yp, 0), YI(3, 6, yp, xb));
+                f[7] = ip(xm, YI(4, 7, ym, xa), YI(4, 7, ym, 0), YI(4, 7, ym, xb));
+                f[8] = ip(xp, YI(5, 8, ym, xa), YI(5, 8, ym, 0), YI(5, 8, ym, xb));
+                gg[0] = SV(NB(3), ix(0, 0), 9);
+                gg[1] = ip(xp, SV(NB(4), ix(1, xa), 10), SV(NB(4), ix(1, 0), 10), SV(NB(4), ix(1, xb), 10));
+                gg[2] = YI(6, 11, yp, 0);
+                gg[3] = ip(xm, SV(NB(5), ix(1, xa), 12), SV(NB(5), ix(1, 0), 12), SV(NB(5), ix(1, xb), 12));
+                gg[4] = YI(7, 13, ym, 0);
+
+                // walls (2B:731-801): centre values of row j
+                auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0), q); };
+                auto CY = [&](int yi, int q) -> C { return SV(YB(yi, j), ix(L::yc(yi), 0), q); };
+                const C two_wT = C(2.0) * C(0.125);
+                if (i == 0) {
+                    f[1] = CN(2, 3); f[5] = CY(4, 7); f[8] = CY(3, 6);
+                    gg[1] = -CN(5, 12) + two_wT * C(G.Thot);
+                }
+                if (i == G.nx - 1) {
+                    f[3] = CN(1, 1); f[6] = CY(5, 8); f[7] = CY(2, 5);
+                    gg[3] = -CN(4, 10) + two_wT * C(G.Tcold);
+                }
+                if (j == ny - 1) {
+                    f[4] = CY(0, 2); f[7] = CY(2, 5); f[8] = CY(3, 6);
+                    gg[4] = CY(6, 11);
+                }
+                if (j == 0) {
+                    f[2] = CY(1, 4); f[5] = CY(4, 7); f[6] = CY(5, 8);
+                    gg[2] = CY(7, 13);
+                }
+
+                const C dt = C(G.dt);
+                const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+#if LBM_EXACT
+                const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
+                const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
+#else
+                const C rinv = C(1.0) / rho;
+                const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
+                const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
+#endif
+                const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+                if (write_macro) {
+                    const int64_t mid = (int64_t)j * G.nx + i;
+                    B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
+                }
+                C fp[9], gp[5], Fy;
+                collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+                Fout[id] = Fy;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    C val = fp[q];
+                    if (Tr<ST>::kShift) val -= C(wU2(q));
+                    dst[q * P + id] = tostore<S, C>(val);
+                }
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    C val = gp[q];
+                    if (Tr<ST>::kShift) val -= C(wT2(q)) * C(G.T0);
+                    dst[(9 + q) * P + id] = tostore<S, C>(val);
+                }
+            }
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
+        }
+        u += jb - ja;
+    }
+    if (aborted && tid == 0) {
+        for (int s = 0; s < 4; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
+    }
+}

@@ -32,7 +32,10 @@ EXPORTS = [
     "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
+    "lbm_set_option", "lbm_get_option",
 ]
+OPT_KERNEL, OPT_NBLOCKS = 1, 2
+KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 
 class LBMError(RuntimeError):
@@ -85,6 +88,8 @@ def lib():
         L.lbm_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         L.lbm_device_bytes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         L.lbm_kernel_launches.restype = ctypes.c_int64
+        L.lbm_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
+        L.lbm_get_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
         _lib = L
     return _lib
 
@@ -143,7 +148,7 @@ class Cavity:
     def __init__(self, dim: int, nx: int, ny: int, nz: int = 1, Ra: float = 1e5, Pr: float = 0.71,
                  Ma: float = 0.1, Thot: float = 1.0, Tcold: float = 0.0, grid: str = "erf",
                  stretch: float = 3.2, storage: str = "f64", mode: str = "fast", device: int = 0,
-                 coords: Mesh | None = None):
+                 coords: Mesh | None = None, kernel: str = "auto", nblocks: int = 0):
         if dim == 2:
             nz = 1
         m = coords or mesh(nx, ny, nz if dim == 3 else 0, grid, stretch)
@@ -160,6 +165,22 @@ class Cavity:
         _chk(lib().lbm_create(ctypes.byref(self.params), _p(self._x), _p(self._y), _p(self._z), ctypes.byref(h)),
              "lbm_create")
         self.h = h
+        if kernel != "auto":
+            self.set_option(OPT_KERNEL, KERNELS[kernel])
+        if nblocks:
+            self.set_option(OPT_NBLOCKS, nblocks)
+
+    def set_option(self, option: int, value: int):
+        _chk(lib().lbm_set_option(self.h, int(option), int(value)), "lbm_set_option")
+
+    def get_option(self, option: int) -> int:
+        v = ctypes.c_int64()
+        _chk(lib().lbm_get_option(self.h, int(option), ctypes.byref(v)), "lbm_get_option")
+        return int(v.value)
+
+    @property
+    def kernel(self) -> str:
+        return "march" if self.get_option(OPT_KERNEL) == 2 else "direct"
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:

@@ -1,0 +1,186 @@
+"""CPU model of the TMA march kernels' schedule and shared-memory indexing.
+
+The march kernels (csrc/lbm_march.cuh) fetch population boxes into ring
+slots and compute every node from shared memory.  This model replays, for
+many domain shapes and grid sizes, exactly the per-CTA schedule the kernels
+run (segments, preloads, one prefetch per step, the slices each step waits
+for) and every shared-memory element index the stencils touch, and checks:
+  * each shared-memory index lies inside its box;
+  * every slice a step reads was issued into its slot and not overwritten;
+  * a slot is only refilled once no remaining step needs its slice;
+  * no copy is left in flight at the end of a segment;
+  * TMA box starts satisfy the 16-byte rule on the innermost coordinate;
+  * the persistent CTAs cover every (tile, slice) work item exactly once.
+"""
+import itertools
+
+import pytest
+
+
+def off_a(i, n):
+    return 1 if i == 0 else -1
+
+
+def off_b(i, n):
+    return 2 if i == 0 else (-2 if i == n - 1 else 1)
+
+
+def need_lo(k, n):
+    return k - 2 if k == n - 1 else (0 if k == 0 else k - 1)
+
+
+def need_hi(k, n):
+    return 2 if k == 0 else (k if k == n - 1 else k + 1)
+
+
+def replay(n, total, grid, nodes_of_unit, check_node):
+    """Replay the march schedule along an axis of n slices for `grid` CTAs.
+    The in-plane indices of a node do not depend on the step, so each tile's
+    nodes are checked once, at every step kind (first, inner, last slice)."""
+    covered = [0] * total
+    checked = set()
+    for b in range(grid):
+        ubeg, uend = total * b // grid, total * (b + 1) // grid
+        slot = {}  # ring slot -> slice currently held
+        nslot = {}
+        inflight = set()
+        u = ubeg
+        while u < uend:
+            t, ka = divmod(u, n)
+            kb = ka + min(uend - u, n - ka)
+            pre_lo, pre_hi = need_lo(ka, n), need_hi(ka, n)
+            seg_hi = max(need_hi(kb - 1, n), pre_hi)
+
+            def issue(s, k_now):
+                assert 0 <= s < n
+                old = slot.get(s & 3)
+                if old is not None and old[0] == t:
+                    # the slice being evicted must not be needed by this or a later step
+                    for kk in range(k_now, kb):
+                        assert not (need_lo(kk, n) <= old[1] <= need_hi(kk, n)), (old, kk)
+                slot[s & 3] = (t, s)
+                inflight.add(s)
+
+            for s in range(pre_lo, pre_hi + 1):
+                issue(s, ka)
+            nslot[ka & 1] = (t, ka)
+            zissued = pre_hi
+            for k in range(ka, kb):
+                if zissued < seg_hi and k + 2 <= seg_hi and k + 2 > zissued:
+                    issue(k + 2, k)
+                    zissued = k + 2
+                if k + 1 < kb:
+                    old = nslot.get((k + 1) & 1)
+                    assert old is None or old[0] != t or old[1] < k
+                    nslot[(k + 1) & 1] = (t, k + 1)
+                for s in range(need_lo(k, n), need_hi(k, n) + 1):
+                    assert slot.get(s & 3) == (t, s), ("slice not resident", s, k)
+                    inflight.discard(s)
+                assert nslot[k & 1] == (t, k)
+                kind = (t, 0 if k == 0 else (2 if k == n - 1 else 1))
+                if kind not in checked:
+                    checked.add(kind)
+                    for node in nodes_of_unit(t):
+                        check_node(node, k)
+                covered[t * n + k] += 1
+            assert not inflight, ("copies left in flight", inflight)
+            u += kb - ka
+    assert all(c == 1 for c in covered)
+
+
+# 3D: tiles of 32 x 8 (x, y), boxes with +-HX columns and +-1 rows
+TX3, TY3 = 32, 8
+
+
+def check_3d(nx, ny, nz, grid, es):
+    HX = 16 // es
+    bx = lambda c: TX3 + (2 * HX if c & 1 else 0)  # noqa: E731
+    by = lambda c: TY3 + (2 if c & 2 else 0)  # noqa: E731
+    ntx, nty = -(-nx // TX3), -(-ny // TY3)
+    ntiles = ntx * nty
+    for tix in range(ntx):
+        i0 = tix * TX3
+        for c in range(4):
+            x0 = i0 - (HX if c & 1 else 0)
+            assert (x0 * es) % 16 == 0 and (bx(c) * es) % 16 == 0 and bx(c) <= 256 and by(c) <= 256
+
+    def nodes(t):
+        i0, j0 = (t % ntx) * TX3, (t // ntx) * TY3
+        for ty, tx in itertools.product(range(TY3), range(TX3)):
+            i, j = i0 + tx, j0 + ty
+            if i < nx and j < ny:
+                yield (tx, ty, i, j)
+
+    def idx(c, tx, ty, dx, dy):
+        r = ty + (1 if c & 2 else 0) + dy
+        col = tx + (HX if c & 1 else 0) + dx
+        assert 0 <= r < by(c) and 0 <= col < bx(c), (c, tx, ty, dx, dy)
+        return r * bx(c) + col
+
+    def check_node(node, k):
+        tx, ty, i, j = node
+        xa, xb, ya, yb = off_a(i, nx), off_b(i, nx), off_a(j, ny), off_b(j, ny)
+        for c in range(4):
+            idx(c, tx, ty, 0, 0)
+        for dx in (xa, 0, xb):
+            idx(1, tx, ty, dx, 0)
+            for dy in (ya, 0, yb):
+                idx(3, tx, ty, dx, dy)
+        for dy in (ya, 0, yb):
+            idx(2, tx, ty, 0, dy)
+        for s in (k + off_a(k, nz), k, k + off_b(k, nz)):
+            assert need_lo(k, nz) <= s <= need_hi(k, nz)
+
+    replay(nz, ntiles * nz, grid, nodes, check_node)
+
+
+def check_2d(nx, ny, grid, es):
+    TX = 128
+    HX = 16 // es
+    bx = lambda c: TX + (2 * HX if c else 0)  # noqa: E731
+    ntx = -(-nx // TX)
+    for t in range(ntx):
+        for c in range(2):
+            x0 = t * TX - (HX if c else 0)
+            assert (x0 * es) % 16 == 0 and (bx(c) * es) % 16 == 0 and bx(c) <= 256
+
+    def nodes(t):
+        for tx in range(TX):
+            i = t * TX + tx
+            if i < nx:
+                yield (tx, i)
+
+    def check_node(node, j):
+        tx, i = node
+        for c in range(2):
+            for dx in (off_a(i, nx), 0, off_b(i, nx)):
+                if c == 0 and dx:
+                    continue
+                col = tx + (HX if c else 0) + dx
+                assert 0 <= col < bx(c)
+        for s in (j + off_a(j, ny), j, j + off_b(j, ny)):
+            assert need_lo(j, ny) <= s <= need_hi(j, ny)
+
+    replay(ny, ntx * ny, grid, nodes, check_node)
+
+
+@pytest.mark.parametrize("shape", [(128, 128, 128), (20, 16, 16), (33, 18, 7), (64, 24, 3), (40, 10, 5), (16, 16, 16)])
+@pytest.mark.parametrize("es", [8, 4, 2])
+def test_march3d_schedule_and_indices(shape, es):
+    nx, ny, nz = shape
+    assert ny % TY3 != 1  # the host routes such shapes to the direct-load kernel
+    ntiles = -(-nx // TX3) * -(-ny // TY3)
+    total = ntiles * nz
+    for grid in sorted({1, 2, 3, 7, 148, min(296, total), total}):
+        if grid <= total:
+            check_3d(nx, ny, nz, grid, es)
+
+
+@pytest.mark.parametrize("shape", [(2048, 64), (128, 128), (130, 9), (48, 48), (300, 3), (40, 24)])
+@pytest.mark.parametrize("es", [8, 4, 2])
+def test_march2d_schedule_and_indices(shape, es):
+    nx, ny = shape
+    total = -(-nx // 128) * ny
+    for grid in sorted({1, 2, 5, 148, 592, total}):
+        if grid <= total:
+            check_2d(nx, ny, grid, es)

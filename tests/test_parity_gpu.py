@@ -15,8 +15,10 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def pair(pkg, ora, dim, nx, ny, nz=1, grid="erf", stretch=3.2, Ra=1e5, Pr=0.71, mode="fast", storage="f64"):
-    cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, mode=mode, storage=storage)
+def pair(pkg, ora, dim, nx, ny, nz=1, grid="erf", stretch=3.2, Ra=1e5, Pr=0.71, mode="fast", storage="f64",
+         kernel="auto", nblocks=0):
+    cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, mode=mode, storage=storage,
+                     kernel=kernel, nblocks=nblocks)
     o = ora.Oracle(dim, nx, ny, nz, x=cav.mesh.x, y=cav.mesh.y, z=cav.mesh.z, dt=cav.mesh.dt,
                    length_LB=cav.mesh.length_LB, Ra=Ra, Pr=Pr)
     cav.initial()
@@ -31,16 +33,20 @@ FIELDS2 = ("rho", "u", "v", "T")
 FIELDS3 = ("rho", "u", "v", "w", "T")
 
 
+@pytest.mark.parametrize("kernel", ["direct", "march"])
 @pytest.mark.parametrize("case", [
     dict(dim=2, nx=32, ny=32, grid="erf", stretch=3.2, steps=150),
     dict(dim=2, nx=40, ny=24, grid="tanh", stretch=1.5, steps=120),
+    dict(dim=2, nx=150, ny=20, grid="tanh", stretch=1.5, steps=40),
     dict(dim=3, nx=14, ny=12, nz=10, grid="erf", stretch=3.2, steps=40),
     dict(dim=3, nx=16, ny=16, nz=16, grid="tanh", stretch=1.5, steps=30),
+    dict(dim=3, nx=40, ny=18, nz=7, grid="tanh", stretch=1.5, steps=25),
 ])
-def test_exact_mode_bit_identical(pkg, ora, case):
+def test_exact_mode_bit_identical(pkg, ora, case, kernel):
     c = dict(case)
     steps = c.pop("steps")
-    cav, o = pair(pkg, ora, mode="exact", **c)
+    cav, o = pair(pkg, ora, mode="exact", kernel=kernel, **c)
+    assert cav.kernel == kernel
     cav.step(steps)
     o.step(steps)
     m = cav.macro()
@@ -52,13 +58,14 @@ def test_exact_mode_bit_identical(pkg, ora, case):
     cav.close()
 
 
+@pytest.mark.parametrize("kernel", ["direct", "march"])
 @pytest.mark.parametrize("case", [
     dict(dim=2, nx=48, ny=48, grid="tanh", stretch=1.5, Ra=1e4),
     dict(dim=2, nx=33, ny=33, grid="erf", stretch=3.2, Ra=1e5),
     dict(dim=3, nx=20, ny=20, nz=20, grid="tanh", stretch=1.5, Ra=1e5),
 ])
-def test_fast_fp64_within_1e12_after_1000_steps(pkg, ora, case):
-    cav, o = pair(pkg, ora, mode="fast", **case)
+def test_fast_fp64_within_1e12_after_1000_steps(pkg, ora, case, kernel):
+    cav, o = pair(pkg, ora, mode="fast", kernel=kernel, **case)
     cav.step(1000)
     o.step(1000)
     f, g = cav.populations()
@@ -137,6 +144,37 @@ def test_reduced_precision_storage(pkg, ora, storage, tol_u, tol_T, dim):
     assert du / umax <= tol_u
     assert dT <= tol_T
     cav.close()
+
+
+@pytest.mark.parametrize("dim,shape", [(3, (40, 18, 12)), (2, (300, 30, 1))])
+def test_march_grid_sizes_bit_identical(pkg, ora, dim, shape):
+    # persistent grids of 1, 3, 7 blocks make every CTA march across several
+    # tiles and restart its ring at tile boundaries
+    o = None
+    for nb in (1, 3, 7, 0):
+        cav, o2 = pair(pkg, ora, dim, *shape, grid="tanh", stretch=1.5, mode="exact", kernel="march", nblocks=nb)
+        cav.step(12)
+        if o is None:
+            o = o2
+            o.step(12)
+        m = cav.macro()
+        for k in (FIELDS2 if dim == 2 else FIELDS3):
+            assert np.array_equal(m[k], o.field(k)), (nb, k)
+        cav.close()
+
+
+def test_kernel_option_reports_choice(pkg):
+    big = pkg.Cavity(3, 64, 64, 64)
+    assert big.kernel == "march" and big.get_option(pkg.lbm.OPT_NBLOCKS) > 0
+    small = pkg.Cavity(2, 20, 20)
+    assert small.kernel == "direct"
+    odd = pkg.Cavity(3, 32, 17, 8)  # a last tile row of one y-row: direct-load only
+    assert odd.kernel == "direct"
+    with pytest.raises(pkg.LBMError) as e:
+        odd.set_option(pkg.lbm.OPT_KERNEL, 2)
+    assert e.value.status == -8
+    for c in (big, small, odd):
+        c.close()
 
 
 def test_step_before_init_is_a_state_error(pkg):

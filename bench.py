@@ -219,6 +219,14 @@ def config_of(args, wl, inner):
             "parallelism": f"{args.gpus} independent cavities, one per GPU"}
 
 
+def add_kernel_config(cfg, cav, pkg):
+    cfg["kernel"] = cav.kernel
+    if cav.kernel == "march":
+        cfg["march_blocks"] = cav.get_option(pkg.lbm.OPT_NBLOCKS)
+        cfg["l2_promotion"] = ["none", "64B", "128B", "256B"][cav.get_option(pkg.lbm.OPT_L2PROMO)]
+    return cfg
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -233,6 +241,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "march"])
+    ap.add_argument("--nblocks", type=int, default=0, help="persistent blocks of the march kernel (0 = auto)")
+    ap.add_argument("--l2promo", type=int, default=-1, help="TMA L2 promotion 0..3 (-1 = library default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -250,7 +260,9 @@ def main():
     wl = WORKLOADS[args.workload]
     dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
     cav = pkg.Cavity(dim, nx, ny, nz, Ra=Ra, Pr=Pr, grid=grid, stretch=stretch, storage=args.storage,
-                     mode=args.mode, device=local, kernel=args.kernel)
+                     mode=args.mode, device=local, kernel=args.kernel, nblocks=args.nblocks)
+    if args.l2promo >= 0:
+        cav.set_option(pkg.lbm.OPT_L2PROMO, args.l2promo)
     shape = cav.shape
     # pinned host fields for the end-to-end leg
     pin = {k: torch.zeros(shape, dtype=torch.float64, pin_memory=True) for k in ("rho", "u", "v", "w", "T")}
@@ -348,7 +360,7 @@ def main():
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "f16s": "f16 storage / f32"}[args.storage],
-            "data": "synthetic", "config": config_of(args, wl, args.inner),
+            "data": "synthetic", "config": add_kernel_config(config_of(args, wl, args.inner), cav, pkg),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_lup": bpl,

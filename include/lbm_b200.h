@@ -56,7 +56,9 @@ extern "C" {
 
 /* options for lbm_set_option / lbm_get_option */
 #define LBM_OPT_KERNEL   1  /* step kernel: 0 automatic, 1 direct-load, 2 TMA march */
-#define LBM_OPT_NBLOCKS  2  /* persistent blocks of the march kernel (0 = one wave) */
+#define LBM_OPT_NBLOCKS  2  /* persistent blocks of the march kernel (0 = automatic) */
+#define LBM_OPT_L2PROMO  3  /* L2 fetch promotion of the march kernel's TMA boxes:
+                               0 none, 1 64 B, 2 128 B, 3 256 B */
 
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */

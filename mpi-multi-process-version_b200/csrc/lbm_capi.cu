@@ -226,6 +226,7 @@ struct lbm_handle {
     int use_march = 0;           // resolved choice
     int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
     int nblocks = 0;             // resolved persistent grid
+    int l2promo = 0;             // LBM_OPT_L2PROMO
     int cur = 0;                 // buffer holding the newest populations
     int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
     int64_t itc = 0;
@@ -308,6 +309,10 @@ static bool encode_maps(lbm_handle *h)
                                                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
     const cuuint64_t es = h->esize;
     const int nplanes = h->Q + h->QT;
+    const CUtensorMapL2promotion promo = h->l2promo == 3   ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+                                         : h->l2promo == 2 ? CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+                                         : h->l2promo == 1 ? CU_TENSOR_MAP_L2_PROMOTION_L2_64B
+                                                           : CU_TENSOR_MAP_L2_PROMOTION_NONE;
     for (int buf = 0; buf < 2; ++buf) {
         for (int c = 0; c < 4; ++c) {
             CUtensorMap *m = &h->tmaps[buf].m[c];
@@ -319,8 +324,7 @@ static bool encode_maps(lbm_handle *h)
                 const cuuint32_t box[4] = {(cuuint32_t)ms.bx[c], (cuuint32_t)ms.by[c], 1, 1};
                 const cuuint32_t estr[4] = {1, 1, 1, 1};
                 r = enc(m, dtype, 4, h->bufs.pop[buf], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             } else {
                 const int cc = c & 1;
                 const cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
@@ -328,11 +332,31 @@ static bool encode_maps(lbm_handle *h)
                 const cuuint32_t box[3] = {(cuuint32_t)ms.bx[cc], 1, 1};
                 const cuuint32_t estr[3] = {1, 1, 1};
                 r = enc(m, dtype, 3, h->bufs.pop[buf], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                        CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             }
             if (r != CUDA_SUCCESS) return false;
         }
+        // the carried force of this buffer: compute type, one value per node
+        const CUtensorMapDataType ftype =
+            h->csize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        const cuuint64_t cs = h->csize;
+        CUresult r;
+        if (g.dim == 3) {
+            const cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz};
+            const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * cs, (cuuint64_t)g.slab * cs};
+            const cuuint32_t box[3] = {(cuuint32_t)ms.TX, (cuuint32_t)ms.TY, 1};
+            const cuuint32_t estr[3] = {1, 1, 1};
+            r = enc(&h->tmaps[buf].fmap, ftype, 3, h->bufs.F[buf], dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        } else {
+            const cuuint64_t dims[2] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny};
+            const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * cs};
+            const cuuint32_t box[2] = {(cuuint32_t)ms.TX, 1};
+            const cuuint32_t estr[2] = {1, 1};
+            r = enc(&h->tmaps[buf].fmap, ftype, 2, h->bufs.F[buf], dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        }
+        if (r != CUDA_SUCCESS) return false;
     }
     return true;
 }
@@ -363,7 +387,24 @@ static int resolve_path(lbm_handle *h)
         }
         int sms = 0;
         CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-        h->nblocks = h->nblocks_opt > 0 ? h->nblocks_opt : bps * sms;
+        const int slots = bps * sms;
+        if (h->nblocks_opt > 0) {
+            h->nblocks = h->nblocks_opt;
+        } else {
+            // z-lockstep grid: every tile column split into the same number of
+            // chunks, so neighbouring tiles are processed at the same slice and
+            // their shared halo rows are served from L2; used when it fills at
+            // least 80 % of the resident slots, otherwise one full wave with an
+            // equal share of tile-slices per block
+            const MarchShape ms = march_shape(h->geo.dim, h->p.storage);
+            const int64_t ntiles = (int64_t)((h->geo.nx + ms.TX - 1) / ms.TX) *
+                                   (h->geo.dim == 3 ? (h->geo.ny + ms.TY - 1) / ms.TY : 1);
+            const int64_t chunks = ntiles <= slots ? slots / ntiles : 0;
+            if (chunks > 0 && ntiles * chunks * 5 >= (int64_t)slots * 4)
+                h->nblocks = (int)(ntiles * chunks);
+            else
+                h->nblocks = slots;
+        }
     }
     return LBM_OK;
 }
@@ -772,6 +813,12 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         if (value < 0 || value > (1 << 20)) return fail(LBM_ERR_PARAM, "nblocks out of range");
         h->nblocks_opt = (int)value;
         return resolve_path(h);
+    case LBM_OPT_L2PROMO:
+        if (value < 0 || value > 3) return fail(LBM_ERR_PARAM, "L2 promotion must be 0..3");
+        CU(cudaStreamSynchronize(h->stream));
+        h->l2promo = (int)value;
+        h->march_ok = encode_maps(h);
+        return resolve_path(h);
     default:
         return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
@@ -783,6 +830,7 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     switch (option) {
     case LBM_OPT_KERNEL: *value = h->use_march ? 2 : 1; return LBM_OK;
     case LBM_OPT_NBLOCKS: *value = h->use_march ? h->nblocks : 0; return LBM_OK;
+    case LBM_OPT_L2PROMO: *value = h->l2promo; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

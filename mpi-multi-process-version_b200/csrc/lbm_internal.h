@@ -31,9 +31,11 @@ struct Bufs {
     int *err;              // device error flag (bounded waits that gave up)
 };
 
-// TMA descriptors of one population buffer, one per box class
+// TMA descriptors of one population buffer (one per box class) and of the
+// carried-force array that goes with it
 struct alignas(64) TmapSet {
     CUtensorMap m[4];
+    CUtensorMap fmap;
 };
 
 // shape of the march kernels' tiles for a lattice and storage (host side)

@@ -457,6 +457,200 @@ __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C
     gp[6] = -DV(np[3],2.0)+DV(np[4],6.0)+DV(np[5],6.0)-DV(np[6],3.0);
 }
 
+#if !LBM_EXACT
+// Fast-path 3D node update: the same collision as collide3d (3M:445-730) with
+// shared subexpressions.  Moments are built from pairwise sums and
+// differences of the +- populations, rho and momentum are taken from the
+// moments (the reference's macro_u sums are the same sums), and the inverse
+// transform groups the +- symmetric populations; ~45 % fewer FP64 operations
+// and shorter dependency chains.  Fz0 is the force carried from the previous
+// collision (macro_u's half-force term).  Writes rho, u, v, w, T.
+template <class C>
+__device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7],
+                                            C &Fz, C &rho, C &u, C &v, C &w, C &T)
+{
+    const C Snu = C(G.Snu), Sq = C(G.Sq), dt = C(G.dt), gbeta = C(G.gbeta), sig_k = C(G.sig_k);
+    // pairwise sums / differences
+    const C a12 = f[1] + f[2], d12 = f[1] - f[2];
+    const C a34 = f[3] + f[4], d34 = f[3] - f[4];
+    const C a56 = f[5] + f[6], d56 = f[5] - f[6];
+    const C p78 = f[7] + f[8], q78 = f[7] - f[8], p910 = f[9] + f[10], q910 = f[9] - f[10];
+    const C p1112 = f[11] + f[12], q1112 = f[11] - f[12], p1314 = f[13] + f[14], q1314 = f[13] - f[14];
+    const C p1516 = f[15] + f[16], q1516 = f[15] - f[16], p1718 = f[17] + f[18], q1718 = f[17] - f[18];
+    const C s_xy = p78 + p910, xy_x = q78 + q910, xy_y = p78 - p910;
+    const C s_xz = p1112 + p1314, xz_x = q1112 + q1314, xz_z = p1112 - p1314;
+    const C s_yz = p1516 + p1718, yz_y = q1516 + q1718, yz_z = p1516 - p1718;
+    const C sA = a12 + (a34 + a56), sD = s_xy + (s_xz + s_yz);
+    const C xsum = xy_x + xz_x, ysum = xy_y + yz_y, zsum = xz_z + yz_z;
+    C m[19];
+    m[0] = f[0] + sA + sD;
+    m[1] = C(-30.0) * f[0] - C(11.0) * sA + C(8.0) * sD;
+    m[2] = C(12.0) * f[0] - C(4.0) * sA + sD;
+    m[3] = d12 + xsum;
+    m[4] = C(-4.0) * d12 + xsum;
+    m[5] = d34 + ysum;
+    m[6] = C(-4.0) * d34 + ysum;
+    m[7] = d56 + zsum;
+    m[8] = C(-4.0) * d56 + zsum;
+    const C a3456 = a34 + a56, sxyxz = s_xy + s_xz;
+    m[9] = C(2.0) * a12 - a3456 + sxyxz - C(2.0) * s_yz;
+    m[10] = C(-4.0) * a12 + C(2.0) * a3456 + sxyxz - C(2.0) * s_yz;
+    const C a34m56 = a34 - a56, sxymxz = s_xy - s_xz;
+    m[11] = a34m56 + sxymxz;
+    m[12] = C(-2.0) * a34m56 + sxymxz;
+    m[13] = q78 - q910;
+    m[14] = q1516 - q1718;
+    m[15] = q1112 - q1314;
+    m[16] = xy_x - xz_x;
+    m[17] = yz_y - xy_y;
+    m[18] = xz_z - yz_z;
+
+    // macro_u / macro_t (3M:988-1025)
+    rho = m[0];
+    const C rinv = C(1.0) / rho;
+    u = m[3] * rinv;
+    v = m[5] * rinv;
+    w = (m[7] + C(0.5) * dt * Fz0) * rinv;
+    T = gg[0] + (gg[1] + gg[2]) + (gg[3] + gg[4]) + (gg[5] + gg[6]);
+
+    // equilibria and relaxation (3M:522-587)
+    const C uu = u * u, vv = v * v, ww = w * w;
+    const C Vs = uu + vv + ww;
+    const C ru = rho * u, rv = rho * v, rw = rho * w;
+    Fz = gbeta * T * rho;
+    const C wF = w * Fz * dt;
+    const C hNu = C(1.0) - C(0.5) * Snu;
+    const C e9 = C(3.0) * rho * uu - rho * Vs;
+    const C e11 = rho * (vv - ww);
+    C mp[19];
+    mp[0] = m[0];
+    mp[1] = m[1] - Snu * (m[1] - (C(-11.0) * rho + C(19.0) * rho * Vs)) + (C(38.0) - C(19.0) * Snu) * wF;
+    mp[2] = m[2] - Snu * (m[2] - (C(3.0) * rho - C(5.5) * rho * Vs)) - (C(11.0) - C(5.5) * Snu) * wF;
+    mp[3] = m[3];
+    mp[4] = m[4] - Sq * (m[4] - C(-2.0 / 3.0) * ru);
+    mp[5] = m[5];
+    mp[6] = m[6] - Sq * (m[6] - C(-2.0 / 3.0) * rv);
+    mp[7] = m[7] + Fz * dt;
+    mp[8] = m[8] - Sq * (m[8] - C(-2.0 / 3.0) * rw) - (C(2.0 / 3.0) * (C(1.0) - C(0.5) * Sq)) * Fz * dt;
+    mp[9] = m[9] - Snu * (m[9] - e9) + (Snu - C(2.0)) * wF;
+    mp[10] = m[10] - Snu * (m[10] + C(0.5) * e9) + hNu * wF;
+    mp[11] = m[11] - Snu * (m[11] - e11) - (C(2.0) - Snu) * wF;
+    mp[12] = m[12] - Snu * (m[12] + C(0.5) * e11) + hNu * wF;
+    mp[13] = m[13] - Snu * (m[13] - ru * v);
+    mp[14] = m[14] - Snu * (m[14] - rv * w) + hNu * v * Fz * dt;
+    mp[15] = m[15] - Snu * (m[15] - ru * w) + hNu * u * Fz * dt;
+    const C oSq = C(1.0) - Sq;
+    mp[16] = oSq * m[16];
+    mp[17] = oSq * m[17];
+    mp[18] = oSq * m[18];
+
+    // inverse transform (3M:589-655), grouped by symmetric pairs
+    const C D0 = mp[0] * C(1.0 / 19.0);
+    fp[0] = D0 - mp[1] * C(5.0 / 399.0) + mp[2] * C(1.0 / 21.0);
+    const C A = D0 - mp[1] * C(11.0 / 2394.0) - mp[2] * C(1.0 / 63.0);
+    const C D = D0 + mp[1] * C(4.0 / 1197.0) + mp[2] * C(1.0 / 252.0);
+    const C h910 = (mp[9] - mp[10]);
+    const C h1112 = (mp[11] - mp[12]);
+    {
+        const C c = A + h910 * C(1.0 / 18.0), o = (mp[3] - mp[4]) * C(0.1);
+        fp[1] = c + o; fp[2] = c - o;
+    }
+    {
+        const C c = A - h910 * C(1.0 / 36.0) + h1112 * C(1.0 / 12.0), o = (mp[5] - mp[6]) * C(0.1);
+        fp[3] = c + o; fp[4] = c - o;
+    }
+    {
+        const C c = A - h910 * C(1.0 / 36.0) - h1112 * C(1.0 / 12.0), o = (mp[7] - mp[8]) * C(0.1);
+        fp[5] = c + o; fp[6] = c - o;
+    }
+    const C X = mp[3] * C(0.1) + mp[4] * C(0.025);
+    const C Y = mp[5] * C(0.1) + mp[6] * C(0.025);
+    const C Z = mp[7] * C(0.1) + mp[8] * C(0.025);
+    const C e9b = mp[9] * C(1.0 / 36.0) + mp[10] * C(1.0 / 72.0);
+    const C e11b = mp[11] * C(1.0 / 12.0) + mp[12] * C(1.0 / 24.0);
+    const C r16 = mp[16] * C(0.125), r17 = mp[17] * C(0.125), r18 = mp[18] * C(0.125);
+    {   // xy plane: 7 (+,+), 8 (-,+), 9 (+,-), 10 (-,-)
+        const C DE = D + e9b + e11b, c = mp[13] * C(0.25);
+        const C P = X + r16, Qy = Y - r17;
+        const C s1 = DE + c, s2 = DE - c;
+        fp[7] = s1 + (P + Qy); fp[10] = s1 - (P + Qy);
+        fp[8] = s2 - (P - Qy); fp[9] = s2 + (P - Qy);
+    }
+    {   // xz plane: 11 (+,+), 12 (-,+), 13 (+,-), 14 (-,-)
+        const C DE = D + e9b - e11b, c = mp[15] * C(0.25);
+        const C P = X - r16, Qz = Z + r18;
+        const C s1 = DE + c, s2 = DE - c;
+        fp[11] = s1 + (P + Qz); fp[14] = s1 - (P + Qz);
+        fp[12] = s2 - (P - Qz); fp[13] = s2 + (P - Qz);
+    }
+    {   // yz plane: 15 (+,+), 16 (-,+), 17 (+,-), 18 (-,-)
+        const C DE = D - mp[9] * C(1.0 / 18.0) - mp[10] * C(1.0 / 36.0), c = mp[14] * C(0.25);
+        const C P = Y + r17, Qz = Z - r18;
+        const C s1 = DE + c, s2 = DE - c;
+        fp[15] = s1 + (P + Qz); fp[18] = s1 - (P + Qz);
+        fp[16] = s2 - (P - Qz); fp[17] = s2 + (P - Qz);
+    }
+
+    // thermal D3Q7 (3M:671-730)
+    const C b12 = gg[1] + gg[2], b34 = gg[3] + gg[4], b56 = gg[5] + gg[6];
+    const C n1 = gg[1] - gg[2], n2 = gg[3] - gg[4], n3 = gg[5] - gg[6];
+    const C n4 = b12 + b34 + b56, n5 = b12 - b34, n6 = b12 - b56;
+    const C np1 = n1 - sig_k * (n1 - T * u);
+    const C np2 = n2 - sig_k * (n2 - T * v);
+    const C np3 = n3 - sig_k * (n3 - T * w);
+    const C np4 = n4 - C(1.2) * (n4 - T * C(0.5));
+    const C np5 = C(-0.2) * n5, np6 = C(-0.2) * n6;
+    gp[0] = T - np4;
+    const C t4 = np4 * C(1.0 / 6.0), t5 = np5 * C(1.0 / 6.0), t6 = np6 * C(1.0 / 6.0);
+    {
+        const C c = t4 + t5 + t6, o = np1 * C(0.5);
+        gp[1] = c + o; gp[2] = c - o;
+    }
+    {
+        const C c = t4 - C(2.0) * t5 + t6, o = np2 * C(0.5);
+        gp[3] = c + o; gp[4] = c - o;
+    }
+    {
+        const C c = t4 + t5 - C(2.0) * t6, o = np3 * C(0.5);
+        gp[5] = c + o; gp[6] = c - o;
+    }
+}
+#endif
+
+// macro_u / macro_t (3M:988-1025) in the reference's operation order
+template <class C>
+__device__ __forceinline__ void macro3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C &rho, C &u, C &v,
+                                        C &w, C &T)
+{
+    const C dt = C(G.dt);
+    rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
+#if LBM_EXACT
+    u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
+    v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
+    w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)/rho;
+#else
+    const C rinv = C(1.0) / rho;
+    u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])*rinv;
+    v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
+    w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
+#endif
+    T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+}
+
+// macro + collision of one node: the reference's order in the exact build,
+// the shared-subexpression form in the fast build
+template <class C>
+__device__ __forceinline__ void node3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7], C &Fz,
+                                       C &rho, C &u, C &v, C &w, C &T)
+{
+#if LBM_EXACT
+    macro3d<C>(f, gg, Fz0, G, rho, u, v, w, T);
+    collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+#else
+    node3d_fast<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+#endif
+}
+
 template <int ST, int KIND>
 __global__ void __launch_bounds__(256)
 k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename Tr<ST>::C *__restrict__ Fin,
@@ -548,22 +742,15 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
         gg[6] = LD(24, 0);
     }
 
-    // macro_u / macro_t (3M:988-1025)
+    // macro_u / macro_t (3M:988-1025) and the collision
     const C Fz0 = Fin[id];
-    const C dt = C(G.dt);
-    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
-#if LBM_EXACT
-    const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
-    const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
-    const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)/rho;
-#else
-    const C rinv = C(1.0) / rho;
-    const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])*rinv;
-    const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
-    const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
-#endif
-    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
-
+    C rho, u, v, w, T, fp[19], gp[7], Fz;
+    if (LBM_EXACT || KIND == 1) {
+        macro3d<C>(f, gg, Fz0, G, rho, u, v, w, T);
+        if (KIND == 0) collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+    } else {
+        node3d<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+    }
     if (write_macro || KIND == 1) {
         const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
         B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
@@ -580,8 +767,6 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
         for (int q = 0; q < 7; ++q) ST_(19 + q, gg[q]);
         return;
     }
-    C fp[19], gp[7], Fz;
-    collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
     Fout[id] = Fz;
 #pragma unroll
     for (int q = 0; q < 19; ++q) ST_(q, fp[q]);

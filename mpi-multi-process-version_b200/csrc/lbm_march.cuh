@@ -82,6 +82,24 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, uint6
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *m, uint64_t *bar, int c0, int c1)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(saddr(dst)),
+        "l"(m), "r"(c0), "r"(c1), "r"(saddr(bar))
+        : "memory");
+}
+
+// plain bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     saddr(dst)),
+                 "l"(src), "r"(bytes), "r"(saddr(bar))
+                 : "memory");
+}
+
 __device__ __forceinline__ void fence_barrier_init()
 {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -104,6 +122,7 @@ __device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k ==
 template <int ST>
 struct L3 {
     using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
     static constexpr int TX = 32, TY = 8, NT = TX * TY;
     static constexpr int HX = 16 / ES;
@@ -145,12 +164,17 @@ struct L3 {
         for (int a = 0; a < ni; ++a) o += padded(nc(a));
         return o;
     }
-    __host__ __device__ static constexpr int nslot() { return noff(14); }
+    // after the planes: the carried-force box of the tile, then the slice's six
+    // z-interpolation weights
+    __host__ __device__ static constexpr int fbytes() { return TX * TY * (int)sizeof(C); }
+    __host__ __device__ static constexpr int fo() { return noff(14); }
+    __host__ __device__ static constexpr int wo() { return fo() + (fbytes() + 127) / 128 * 128; }
+    __host__ __device__ static constexpr int nslot() { return wo() + 128; }
     __host__ __device__ static constexpr int ntx()
     {
         int b = 0;
         for (int a = 0; a < 14; ++a) b += bytes(nc(a));
-        return b;
+        return b + fbytes() + 48;
     }
     // ring slots, 6 barriers and the abort flag, and slack for 128-byte alignment
     __host__ __device__ static constexpr int smem() { return 4 * zslot() + 2 * nslot() + 64 + 128; }
@@ -217,6 +241,8 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 tma_load4(base + L::noff(ni), &maps.m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
                           s, L::nq(ni));
             }
+            tma_load3(base + L::fo(), &maps.fmap, bar, i0, j0, s);
+            bulk_load(base + L::wo(), G.wgt[2] + (int64_t)s * 6, 48, bar);
         }
         nnext ^= 1u << slot;
     };
@@ -261,8 +287,6 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
             if (k + 1 < kb) issue_n(k + 1);
 
             const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
-            C Fz0 = C(0);
-            if (active) Fz0 = Fin[id];
             bool ok = true;
             for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
             ok = ok && wait_n(k);
@@ -272,8 +296,10 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
             }
             if (active && ok) {
                 const int ka_ = k + off_a(k, nz), kb_ = k + off_b(k, nz);
-                C zp[3], zm[3];
-                load_w(G.wgt[2], k, zp, zm);
+                const unsigned char *nslot_k = sm + 4 * L::zslot() + (k & 1) * L::nslot();
+                const C Fz0 = ((const C *)(nslot_k + L::fo()))[ty * TX + tx];
+                const double *wz = (const double *)(nslot_k + L::wo());
+                const C zp[3] = {C(wz[0]), C(wz[1]), C(wz[2])}, zm[3] = {C(wz[3]), C(wz[4]), C(wz[5])};
                 auto SV = [&](const unsigned char *box, int idx, int q) -> C {
                     C val = tocomp(((const S *)box)[idx]);
                     if (Tr<ST>::kShift) val += (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
@@ -360,27 +386,14 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                     gg[6] = CZ(10, 24);
                 }
 
-                // macro_u / macro_t (3M:988-1025)
-                const C dt = C(G.dt);
-                const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
-#if LBM_EXACT
-                const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
-                const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
-                const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)/rho;
-#else
-                const C rinv = C(1.0) / rho;
-                const C u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])*rinv;
-                const C v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
-                const C w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
-#endif
-                const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+                // macro_u / macro_t (3M:988-1025) and the collision
+                C rho, u, v, w, T, fp[19], gp[7], Fz;
+                node3d<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
                 if (write_macro) {
                     const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
                     B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
                     B.w[mid] = double(w); B.T[mid] = double(T);
                 }
-                C fp[19], gp[7], Fz;
-                collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
                 Fout[id] = Fz;
 #pragma unroll
                 for (int q = 0; q < 19; ++q) {
@@ -416,6 +429,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 template <int ST>
 struct L2 {
     using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
     static constexpr int TX = 128, NT = TX;
     static constexpr int HX = 16 / ES;
@@ -453,12 +467,15 @@ struct L2 {
         for (int a = 0; a < ni; ++a) o += padded(nc(a));
         return o;
     }
-    __host__ __device__ static constexpr int nslot() { return noff(6); }
+    __host__ __device__ static constexpr int fbytes() { return TX * (int)sizeof(C); }
+    __host__ __device__ static constexpr int fo() { return noff(6); }
+    __host__ __device__ static constexpr int wo() { return fo() + (fbytes() + 127) / 128 * 128; }
+    __host__ __device__ static constexpr int nslot() { return wo() + 128; }
     __host__ __device__ static constexpr int ntx()
     {
         int b = 0;
         for (int a = 0; a < 6; ++a) b += bytes(nc(a));
-        return b;
+        return b + fbytes() + 48;
     }
     __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + 128; }
 };
@@ -482,7 +499,6 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     const int tid = threadIdx.x;
     const int tx = tid;
     const int ny = G.ny;
-    const int ntx = (G.nx + TX - 1) / TX;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
@@ -518,6 +534,8 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 const int c = L::nc(ni);
                 tma_load3(base + L::noff(ni), &maps.m[c], bar, i0 - (c ? HX : 0), s, L::nq(ni));
             }
+            tma_load2(base + L::fo(), &maps.fmap, bar, i0, s);
+            bulk_load(base + L::wo(), G.wgt[1] + (int64_t)s * 6, 48, bar);
         }
         nnext ^= 1u << slot;
     };
@@ -556,8 +574,6 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
             if (j + 1 < jb) issue_n(j + 1);
 
             const int64_t id = (int64_t)j * G.pitch + i;
-            C Fy0 = C(0);
-            if (active) Fy0 = Fin[id];
             bool ok = true;
             for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
             ok = ok && wait_n(j);
@@ -567,8 +583,10 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
             }
             if (active && ok) {
                 const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
-                C yp[3], ym[3];
-                load_w(G.wgt[1], j, yp, ym);
+                const unsigned char *nslot_j = sm + 4 * L::yslot() + (j & 1) * L::nslot();
+                const C Fy0 = ((const C *)(nslot_j + L::fo()))[tx];
+                const double *wy = (const double *)(nslot_j + L::wo());
+                const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
                 auto SV = [&](const unsigned char *box, int idx, int q) -> C {
                     C val = tocomp(((const S *)box)[idx]);
                     if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);

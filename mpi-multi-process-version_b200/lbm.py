@@ -34,7 +34,7 @@ EXPORTS = [
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
     "lbm_set_option", "lbm_get_option",
 ]
-OPT_KERNEL, OPT_NBLOCKS = 1, 2
+OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO = 1, 2, 3
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 

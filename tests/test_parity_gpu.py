@@ -234,3 +234,36 @@ def test_runs_are_deterministic(pkg):
     for k in out[0][0]:
         assert np.array_equal(out[0][0][k], out[1][0][k])
     assert out[0][1] == out[1][1] and out[0][2] == out[1][2]
+
+
+# ---------------------------------------------------------------------------
+# against the golden fixtures produced by the reference programs themselves
+# ---------------------------------------------------------------------------
+import glob as _glob  # noqa: E402
+import os as _os  # noqa: E402
+
+_GOLDEN = sorted(_glob.glob(_os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "golden", "ref_*.npz")))
+
+
+@pytest.mark.parametrize("kernel", ["direct", "march"])
+@pytest.mark.parametrize("path", _GOLDEN, ids=[_os.path.basename(p) for p in _GOLDEN])
+def test_gpu_matches_reference_fixture(pkg, path, kernel):
+    d = dict(np.load(path))
+    dim = d["f"].ndim - 1
+    shape = d["f"].shape[:-1]
+    nz, ny, nx = (shape if dim == 3 else (1,) + shape)
+    m = pkg.Mesh(d["x"], d["y"], d.get("z"), 0.0, float(d["length_LB"]), float(d["dt"]))
+    for mode in ("exact", "fast"):
+        cav = pkg.Cavity(dim, nx, ny, nz, Ra=float(d["Ra"]), Pr=float(d["Pr"]), Ma=float(d["Ma"]), coords=m,
+                         mode=mode, kernel=kernel)
+        cav.initial()
+        cav.step(int(d["itc"]))
+        f, g = cav.populations()
+        mac = cav.macro()
+        if mode == "exact":
+            assert np.array_equal(f, d["f"]) and np.array_equal(g, d["g"])
+            for k in mac:
+                assert np.array_equal(mac[k], d[k]), k
+        else:
+            assert rel_err(f, d["f"]) <= 1e-12 and rel_err(g, d["g"]) <= 1e-12
+        cav.close()

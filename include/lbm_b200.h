@@ -186,6 +186,27 @@ int lbm_device_bytes(const lbm_handle *h, int64_t *bytes);
 /* Number of kernels this library launched since load (all handles). */
 int64_t lbm_kernel_launches(void);
 
+/* The check() residuals for callers that cannot allocate device memory.
+ * No counterpart in the reference: it is check() (2M:755-805) on the
+ * caller's own device arrays, for hosts that own all device memory (a
+ * Fortran code keeping its fields in OpenACC / CUDA Fortran arrays inside a
+ * reserved pool, a loop that must not trigger an allocation).  It allocates
+ * nothing: the per-block partial sums go to a fixed 256 KiB array in device
+ * memory that every GPU using this library holds until the process exits.
+ * u, v, T (and w in 3D) are device arrays of n doubles; u_prev, v_prev, T_prev
+ * (and w_prev) hold the fields of the previous check and are overwritten with
+ * the current ones; w and w_prev are NULL in 2D.  n may be at most
+ * LBM_NOALLOC_MAX_NODES; larger n is rejected with LBM_ERR_PARAM.  Work runs
+ * on `stream` (a cudaStream_t, NULL for the default stream); the call waits
+ * for it and writes errU, errT on the host.  The first call on each device
+ * looks up the array's device address; make it before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
+#define LBM_NOALLOC_MAX_NODES 67108864LL
+int lbm_check_noalloc(const double *u, const double *v, const double *w,
+                      const double *T, double *u_prev, double *v_prev,
+                      double *w_prev, double *T_prev, int64_t n,
+                      double *errU, double *errT, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

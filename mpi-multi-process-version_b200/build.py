@@ -37,6 +37,7 @@ UNITS = [
     ("kernels_exact.o", "lbm_kernels.cu", ["-DLBM_NS=exact", "-DLBM_EXACT=1", "--fmad=false"]),
     ("reduce.o", "lbm_reduce.cu", ["--fmad=false"]),
     ("capi.o", "lbm_capi.cu", []),
+    ("noalloc.o", "lbm_noalloc.cu", []),
 ]
 
 HEADERS = ["lbm_internal.h"]

@@ -46,6 +46,18 @@ static int fail(int code, const char *fmt, ...)
                         "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
     } while (0)
 
+// error reporting for the other translation units of the library
+int lbm::set_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
 extern "C" int lbm_abi_version(void) { return LBM_ABI_VERSION; }
 
 extern "C" const char *lbm_error_string(int status)

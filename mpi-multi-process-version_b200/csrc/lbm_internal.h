@@ -87,6 +87,9 @@ cudaError_t macro_from_pops(const Geo &g, int store, const void *pop, const Bufs
 
 extern int64_t g_launches;  // kernels launched by this library
 
+// record a message for lbm_last_error() and return code
+int set_error(int code, const char *fmt, ...);
+
 // tile shape of the march kernels (identical in both arithmetic modes)
 MarchShape march_shape(int dim, int store);
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
-    "lbm_set_option", "lbm_get_option",
+    "lbm_set_option", "lbm_get_option", "lbm_check_noalloc",
 ]
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO = 1, 2, 3
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
@@ -90,6 +90,7 @@ def lib():
         L.lbm_kernel_launches.restype = ctypes.c_int64
         L.lbm_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
         L.lbm_get_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_check_noalloc.argtypes = [ctypes.c_void_p] * 8 + [ctypes.c_int64, _dp, _dp, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -108,6 +109,23 @@ def _p(a):
 
 def kernel_launches() -> int:
     return int(lib().lbm_kernel_launches())
+
+
+NOALLOC_MAX_NODES = 67108864
+
+
+def check_noalloc(u, v, w, T, u_prev, v_prev, w_prev, T_prev, n, stream=0):
+    """check() residuals on caller-owned device arrays, without any device
+    allocation by the library (lbm_check_noalloc).  Arguments are device
+    addresses (ints, e.g. a tensor's data_ptr()); w and w_prev are None in 2D.
+    The previous-field arrays are overwritten with the current fields.
+    Returns (errU, errT)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    ptr = lambda x: None if x is None else ctypes.c_void_p(int(x))  # noqa: E731
+    _chk(lib().lbm_check_noalloc(ptr(u), ptr(v), ptr(w), ptr(T), ptr(u_prev), ptr(v_prev), ptr(w_prev),
+                                 ptr(T_prev), int(n), ctypes.byref(a), ctypes.byref(b),
+                                 ctypes.c_void_p(int(stream)) if stream else None), "lbm_check_noalloc")
+    return a.value, b.value
 
 
 # ---------------------------------------------------------------------------

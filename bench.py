@@ -227,6 +227,99 @@ def add_kernel_config(cfg, cav, pkg):
     return cfg
 
 
+def run_batch(args, world, rank, local):
+    """The seeded sweep of 256 2D cavities (widths 64..512, aspect 1-4, Ra
+    1e3..1e6, Pr 0.71..7, tanh stretch 1..2) through one persistent kernel per
+    step, against stepping each cavity with its own launch (FP64)."""
+    import torch
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    specs = pkg.sweep_specs(256, seed=0)
+    b = pkg.Batch(2, specs, storage=args.storage, mode=args.mode, device=local)
+    b.initial()
+    tuned = b.tune(steps=6)
+    stream = torch.cuda.ExternalStream(b.stream_ptr(), device=torch.device("cuda", local))
+
+    def timed(nsteps, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            b.step(nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        b.step(args.inner)
+    b.synchronize()
+    sampler = None
+    if not args.no_clocks and rank == 0:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        sampler = ClockSampler(vis.split(",")[local] if vis else str(local))
+        sampler.start()
+        time.sleep(0.3)
+    l0 = pkg.kernel_launches()
+    ms = timed(args.inner, args.steps)
+    launches = pkg.kernel_launches() - l0
+    clocks = sampler.stop() if sampler else None
+    nodes = b.nodes
+    iters = args.steps * args.inner
+    value = world * nodes * iters / (ms / 1e3) / 1e6
+    # one launch per cavity per step, same batch and precision
+    b.set_option("persistent", 0)
+    b.step(2)
+    base_steps = max(2, args.inner // 10)
+    ms_base = timed(base_steps, 2)
+    baseline = nodes * base_steps * 2 / (ms_base / 1e3) / 1e6
+    b.set_option("persistent", 1)
+    bpl = bytes_per_lup(2, args.storage)
+    peak, peak_kind = measured_peak()
+    achieved = bpl * nodes * iters / (ms / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        # every step: upload each member's initial fields from pinned memory,
+        # advance, read back each member's Nusselt numbers
+        big = max(m.nnode for m in b.members)
+        pin = {k: torch.zeros(big, dtype=torch.float64, pin_memory=True).numpy() for k in ("rho", "u", "v", "T")}
+        pin["rho"][:] = 1.0
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(max(1, args.steps // 4)):
+            for m in b.members:
+                nn = m.nnode
+                m.init_equilibrium(*(pin[k][:nn].reshape(m.shape) for k in ("rho", "u", "v")), None,
+                                   pin["T"][:nn].reshape(m.shape))
+            b.step(args.inner)
+            b.nusselt()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        reps = max(1, args.steps // 4)
+        e2e = {"value": world * nodes * args.inner * reps / (ems / 1e3) / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": 4 * nodes * 8, "d2h_bytes_per_step": 2 * 8 * len(specs),
+               "path": "lbm_init_equilibrium per member (pinned host fields) + lbm_batch_step + lbm_batch_nusselt"}
+    if rank == 0:
+        line = {
+            "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": "batch256", "cavities": len(specs), "nodes": nodes, "lattice": "D2Q9+D2Q5",
+                       "sweep": "widths {64..512}, aspect 1-4, Ra 1e3-1e6 log, Pr 0.71-7, tanh stretch 1-2, seed 0",
+                       "storage": args.storage, "mode": args.mode, "iterations_per_step": args.inner,
+                       "tile": tuned["tile"], "blocks": tuned["nblocks"], "graphs": True,
+                       "one_launch_per_cavity_mlups": baseline,
+                       "speedup_vs_one_launch_per_cavity": value / baseline if baseline else None},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind, "bytes_per_lup": bpl, "kernel": "k_march2d_batch"},
+            "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -234,7 +327,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--inner", type=int, default=100, help="LBM iterations per bench step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS) + ["batch256"])
     ap.add_argument("--storage", default="f64", choices=["f64", "f32", "f16s"])
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -252,6 +345,8 @@ def main():
         run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
         return
     world, rank, local = dist_setup()
+    if args.workload == "batch256":
+        return run_batch(args, world, rank, local)
 
     import torch
     torch.cuda.set_device(local)

@@ -186,6 +186,49 @@ int lbm_device_bytes(const lbm_handle *h, int64_t *bytes);
 /* Number of kernels this library launched since load (all handles). */
 int64_t lbm_kernel_launches(void);
 
+/* ------------------------------------------------------------------------ */
+/* Batches of independent cavities (no counterpart in the reference, which  */
+/* runs one cavity per program; each member behaves as the reference's      */
+/* program main would on its own parameters).                               */
+/* ------------------------------------------------------------------------ */
+typedef struct lbm_batch lbm_batch;
+
+#define LBM_BATCH_OPT_TILE        1  /* tile width of the 2D batch kernel: 32, 64, 128 */
+#define LBM_BATCH_OPT_NBLOCKS     2  /* persistent blocks (0 = one full wave) */
+#define LBM_BATCH_OPT_PERSISTENT  3  /* 1: one persistent kernel per step, 0: one launch per cavity */
+#define LBM_BATCH_OPT_GRAPHS      4  /* 1: replay steps from CUDA graphs */
+
+/* Create n cavities (same dim, storage, mode and device; any size and
+ * parameters).  x[i], y[i], z[i] are the coordinate arrays of cavity i as for
+ * lbm_create; z may be NULL in 2D. */
+int lbm_batch_create(int32_t n, const lbm_params *params, const double *const *x,
+                     const double *const *y, const double *const *z, lbm_batch **out);
+int lbm_batch_destroy(lbm_batch *b);
+int lbm_batch_size(const lbm_batch *b, int32_t *n);
+/* Member i as an ordinary handle (init, check, getters); it runs on the
+ * batch's stream.  Do not destroy it. */
+int lbm_batch_cavity(lbm_batch *b, int32_t i, lbm_handle **h);
+/* lbm_init_reference on every member. */
+int lbm_batch_init_reference(lbm_batch *b);
+/* nsteps iterations of every member (lbm_step semantics; asynchronous). */
+int lbm_batch_step(lbm_batch *b, int32_t nsteps);
+/* Per-member check() residuals / Nusselt numbers into arrays of n. */
+int lbm_batch_check(lbm_batch *b, double *errU, double *errT);
+int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold);
+/* The reference's loop for every member (2M:307-330): step check_every
+ * iterations, check, and retire members whose errorU and errorT are both at
+ * most eps; stop when all are retired or after max_steps.  converged[i] and
+ * steps_done[i] (optional) report each member's outcome. */
+int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps,
+                  int32_t *converged, int64_t *steps_done);
+/* Time each tile width and grid size on the batch itself (the timed steps
+ * advance the members) and keep the fastest; reports the choice. */
+int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups);
+int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value);
+int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t *value);
+int lbm_batch_synchronize(lbm_batch *b);
+int lbm_batch_stream(const lbm_batch *b, void **stream);
+
 /* The check() residuals for callers that cannot allocate device memory.
  * No counterpart in the reference: it is check() (2M:755-805) on the
  * caller's own device arrays, for hosts that own all device memory (a

@@ -1,8 +1,9 @@
 """B200-native thermal lattice-Boltzmann time step (MRT D2Q9/D3Q19 + D2Q5/D3Q7
 ISLBM on stretched grids): the drop-in for the time step of
 zzhao0930/MPI-Multi-Process-Version, behind the C ABI in include/lbm_b200.h."""
-from .lbm import (EXPORTS, GRID, MODE, NOALLOC_MAX_NODES, STORE, Cavity, LBMError, Mesh, check_noalloc, fortran_e,
-                  kernel_launches, lbm_params, lib, mesh, output_ascii, run_main)
+from .lbm import (EXPORTS, GRID, MODE, NOALLOC_MAX_NODES, STORE, Batch, Cavity, LBMError, Mesh, check_noalloc,
+                  fortran_e, kernel_launches, lbm_params, lib, mesh, output_ascii, run_main, sweep_specs)
 
-__all__ = ["EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Cavity", "LBMError", "Mesh", "check_noalloc",
+__all__ = ["EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Batch", "Cavity", "LBMError", "Mesh",
+           "check_noalloc", "sweep_specs",
            "fortran_e", "kernel_launches", "lbm_params", "lib", "mesh", "output_ascii", "run_main"]

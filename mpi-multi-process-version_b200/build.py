@@ -38,9 +38,10 @@ UNITS = [
     ("reduce.o", "lbm_reduce.cu", ["--fmad=false"]),
     ("capi.o", "lbm_capi.cu", []),
     ("noalloc.o", "lbm_noalloc.cu", []),
+    ("batch.o", "lbm_batch.cu", []),
 ]
 
-HEADERS = ["lbm_internal.h"]
+HEADERS = ["lbm_internal.h", "lbm_handle.h", "lbm_march.cuh"]
 
 
 def _stale(target: str, deps: list[str]) -> bool:

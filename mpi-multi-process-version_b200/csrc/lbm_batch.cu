@@ -1,0 +1,508 @@
+// Batches of independent cavities (the parameter-sweep use of the time step).
+//
+// The reference runs one cavity per program (natural-convection_2dim_mono.f90
+// `program main`, 283-380).  A batch holds many cavities of different size and
+// parameters and advances all of them at once:
+//   * 2D batches: one persistent TMA march kernel per step (k_march2d_batch)
+//     walks a work list of segments -- (cavity, column strip, row range) --
+//     that splits the total work into equal contiguous shares, one per block;
+//     the per-cavity geometry, TMA descriptors and buffers come from tables
+//     in device memory;
+//   * steps between checks are replayed from 2-step CUDA graphs;
+//   * lbm_batch_run applies the reference's stop test per cavity (errorU and
+//     errorT at most eps at a check, 2M:307) and drops converged cavities
+//     from the work list;
+//   * lbm_batch_tune times the tile widths and grid sizes on the batch itself
+//     and keeps the fastest;
+//   * 3D batches (and 2D batches with the persistent kernel switched off)
+//     step every cavity with its own kernel launch on the batch's stream.
+// Every member is an ordinary lbm_handle (lbm_batch_cavity) sharing the
+// batch's stream, so initialisation, checks and getters are the single-
+// cavity entry points.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "lbm_handle.h"
+
+using namespace lbm;
+
+#define BCU(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return set_error(e_ == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA, "%s: %s (%s:%d)", \
+                             #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
+    } while (0)
+
+struct lbm_batch {
+    int n = 0;
+    int dim = 2, storage = 0, mode = 0, device = 0;
+    std::vector<lbm_handle *> cav;
+    std::vector<char> active;
+    cudaStream_t stream = nullptr;
+    int tile_opt = 0, tile = 64;   // tile width of the 2D batch kernel (32, 64, 128)
+    int nblocks_opt = 0, nblocks = 0;
+    int persistent = 1;            // 0: one launch per cavity
+    int use_graphs = 1;
+    Geo *d_geo = nullptr;
+    TmapSet *d_maps = nullptr;
+    Bufs *d_bufs = nullptr;
+    int4 *d_segs = nullptr;
+    int *d_segoff = nullptr;
+    int *d_err = nullptr;
+    size_t segs_cap = 0, segoff_cap = 0;
+    BatchDev dev{};
+    bool dirty = true;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t active_nodes = 0;
+};
+
+static void drop_graphs(lbm_batch *b)
+{
+    for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+extern "C" int lbm_batch_destroy(lbm_batch *b)
+{
+    if (!b) return LBM_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graphs(b);
+    for (lbm_handle *h : b->cav) lbm_destroy(h);
+    void *ptrs[] = {b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff, b->d_err};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const double *const *x, const double *const *y,
+                                const double *const *z, lbm_batch **out)
+{
+    if (!out) return set_error(LBM_ERR_PARAM, "out is NULL");
+    *out = nullptr;
+    if (n < 1 || !params || !x || !y) return set_error(LBM_ERR_PARAM, "lbm_batch_create: need n >= 1, params, x, y");
+    for (int i = 1; i < n; ++i)
+        if (params[i].dim != params[0].dim || params[i].storage != params[0].storage ||
+            params[i].mode != params[0].mode || params[i].device != params[0].device)
+            return set_error(LBM_ERR_PARAM, "lbm_batch_create: cavity %d differs in dim/storage/mode/device", i);
+    if (params[0].dim == 3 && !z) return set_error(LBM_ERR_PARAM, "lbm_batch_create: z is required in 3D");
+    lbm_batch *b = new lbm_batch();
+    b->n = n;
+    b->dim = params[0].dim;
+    b->storage = params[0].storage;
+    b->mode = params[0].mode;
+    b->device = params[0].device;
+    auto bail = [&](int code) {
+        lbm_batch_destroy(b);
+        return code;
+    };
+    {
+        cudaError_t e = cudaSetDevice(b->device);
+        if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e)));
+        e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
+    }
+    for (int i = 0; i < n; ++i) {
+        lbm_handle *h = nullptr;
+        int st = lbm_create(&params[i], x[i], y[i], z ? z[i] : nullptr, &h);
+        if (st) return bail(st);
+        cudaStreamDestroy(h->stream);
+        h->stream = b->stream;
+        h->owns_stream = false;
+        b->cav.push_back(h);
+    }
+    b->active.assign(n, 1);
+    if (b->dim == 2) {
+        cudaError_t e = cudaMalloc(&b->d_geo, sizeof(Geo) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_bufs, sizeof(Bufs) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, sizeof(TmapSet) * 2 * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_err, 16);
+        if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, 16);
+        if (e != cudaSuccess) return bail(set_error(LBM_ERR_NOMEM, "batch tables: %s", cudaGetErrorString(e)));
+        std::vector<Geo> geo(n);
+        std::vector<Bufs> bufs(n);
+        for (int i = 0; i < n; ++i) {
+            geo[i] = b->cav[i]->geo;
+            bufs[i] = b->cav[i]->bufs;
+        }
+        e = cudaMemcpy(b->d_geo, geo.data(), sizeof(Geo) * n, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e)));
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+// descriptors for the tile width, and the work list of the active cavities
+static int build_tables(lbm_batch *b)
+{
+    drop_graphs(b);
+    const int TX = b->tile;
+    std::vector<TmapSet> maps(2 * (size_t)b->n);
+    for (int i = 0; i < b->n; ++i)
+        if (!encode_maps_tx(b->cav[i], TX, &maps[2 * (size_t)i]))
+            return set_error(LBM_ERR_UNSUPPORTED, "batch: TMA descriptors for cavity %d could not be encoded", i);
+    BCU(cudaMemcpyAsync(b->d_maps, maps.data(), sizeof(TmapSet) * maps.size(), cudaMemcpyHostToDevice, b->stream));
+
+    struct Col {
+        int cav, i0, ny;
+    };
+    std::vector<Col> cols;
+    int64_t total = 0;
+    b->active_nodes = 0;
+    for (int i = 0; i < b->n; ++i) {
+        if (!b->active[i]) continue;
+        const Geo &g = b->cav[i]->geo;
+        for (int i0 = 0; i0 < g.nx; i0 += TX) cols.push_back({i, i0, g.ny});
+        total += (int64_t)((g.nx + TX - 1) / TX) * g.ny;
+        b->active_nodes += g.nnode;
+    }
+    const int bps = b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, TX)
+                                              : fast::march_batch_blocks_per_sm(b->storage, TX);
+    if (bps <= 0) return set_error(LBM_ERR_UNSUPPORTED, "batch kernel with tile %d cannot be resident", TX);
+    int sms = 0;
+    BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    int64_t G = b->nblocks_opt > 0 ? b->nblocks_opt : (int64_t)bps * sms;
+    if (G > total) G = total;
+    if (G < 1) G = 1;
+    b->nblocks = (int)G;
+    // equal contiguous shares of the (column, row) items
+    std::vector<int4> segs;
+    std::vector<int> off(G + 1, 0);
+    size_t c = 0;
+    int64_t colbase = 0;  // first item of column c
+    for (int64_t blk = 0; blk < G; ++blk) {
+        off[blk] = (int)segs.size();
+        const int64_t lo = total * blk / G, hi = total * (blk + 1) / G;
+        int64_t u = lo;
+        while (u < hi) {
+            while (c < cols.size() && colbase + cols[c].ny <= u) colbase += cols[c++].ny;
+            const int64_t end = std::min<int64_t>(hi, colbase + cols[c].ny);
+            segs.push_back(make_int4(cols[c].cav, cols[c].i0, (int)(u - colbase), (int)(end - colbase)));
+            u = end;
+        }
+    }
+    off[G] = (int)segs.size();
+    if (segs.size() > b->segs_cap) {
+        if (b->d_segs) cudaFree(b->d_segs);
+        b->segs_cap = segs.size() * 2 + 16;
+        BCU(cudaMalloc(&b->d_segs, sizeof(int4) * b->segs_cap));
+    }
+    if (off.size() > b->segoff_cap) {
+        if (b->d_segoff) cudaFree(b->d_segoff);
+        b->segoff_cap = off.size() * 2 + 16;
+        BCU(cudaMalloc(&b->d_segoff, sizeof(int) * b->segoff_cap));
+    }
+    if (!segs.empty())
+        BCU(cudaMemcpyAsync(b->d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaMemcpyAsync(b->d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    b->dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff};
+    b->dirty = false;
+    return LBM_OK;
+}
+
+static cudaError_t launch_step(lbm_batch *b, int cur, int wm)
+{
+    return b->mode == LBM_MODE_EXACT
+               ? exact::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream)
+               : fast::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream);
+}
+
+// a 2-step graph starting from buffer `cur`
+static int get_graph(lbm_batch *b, int cur, cudaGraphExec_t *out)
+{
+    if (!b->graph[cur]) {
+        cudaGraph_t g = nullptr;
+        BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e1 = launch_step(b, cur, 0);
+        cudaError_t e2 = launch_step(b, 1 - cur, 0);
+        cudaError_t e3 = cudaStreamEndCapture(b->stream, &g);
+        g_launches -= 2;  // counted when replayed
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return set_error(LBM_ERR_CUDA, "batch graph capture failed: %s",
+                             cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+        }
+        cudaError_t e = cudaGraphInstantiate(&b->graph[cur], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return set_error(LBM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = b->graph[cur];
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_step(lbm_batch *b, int32_t nsteps)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    if (nsteps < 0) return set_error(LBM_ERR_PARAM, "nsteps < 0");
+    BCU(cudaSetDevice(b->device));
+    if (nsteps == 0) return LBM_OK;
+    for (int i = 0; i < b->n; ++i)
+        if (b->active[i] && b->cav[i]->phase == 0)
+            return set_error(LBM_ERR_STATE, "batch: cavity %d stepped before an init call", i);
+    if (b->dim == 3 || !b->persistent) {
+        for (int i = 0; i < b->n; ++i)
+            if (b->active[i]) {
+                int st = lbm_step(b->cav[i], nsteps);
+                if (st) return st;
+            }
+        return LBM_OK;
+    }
+    int cur = -1;
+    for (int i = 0; i < b->n; ++i) {
+        if (!b->active[i]) continue;
+        int st = first_collision(b->cav[i]);
+        if (st) return st;
+        if (cur < 0) cur = b->cav[i]->cur;
+        if (b->cav[i]->cur != cur)
+            return set_error(LBM_ERR_STATE, "batch: cavity %d is out of step with the others", i);
+    }
+    if (cur < 0) return LBM_OK;  // nothing active
+    if (b->dirty) {
+        int st = build_tables(b);
+        if (st) return st;
+    }
+    int done = 0;
+    // whole 2-step graphs for all but the last step, then the last step with the macroscopic output
+    if (b->use_graphs) {
+        while (nsteps - done > 2) {
+            cudaGraphExec_t g;
+            int st = get_graph(b, cur, &g);
+            if (st) return st;
+            BCU(cudaGraphLaunch(g, b->stream));
+            g_launches += 2;
+            done += 2;
+        }
+    }
+    while (done < nsteps) {
+        BCU(launch_step(b, cur, done == nsteps - 1));
+        cur = 1 - cur;
+        ++done;
+    }
+    // each graph replay flips the buffers twice, each single launch once
+    const int final_cur = cur;
+    for (int i = 0; i < b->n; ++i)
+        if (b->active[i]) {
+            b->cav[i]->cur = final_cur;
+            b->cav[i]->itc += nsteps;
+        }
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_synchronize(lbm_batch *b)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaStreamSynchronize(b->stream));
+    if (b->d_err) {
+        int flag = 0;
+        BCU(cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) {
+            BCU(cudaMemset(b->d_err, 0, sizeof(int)));
+            return set_error(LBM_ERR_TIMEOUT, "batch kernel: a bounded wait for TMA copies gave up");
+        }
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_size(const lbm_batch *b, int32_t *n)
+{
+    if (!b || !n) return set_error(LBM_ERR_PARAM, "NULL argument");
+    *n = b->n;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_cavity(lbm_batch *b, int32_t i, lbm_handle **h)
+{
+    if (!b || !h || i < 0 || i >= b->n) return set_error(LBM_ERR_PARAM, "lbm_batch_cavity: bad index");
+    *h = b->cav[i];
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_init_reference(lbm_batch *b)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    for (lbm_handle *h : b->cav) {
+        int st = lbm_init_reference(h);
+        if (st) return st;
+    }
+    b->active.assign(b->n, 1);
+    b->dirty = true;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_check(lbm_batch *b, double *errU, double *errT)
+{
+    if (!b || !errU || !errT) return set_error(LBM_ERR_PARAM, "NULL argument");
+    int st = lbm_batch_synchronize(b);
+    if (st) return st;
+    for (int i = 0; i < b->n; ++i) {
+        st = lbm_check(b->cav[i], &errU[i], &errT[i]);
+        if (st) return st;
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold)
+{
+    if (!b || !nu_hot || !nu_cold) return set_error(LBM_ERR_PARAM, "NULL argument");
+    int st = lbm_batch_synchronize(b);
+    if (st) return st;
+    for (int i = 0; i < b->n; ++i) {
+        st = lbm_nusselt(b->cav[i], &nu_hot[i], &nu_cold[i]);
+        if (st) return st;
+    }
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps, int32_t *converged,
+                             int64_t *steps_done)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    if (max_steps < 0 || check_every < 1) return set_error(LBM_ERR_PARAM, "need max_steps >= 0, check_every >= 1");
+    std::vector<double> eu(b->n), et(b->n);
+    for (int i = 0; i < b->n; ++i) {
+        if (converged) converged[i] = 0;
+        if (steps_done) steps_done[i] = 0;
+    }
+    b->active.assign(b->n, 1);
+    b->dirty = true;
+    int64_t steps = 0;
+    int remaining = b->n;
+    while (steps < max_steps && remaining > 0) {
+        const int k = (int)std::min<int64_t>(check_every, max_steps - steps);
+        int st = lbm_batch_step(b, k);
+        if (st) return st;
+        steps += k;
+        st = lbm_batch_synchronize(b);
+        if (st) return st;
+        bool changed = false;
+        for (int i = 0; i < b->n; ++i) {
+            if (!b->active[i]) continue;
+            st = lbm_check(b->cav[i], &eu[i], &et[i]);
+            if (st) return st;
+            if (steps_done) steps_done[i] = steps;
+            // the reference keeps iterating while errorU > eps or errorT > eps (2M:307)
+            if (!(eu[i] > eps || et[i] > eps)) {
+                b->active[i] = 0;
+                if (converged) converged[i] = 1;
+                --remaining;
+                changed = true;
+            }
+        }
+        if (changed) b->dirty = true;
+    }
+    b->active.assign(b->n, 1);
+    b->dirty = true;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    if (b->dim != 2) return set_error(LBM_ERR_UNSUPPORTED, "lbm_batch_tune: 2D batches only");
+    if (steps < 2) steps = 2;
+    BCU(cudaSetDevice(b->device));
+    int sms = 0;
+    BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    const int tiles[3] = {32, 64, 128};
+    double best = -1.0;
+    int best_tile = b->tile, best_nb = 0;
+    cudaEvent_t e0, e1;
+    BCU(cudaEventCreate(&e0));
+    BCU(cudaEventCreate(&e1));
+    const int keep_nb = b->nblocks_opt;
+    for (int t : tiles) {
+        const int bps = b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, t)
+                                                  : fast::march_batch_blocks_per_sm(b->storage, t);
+        if (bps <= 0) continue;
+        const int cands[2] = {bps, bps > 1 ? bps / 2 : 0};
+        for (int c : cands) {
+            if (c <= 0) continue;
+            b->tile = t;
+            b->nblocks_opt = c * sms;
+            b->dirty = true;
+            int st = lbm_batch_step(b, 2);  // warm-up, builds the tables
+            if (st) return st;
+            BCU(cudaEventRecord(e0, b->stream));
+            st = lbm_batch_step(b, steps);
+            if (st) return st;
+            BCU(cudaEventRecord(e1, b->stream));
+            st = lbm_batch_synchronize(b);
+            if (st) return st;
+            float ms = 0.f;
+            BCU(cudaEventElapsedTime(&ms, e0, e1));
+            const double v = (double)b->active_nodes * steps / (ms * 1e-3) / 1e6;
+            if (v > best) {
+                best = v;
+                best_tile = t;
+                best_nb = b->nblocks_opt;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tile = best_tile;
+    b->tile_opt = best_tile;
+    b->nblocks_opt = keep_nb > 0 ? keep_nb : best_nb;
+    b->dirty = true;
+    if (tile) *tile = best_tile;
+    if (nblocks) *nblocks = best_nb;
+    if (mlups) *mlups = best;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    switch (option) {
+    case LBM_BATCH_OPT_TILE:
+        if (value != 32 && value != 64 && value != 128) return set_error(LBM_ERR_PARAM, "tile must be 32, 64 or 128");
+        b->tile = b->tile_opt = (int)value;
+        break;
+    case LBM_BATCH_OPT_NBLOCKS:
+        if (value < 0 || value > (1 << 20)) return set_error(LBM_ERR_PARAM, "nblocks out of range");
+        b->nblocks_opt = (int)value;
+        break;
+    case LBM_BATCH_OPT_PERSISTENT:
+        b->persistent = value != 0;
+        break;
+    case LBM_BATCH_OPT_GRAPHS:
+        b->use_graphs = value != 0;
+        break;
+    default:
+        return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
+    }
+    b->dirty = true;
+    return LBM_OK;
+}
+
+extern "C" int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t *value)
+{
+    if (!b || !value) return set_error(LBM_ERR_PARAM, "NULL argument");
+    switch (option) {
+    case LBM_BATCH_OPT_TILE: *value = b->tile; return LBM_OK;
+    case LBM_BATCH_OPT_NBLOCKS: *value = b->nblocks; return LBM_OK;
+    case LBM_BATCH_OPT_PERSISTENT: *value = b->persistent; return LBM_OK;
+    case LBM_BATCH_OPT_GRAPHS: *value = b->use_graphs; return LBM_OK;
+    default: return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
+    }
+}
+
+extern "C" int lbm_batch_stream(const lbm_batch *b, void **stream)
+{
+    if (!b || !stream) return set_error(LBM_ERR_PARAM, "NULL argument");
+    *stream = (void *)b->stream;
+    return LBM_OK;
+}

@@ -17,7 +17,7 @@
 #include <vector>
 
 #include "../../include/lbm_b200.h"
-#include "lbm_internal.h"
+#include "lbm_handle.h"
 
 using namespace lbm;
 
@@ -126,10 +126,6 @@ extern "C" int lbm_mesh(int32_t kind, double stretch, int32_t nx, int32_t ny, in
     return LBM_OK;
 }
 
-struct Derived {
-    double viscosity_LB, kappa, gbeta, tauf, Snu, Sq, sig_k;
-};
-
 static Derived derive(const lbm_params &p)
 {
     // 2M:152-162 and 3M:207-229
@@ -214,37 +210,6 @@ static void cell_widths(const double *c, int n, double dt, double *wd)
     }
 }
 
-// ---------------------------------------------------------------------------
-// handle
-// ---------------------------------------------------------------------------
-struct lbm_handle {
-    lbm_params p;
-    Derived d;
-    int Q, QT;
-    int device;
-    size_t esize, csize;      // storage / compute element size
-    Geo geo;
-    Bufs bufs;
-    std::vector<double> coord[3];
-    double *d_wgt[3] = {nullptr, nullptr, nullptr};
-    double *d_coord[3] = {nullptr, nullptr, nullptr};
-    double *d_cellw[3] = {nullptr, nullptr, nullptr};
-    void *staging = nullptr;     // population planes for stream-only output
-    double *aos = nullptr;       // Fortran-layout staging
-    cudaStream_t stream = nullptr;
-    TmapSet tmaps[2];            // TMA descriptors of pop[0] and pop[1]
-    bool march_ok = false;       // tile shape and descriptors usable
-    int kernel_opt = 0;          // LBM_OPT_KERNEL as set
-    int use_march = 0;           // resolved choice
-    int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
-    int nblocks = 0;             // resolved persistent grid
-    int l2promo = 0;             // LBM_OPT_L2PROMO
-    int cur = 0;                 // buffer holding the newest populations
-    int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
-    int64_t itc = 0;
-    int64_t bytes = 0;
-};
-
 static int set_device(const lbm_handle *h)
 {
     CU(cudaSetDevice(h->device));
@@ -273,7 +238,7 @@ static void free_all(lbm_handle *h)
                     h->aos, h->bufs.err};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream && h->owns_stream) cudaStreamDestroy(h->stream);
 }
 
 extern "C" int lbm_destroy(lbm_handle *h)
@@ -310,12 +275,12 @@ static EncodeTiledFn encode_fn()
 
 // Describe a population buffer as a (x, y, [z,] plane) tensor; one descriptor
 // per box class of the march kernel.  Returns false if TMA cannot be used.
-static bool encode_maps(lbm_handle *h)
+bool lbm::encode_maps_tx(const lbm_handle *h, int tx, TmapSet out[2])
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     const Geo &g = h->geo;
-    const MarchShape ms = march_shape(g.dim, h->p.storage);
+    const MarchShape ms = march_shape(g.dim, h->p.storage, tx);
     const CUtensorMapDataType dtype = h->p.storage == LBM_STORE_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                       : h->p.storage == LBM_STORE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
@@ -327,7 +292,7 @@ static bool encode_maps(lbm_handle *h)
                                                            : CU_TENSOR_MAP_L2_PROMOTION_NONE;
     for (int buf = 0; buf < 2; ++buf) {
         for (int c = 0; c < 4; ++c) {
-            CUtensorMap *m = &h->tmaps[buf].m[c];
+            CUtensorMap *m = &out[buf].m[c];
             CUresult r;
             if (g.dim == 3) {
                 const cuuint64_t dims[4] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)g.nz, (cuuint64_t)nplanes};
@@ -358,20 +323,22 @@ static bool encode_maps(lbm_handle *h)
             const cuuint64_t strides[2] = {(cuuint64_t)g.pitch * cs, (cuuint64_t)g.slab * cs};
             const cuuint32_t box[3] = {(cuuint32_t)ms.TX, (cuuint32_t)ms.TY, 1};
             const cuuint32_t estr[3] = {1, 1, 1};
-            r = enc(&h->tmaps[buf].fmap, ftype, 3, h->bufs.F[buf], dims, strides, box, estr,
+            r = enc(&out[buf].fmap, ftype, 3, h->bufs.F[buf], dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         } else {
             const cuuint64_t dims[2] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny};
             const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * cs};
             const cuuint32_t box[2] = {(cuuint32_t)ms.TX, 1};
             const cuuint32_t estr[2] = {1, 1};
-            r = enc(&h->tmaps[buf].fmap, ftype, 2, h->bufs.F[buf], dims, strides, box, estr,
+            r = enc(&out[buf].fmap, ftype, 2, h->bufs.F[buf], dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         }
         if (r != CUDA_SUCCESS) return false;
     }
     return true;
 }
+
+static bool encode_maps(lbm_handle *h) { return lbm::encode_maps_tx(h, 0, h->tmaps); }
 
 // The march kernel handles every size except, in 3D, a last tile row holding
 // a single y-row (its one-sided stencil would reach two rows below the box).
@@ -605,6 +572,20 @@ extern "C" int lbm_init_equilibrium(lbm_handle *h, const double *rho, const doub
     return LBM_OK;
 }
 
+int lbm::first_collision(lbm_handle *h)
+{
+    if (h->phase != 1) return LBM_OK;
+    // first collision of the run, from the pre-collision state
+    const bool ex = h->p.mode == LBM_MODE_EXACT;
+    Bufs &b = h->bufs;
+    const int nxt = 1 - h->cur;
+    CU(ex ? exact::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream)
+          : fast::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream));
+    h->cur = nxt;
+    h->phase = 2;
+    return LBM_OK;
+}
+
 extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
 {
     CHECK_H(h);
@@ -613,14 +594,8 @@ extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
     if (nsteps == 0) return LBM_OK;
     const bool ex = h->p.mode == LBM_MODE_EXACT;
     Bufs &b = h->bufs;
-    if (h->phase == 1) {
-        // first collision of the run, from the pre-collision state
-        const int nxt = 1 - h->cur;
-        CU(ex ? exact::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream)
-              : fast::collide(h->geo, h->p.storage, b.pop[h->cur], b.pop[nxt], b.F[nxt], b, h->stream));
-        h->cur = nxt;
-        h->phase = 2;
-    }
+    int st = lbm::first_collision(h);
+    if (st) return st;
     for (int s = 0; s < nsteps; ++s) {
         const int nxt = 1 - h->cur;
         const int wm = (s == nsteps - 1);
@@ -660,6 +635,8 @@ static int sync_and_check(lbm_handle *h)
     }
     return LBM_OK;
 }
+
+int lbm::sync_handle(lbm_handle *h) { return sync_and_check(h); }
 
 static int read_scal(lbm_handle *h, int first, int count, double *out)
 {

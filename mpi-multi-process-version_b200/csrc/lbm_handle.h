@@ -1,0 +1,62 @@
+// Internal: the cavity handle behind the C ABI, shared by lbm_capi.cu and
+// lbm_batch.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_internal.h"
+
+struct Derived {
+    double viscosity_LB, kappa, gbeta, tauf, Snu, Sq, sig_k;
+};
+
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+struct lbm_handle {
+    using Geo = lbm::Geo;
+    using Bufs = lbm::Bufs;
+    using TmapSet = lbm::TmapSet;
+    lbm_params p;
+    Derived d;
+    int Q, QT;
+    int device;
+    size_t esize, csize;      // storage / compute element size
+    Geo geo;
+    Bufs bufs;
+    std::vector<double> coord[3];
+    double *d_wgt[3] = {nullptr, nullptr, nullptr};
+    double *d_coord[3] = {nullptr, nullptr, nullptr};
+    double *d_cellw[3] = {nullptr, nullptr, nullptr};
+    void *staging = nullptr;     // population planes for stream-only output
+    double *aos = nullptr;       // Fortran-layout staging
+    cudaStream_t stream = nullptr;
+    bool owns_stream = true;     // false for members of a batch (the batch's stream)
+    TmapSet tmaps[2];            // TMA descriptors of pop[0] and pop[1]
+    bool march_ok = false;       // tile shape and descriptors usable
+    int kernel_opt = 0;          // LBM_OPT_KERNEL as set
+    int use_march = 0;           // resolved choice
+    int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
+    int nblocks = 0;             // resolved persistent grid
+    int l2promo = 0;             // LBM_OPT_L2PROMO
+    int cur = 0;                 // buffer holding the newest populations
+    int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
+    int64_t itc = 0;
+    int64_t bytes = 0;
+};
+
+
+// helpers of lbm_capi.cu used by the batch
+namespace lbm {
+// encode the TMA descriptors of h's two population buffers for the march
+// kernel with tile width tx (0: the single-cavity default); false if TMA
+// cannot be used
+bool encode_maps_tx(const lbm_handle *h, int tx, lbm::TmapSet out[2]);
+// the first collision of a run if h is still in its pre-collision state
+int first_collision(lbm_handle *h);
+// synchronise h's stream and report a kernel's bounded wait that gave up
+int sync_handle(lbm_handle *h);
+}  // namespace lbm

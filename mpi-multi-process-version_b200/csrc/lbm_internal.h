@@ -38,6 +38,15 @@ struct alignas(64) TmapSet {
     CUtensorMap fmap;
 };
 
+// Per-cavity tables of a batch of 2D cavities (device memory)
+struct BatchDev {
+    const Geo *geo;          // [ncav]
+    const TmapSet *maps;     // [ncav][2]: descriptors of pop[0], pop[1] (+ their force arrays)
+    const Bufs *bufs;        // [ncav]
+    const int4 *segs;        // all segments: (cavity, i0, ja, jb)
+    const int *seg_off;      // [nblocks + 1]
+};
+
 // shape of the march kernels' tiles for a lattice and storage (host side)
 struct MarchShape {
     int TX, TY, HX, threads, smem;
@@ -67,6 +76,10 @@ enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
                       cudaStream_t s);                                                        \
     /* resident blocks per SM of the march kernel (0 if it cannot launch) */                  \
     int march_blocks_per_sm(const Geo &g, int store);                                         \
+    /* one step of every cavity of a 2D batch (tile width TX = 32, 64 or 128) */              \
+    cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur,       \
+                            int write_macro, int *err, cudaStream_t s);                       \
+    int march_batch_blocks_per_sm(int store, int TX);                                         \
     }
 
 LBM_DECLARE_LAUNCHERS(fast)
@@ -90,7 +103,8 @@ extern int64_t g_launches;  // kernels launched by this library
 // record a message for lbm_last_error() and return code
 int set_error(int code, const char *fmt, ...);
 
-// tile shape of the march kernels (identical in both arithmetic modes)
-MarchShape march_shape(int dim, int store);
+// tile shape of the march kernels (identical in both arithmetic modes); tx
+// selects the tile width of the 2D kernels (0: the single-cavity default)
+MarchShape march_shape(int dim, int store, int tx = 0);
 
 }  // namespace lbm

@@ -1035,11 +1035,82 @@ cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in,
 #undef CALL
 }
 
+template <int ST, int TX>
+static cudaError_t prepare_batch()
+{
+    static bool done = false;
+    if (!done) {
+        cudaError_t e = cudaFuncSetAttribute(k_march2d_batch<ST, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L2<ST, TX>::smem());
+        if (e != cudaSuccess) return e;
+        done = true;
+    }
+    return cudaSuccess;
+}
+
+template <int ST, int TX>
+static cudaError_t launch_batch(const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+{
+    cudaError_t e = prepare_batch<ST, TX>();
+    if (e != cudaSuccess) return e;
+    k_march2d_batch<ST, TX><<<nblocks, TX, L2<ST, TX>::smem(), s>>>(D, cur, wm, err);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+template <int ST, int TX>
+static int batch_bps()
+{
+    if (prepare_batch<ST, TX>() != cudaSuccess) return 0;
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d_batch<ST, TX>, TX, L2<ST, TX>::smem()) ==
+                   cudaSuccess
+               ? n
+               : 0;
+}
+
+template <int ST>
+static cudaError_t launch_batch_tx(int TX, const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+{
+    switch (TX) {
+    case 32: return launch_batch<ST, 32>(D, nblocks, cur, wm, err, s);
+    case 64: return launch_batch<ST, 64>(D, nblocks, cur, wm, err, s);
+    case 128: return launch_batch<ST, 128>(D, nblocks, cur, wm, err, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int ST>
+static int batch_bps_tx(int TX)
+{
+    switch (TX) {
+    case 32: return batch_bps<ST, 32>();
+    case 64: return batch_bps<ST, 64>();
+    case 128: return batch_bps<ST, 128>();
+    default: return 0;
+    }
+}
+
+cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur, int write_macro, int *err,
+                        cudaStream_t s)
+{
+#define CALL(ST) launch_batch_tx<ST>(TX, D, nblocks, cur, write_macro, err, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+int march_batch_blocks_per_sm(int store, int TX)
+{
+#define CALL(ST) batch_bps_tx<ST>(TX)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
 }  // namespace LBM_NS
 
 #if !LBM_EXACT
 // tile shapes of the march kernels, for the host's tensor-map encoding
-MarchShape march_shape(int dim, int store)
+MarchShape march_shape(int dim, int store, int tx)
 {
     MarchShape m{};
     auto fill = [&](auto layout, int dims) {
@@ -1061,11 +1132,16 @@ MarchShape march_shape(int dim, int store)
             m.by[c] = m.TY + ((c & 2) ? 2 : 0);
         }
     } else {
-        switch (store) {
-        case kF64: fill(fast::L2<kF64>{}, 2); break;
-        case kF32: fill(fast::L2<kF32>{}, 2); break;
-        default: fill(fast::L2<kF16S>{}, 2); break;
+#define LBM_FILL2(TXV)                                                    \
+        switch (store) {                                                  \
+        case kF64: fill(fast::L2<kF64, TXV>{}, 2); break;                 \
+        case kF32: fill(fast::L2<kF32, TXV>{}, 2); break;                 \
+        default: fill(fast::L2<kF16S, TXV>{}, 2); break;                  \
         }
+        if (tx == 32) { LBM_FILL2(32) }
+        else if (tx == 64) { LBM_FILL2(64) }
+        else { LBM_FILL2(128) }
+#undef LBM_FILL2
         for (int c = 0; c < 4; ++c) {
             m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);
             m.by[c] = 1;

@@ -426,12 +426,12 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 // ---------------------------------------------------------------------------
 // 2D layout: a tile is TX nodes of one row; the march runs along y
 // ---------------------------------------------------------------------------
-template <int ST>
+template <int ST, int TX_ = 128>
 struct L2 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
-    static constexpr int TX = 128, NT = TX;
+    static constexpr int TX = TX_, NT = TX;
     static constexpr int HX = 16 / ES;
     __host__ __device__ static constexpr int bx(int c) { return TX + (c ? 2 * HX : 0); }
     __host__ __device__ static constexpr int bytes(int c) { return bx(c) * ES; }
@@ -480,16 +480,120 @@ struct L2 {
     __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + 128; }
 };
 
-template <int ST>
-__global__ void __launch_bounds__(128, 4)
-k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
-          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
-          int write_macro, int64_t total, int *err)
+// One node of the 2D march at row j, from the ring slots in shared memory:
+// interpolation, walls, macro, collision, stores.
+template <int ST, int TX>
+__device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo &G, int tx, int i, int j, int xa,
+                                             int xb, const typename Tr<ST>::C *xp, const typename Tr<ST>::C *xm,
+                                             typename Tr<ST>::S *__restrict__ dst,
+                                             typename Tr<ST>::C *__restrict__ Fout, const Bufs &B, int write_macro)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    using L = L2<ST>;
-    constexpr int TX = L::TX, HX = L::HX;
+    using L = L2<ST, TX>;
+    constexpr int HX = L::HX;
+    const int ny = G.ny;
+    const int64_t P = G.plane;
+    const int64_t id = (int64_t)j * G.pitch + i;
+    const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
+    const unsigned char *nslot_j = sm + 4 * L::yslot() + (j & 1) * L::nslot();
+    const C Fy0 = ((const C *)(nslot_j + L::fo()))[tx];
+    const double *wy = (const double *)(nslot_j + L::wo());
+    const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
+    auto SV = [&](const unsigned char *box, int idx, int q) -> C {
+        C val = tocomp(((const S *)box)[idx]);
+        if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        return val;
+    };
+    auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
+    auto NB = [&](int ni) -> const unsigned char * { return nslot_j + L::noff(ni); };
+    auto ix = [&](int c, int dx) -> int { return tx + (c ? HX : 0) + dx; };
+    // y-interpolation of a y-ring plane at x-offset dx
+    auto YI = [&](int yi, int q, const C *w, int dx) -> C {
+        const int c = L::yc(yi);
+        const int e = ix(c, dx);
+        return ip(w, SV(YB(yi, ja_), e, q), SV(YB(yi, j), e, q), SV(YB(yi, jb_), e, q));
+    };
+    C f[9], gg[5];
+    f[0] = SV(NB(0), ix(0, 0), 0);
+    f[1] = ip(xp, SV(NB(1), ix(1, xa), 1), SV(NB(1), ix(1, 0), 1), SV(NB(1), ix(1, xb), 1));
+    f[2] = YI(0, 2, yp, 0);
+    f[3] = ip(xm, SV(NB(2), ix(1, xa), 3), SV(NB(2), ix(1, 0), 3), SV(NB(2), ix(1, xb), 3));
+    f[4] = YI(1, 4, ym, 0);
+    f[5] = ip(xp, YI(2, 5, yp, xa), YI(2, 5, yp, 0), YI(2, 5, yp, xb));
+    f[6] = ip(xm, YI(3, 6, yp, xa), YI(3, 6, yp, 0), YI(3, 6, yp, xb));
+    f[7] = ip(xm, YI(4, 7, ym, xa), YI(4, 7, ym, 0), YI(4, 7, ym, xb));
+    f[8] = ip(xp, YI(5, 8, ym, xa), YI(5, 8, ym, 0), YI(5, 8, ym, xb));
+    gg[0] = SV(NB(3), ix(0, 0), 9);
+    gg[1] = ip(xp, SV(NB(4), ix(1, xa), 10), SV(NB(4), ix(1, 0), 10), SV(NB(4), ix(1, xb), 10));
+    gg[2] = YI(6, 11, yp, 0);
+    gg[3] = ip(xm, SV(NB(5), ix(1, xa), 12), SV(NB(5), ix(1, 0), 12), SV(NB(5), ix(1, xb), 12));
+    gg[4] = YI(7, 13, ym, 0);
+
+    // walls (2B:731-801): centre values of row j
+    auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0), q); };
+    auto CY = [&](int yi, int q) -> C { return SV(YB(yi, j), ix(L::yc(yi), 0), q); };
+    const C two_wT = C(2.0) * C(0.125);
+    if (i == 0) {
+        f[1] = CN(2, 3); f[5] = CY(4, 7); f[8] = CY(3, 6);
+        gg[1] = -CN(5, 12) + two_wT * C(G.Thot);
+    }
+    if (i == G.nx - 1) {
+        f[3] = CN(1, 1); f[6] = CY(5, 8); f[7] = CY(2, 5);
+        gg[3] = -CN(4, 10) + two_wT * C(G.Tcold);
+    }
+    if (j == ny - 1) {
+        f[4] = CY(0, 2); f[7] = CY(2, 5); f[8] = CY(3, 6);
+        gg[4] = CY(6, 11);
+    }
+    if (j == 0) {
+        f[2] = CY(1, 4); f[5] = CY(4, 7); f[6] = CY(5, 8);
+        gg[2] = CY(7, 13);
+    }
+
+    const C dt = C(G.dt);
+    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+#if LBM_EXACT
+    const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
+    const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
+#else
+    const C rinv = C(1.0) / rho;
+    const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
+    const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
+#endif
+    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+    if (write_macro) {
+        const int64_t mid = (int64_t)j * G.nx + i;
+        B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
+    }
+    C fp[9], gp[5], Fy;
+    collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    Fout[id] = Fy;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        C val = fp[q];
+        if (Tr<ST>::kShift) val -= C(wU2(q));
+        dst[q * P + id] = tostore<S, C>(val);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        C val = gp[q];
+        if (Tr<ST>::kShift) val -= C(wT2(q)) * C(G.T0);
+        dst[(9 + q) * P + id] = tostore<S, C>(val);
+    }
+}
+
+// The 2D march over a list of segments (a cavity, a TX-wide column strip at
+// x-offset i0, rows [ja, jb)).  `seg(k, cav, i0, ja, jb)` yields the block's
+// k-th segment; `cavity(cav, G, maps, dst, Fout, B)` yields the cavity's
+// geometry, the TMA descriptors of its source buffer and its outputs.
+template <int ST, int TX, class SegFn, class CavFn>
+__device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, int write_macro, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    using L = L2<ST, TX>;
+    constexpr int HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
     uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
@@ -498,7 +602,6 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 
     const int tid = threadIdx.x;
     const int tx = tid;
-    const int ny = G.ny;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
@@ -508,50 +611,52 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     __syncthreads();
 
     uint32_t ynext = 0, nnext = 0;
-    int i0 = 0;
-    auto issue_y = [&](int s) {
-        const int slot = s & 3;
-        if (tid == 0) {
-            uint64_t *bar = &ybar[slot];
-            mbar_arrive_tx(bar, L::ytx());
-            unsigned char *base = sm + slot * L::yslot();
-#pragma unroll
-            for (int yi = 0; yi < 8; ++yi) {
-                const int c = L::yc(yi);
-                tma_load3(base + L::yoff(yi), &maps.m[c], bar, i0 - (c ? HX : 0), s, L::yq(yi));
-            }
-        }
-        ynext ^= 1u << slot;
-    };
-    auto issue_n = [&](int s) {
-        const int slot = s & 1;
-        if (tid == 0) {
-            uint64_t *bar = &nbar[slot];
-            mbar_arrive_tx(bar, L::ntx());
-            unsigned char *base = sm + 4 * L::yslot() + slot * L::nslot();
-#pragma unroll
-            for (int ni = 0; ni < 6; ++ni) {
-                const int c = L::nc(ni);
-                tma_load3(base + L::noff(ni), &maps.m[c], bar, i0 - (c ? HX : 0), s, L::nq(ni));
-            }
-            tma_load2(base + L::fo(), &maps.fmap, bar, i0, s);
-            bulk_load(base + L::wo(), G.wgt[1] + (int64_t)s * 6, 48, bar);
-        }
-        nnext ^= 1u << slot;
-    };
-    auto wait_y = [&](int s) -> bool { return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u); };
-    auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
-
-    const int64_t G_ = gridDim.x;
-    const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
-    const int64_t P = G.plane;
     bool aborted = false;
+    for (int k = 0; k < nseg && !aborted; ++k) {
+        int cav, i0, ja, jb;
+        seg(k, cav, i0, ja, jb);
+        const Geo *Gp;
+        const CUtensorMap *maps;
+        S *dst;
+        C *Fout;
+        const Bufs *Bp;
+        cavity(cav, Gp, maps, dst, Fout, Bp);
+        const Geo &G = *Gp;
+        const int ny = G.ny;
 
-    for (int64_t u = ubeg; u < uend && !aborted;) {
-        const int64_t t = u / ny;
-        const int ja = int(u % ny);
-        const int jb = int(ja + ((uend - u) < (ny - ja) ? (uend - u) : (ny - ja)));
-        i0 = int(t) * TX;
+        auto issue_y = [&](int s) {
+            const int slot = s & 3;
+            if (tid == 0) {
+                uint64_t *bar = &ybar[slot];
+                mbar_arrive_tx(bar, L::ytx());
+                unsigned char *base = sm + slot * L::yslot();
+#pragma unroll
+                for (int yi = 0; yi < 8; ++yi) {
+                    const int c = L::yc(yi);
+                    tma_load3(base + L::yoff(yi), &maps[c], bar, i0 - (c ? HX : 0), s, L::yq(yi));
+                }
+            }
+            ynext ^= 1u << slot;
+        };
+        auto issue_n = [&](int s) {
+            const int slot = s & 1;
+            if (tid == 0) {
+                uint64_t *bar = &nbar[slot];
+                mbar_arrive_tx(bar, L::ntx());
+                unsigned char *base = sm + 4 * L::yslot() + slot * L::nslot();
+#pragma unroll
+                for (int ni = 0; ni < 6; ++ni) {
+                    const int c = L::nc(ni);
+                    tma_load3(base + L::noff(ni), &maps[c], bar, i0 - (c ? HX : 0), s, L::nq(ni));
+                }
+                tma_load2(base + L::fo(), &maps[4], bar, i0, s);
+                bulk_load(base + L::wo(), G.wgt[1] + (int64_t)s * 6, 48, bar);
+            }
+            nnext ^= 1u << slot;
+        };
+        auto wait_y = [&](int s) -> bool { return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u); };
+        auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
+
         const int pre_lo = need_lo(ja, ny), pre_hi = need_hi(ja, ny);
         const int seg_hi = need_hi(jb - 1, ny) > pre_hi ? need_hi(jb - 1, ny) : pre_hi;
         for (int s = pre_lo; s <= pre_hi; ++s) issue_y(s);
@@ -572,8 +677,6 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 yissued = j + 2;
             }
             if (j + 1 < jb) issue_n(j + 1);
-
-            const int64_t id = (int64_t)j * G.pitch + i;
             bool ok = true;
             for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
             ok = ok && wait_n(j);
@@ -581,106 +684,79 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 atomicExch(err, 1);
                 s_abort = 1;
             }
-            if (active && ok) {
-                const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
-                const unsigned char *nslot_j = sm + 4 * L::yslot() + (j & 1) * L::nslot();
-                const C Fy0 = ((const C *)(nslot_j + L::fo()))[tx];
-                const double *wy = (const double *)(nslot_j + L::wo());
-                const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
-                auto SV = [&](const unsigned char *box, int idx, int q) -> C {
-                    C val = tocomp(((const S *)box)[idx]);
-                    if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
-                    return val;
-                };
-                auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
-                auto NB = [&](int ni) -> const unsigned char * {
-                    return sm + 4 * L::yslot() + (j & 1) * L::nslot() + L::noff(ni);
-                };
-                auto ix = [&](int c, int dx) -> int { return tx + (c ? HX : 0) + dx; };
-                // y-interpolation of a y-ring plane at x-offset dx
-                auto YI = [&](int yi, int q, const C *w, int dx) -> C {
-                    const int c = L::yc(yi);
-                    const int e = ix(c, dx);
-                    return ip(w, SV(YB(yi, ja_), e, q), SV(YB(yi, j), e, q), SV(YB(yi, jb_), e, q));
-                };
-                C f[9], gg[5];
-                f[0] = SV(NB(0), ix(0, 0), 0);
-                f[1] = ip(xp, SV(NB(1), ix(1, xa), 1), SV(NB(1), ix(1, 0), 1), SV(NB(1), ix(1, xb), 1));
-                f[2] = YI(0, 2, yp, 0);
-                f[3] = ip(xm, SV(NB(2), ix(1, xa), 3), SV(NB(2), ix(1, 0), 3), SV(NB(2), ix(1, xb), 3));
-                f[4] = YI(1, 4, ym, 0);
-                f[5] = ip(xp, YI(2, 5, yp, xa), YI(2, 5, yp, 0), YI(2, 5, yp, xb));
-                f[6] = ip(xm, YI(3, 6, yp, xa), YI(3, 6, yp, 0), YI(3, 6, yp, xb));
-                f[7] = ip(xm, YI(4, 7, ym, xa), YI(4, 7, ym, 0), YI(4, 7, ym, xb));
-                f[8] = ip(xp, YI(5, 8, ym, xa), YI(5, 8, ym, 0), YI(5, 8, ym, xb));
-                gg[0] = SV(NB(3), ix(0, 0), 9);
-                gg[1] = ip(xp, SV(NB(4), ix(1, xa), 10), SV(NB(4), ix(1, 0), 10), SV(NB(4), ix(1, xb), 10));
-                gg[2] = YI(6, 11, yp, 0);
-                gg[3] = ip(xm, SV(NB(5), ix(1, xa), 12), SV(NB(5), ix(1, 0), 12), SV(NB(5), ix(1, xb), 12));
-                gg[4] = YI(7, 13, ym, 0);
-
-                // walls (2B:731-801): centre values of row j
-                auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0), q); };
-                auto CY = [&](int yi, int q) -> C { return SV(YB(yi, j), ix(L::yc(yi), 0), q); };
-                const C two_wT = C(2.0) * C(0.125);
-                if (i == 0) {
-                    f[1] = CN(2, 3); f[5] = CY(4, 7); f[8] = CY(3, 6);
-                    gg[1] = -CN(5, 12) + two_wT * C(G.Thot);
-                }
-                if (i == G.nx - 1) {
-                    f[3] = CN(1, 1); f[6] = CY(5, 8); f[7] = CY(2, 5);
-                    gg[3] = -CN(4, 10) + two_wT * C(G.Tcold);
-                }
-                if (j == ny - 1) {
-                    f[4] = CY(0, 2); f[7] = CY(2, 5); f[8] = CY(3, 6);
-                    gg[4] = CY(6, 11);
-                }
-                if (j == 0) {
-                    f[2] = CY(1, 4); f[5] = CY(4, 7); f[6] = CY(5, 8);
-                    gg[2] = CY(7, 13);
-                }
-
-                const C dt = C(G.dt);
-                const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
-#if LBM_EXACT
-                const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
-                const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
-#else
-                const C rinv = C(1.0) / rho;
-                const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
-                const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
-#endif
-                const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
-                if (write_macro) {
-                    const int64_t mid = (int64_t)j * G.nx + i;
-                    B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
-                }
-                C fp[9], gp[5], Fy;
-                collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
-                Fout[id] = Fy;
-#pragma unroll
-                for (int q = 0; q < 9; ++q) {
-                    C val = fp[q];
-                    if (Tr<ST>::kShift) val -= C(wU2(q));
-                    dst[q * P + id] = tostore<S, C>(val);
-                }
-#pragma unroll
-                for (int q = 0; q < 5; ++q) {
-                    C val = gp[q];
-                    if (Tr<ST>::kShift) val -= C(wT2(q)) * C(G.T0);
-                    dst[(9 + q) * P + id] = tostore<S, C>(val);
-                }
-            }
+            if (active && ok) march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, dst, Fout, *Bp, write_macro);
             __syncthreads();
             if (s_abort) {
                 aborted = true;
                 break;
             }
         }
-        u += jb - ja;
     }
     if (aborted && tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
         for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
     }
+}
+
+// one cavity: each block takes an equal contiguous share of the
+// (strip-major, row-minor) work items
+template <int ST>
+__global__ void __launch_bounds__(128, 4)
+k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
+          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+          int write_macro, int64_t total, int *err)
+{
+    (void)Fin;
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    constexpr int TX = L2<ST, 128>::TX;
+    const int ny = G.ny;
+    const int64_t G_ = gridDim.x;
+    const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
+    // segments: the block's range split at strip boundaries
+    const int nseg = ubeg >= uend ? 0 : int((uend - 1) / ny - ubeg / ny + 1);
+    auto seg = [&](int k, int &cav, int &i0, int &ja, int &jb) {
+        const int64_t t = ubeg / ny + k;
+        const int64_t lo = t * ny > ubeg ? t * ny : ubeg;
+        const int64_t hi = (t + 1) * ny < uend ? (t + 1) * ny : uend;
+        cav = 0;
+        i0 = int(t) * TX;
+        ja = int(lo - t * ny);
+        jb = int(hi - t * ny);
+    };
+    const CUtensorMap *mp = &maps.m[0];
+    auto cavity = [&](int, const Geo *&Gp, const CUtensorMap *&m, S *&d, C *&Fo, const Bufs *&Bp) {
+        Gp = &G;
+        m = mp;
+        d = dst;
+        Fo = Fout;
+        Bp = &B;
+    };
+    march2d_run<ST, TX>(nseg, seg, cavity, write_macro, err);
+}
+
+// many cavities: block b runs segments seg_off[b] .. seg_off[b+1]-1; `cur`
+// is the ping-pong buffer holding the populations read this step
+template <int ST, int TX>
+__global__ void __launch_bounds__(TX, 512 / TX)
+k_march2d_batch(const BatchDev D, int cur, int write_macro, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int s0 = D.seg_off[blockIdx.x], s1 = D.seg_off[blockIdx.x + 1];
+    auto seg = [&](int k, int &cav, int &i0, int &ja, int &jb) {
+        const int4 q = D.segs[s0 + k];
+        cav = q.x;
+        i0 = q.y;
+        ja = q.z;
+        jb = q.w;
+    };
+    auto cavity = [&](int c, const Geo *&Gp, const CUtensorMap *&m, S *&d, C *&Fo, const Bufs *&Bp) {
+        Gp = &D.geo[c];
+        m = &D.maps[(int64_t)c * 2 + cur].m[0];
+        Bp = &D.bufs[c];
+        d = (S *)D.bufs[c].pop[1 - cur];
+        Fo = (C *)D.bufs[c].F[1 - cur];
+    };
+    march2d_run<ST, TX>(s1 - s0, seg, cavity, write_macro, err);
 }

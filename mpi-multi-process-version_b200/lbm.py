@@ -33,7 +33,11 @@ EXPORTS = [
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
     "lbm_set_option", "lbm_get_option", "lbm_check_noalloc",
+    "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_size", "lbm_batch_cavity", "lbm_batch_init_reference",
+    "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_tune",
+    "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
 ]
+BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO = 1, 2, 3
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
@@ -91,6 +95,24 @@ def lib():
         L.lbm_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
         L.lbm_get_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
         L.lbm_check_noalloc.argtypes = [ctypes.c_void_p] * 8 + [ctypes.c_int64, _dp, _dp, ctypes.c_void_p]
+        _pp = ctypes.POINTER(_dp)
+        L.lbm_batch_create.argtypes = [ctypes.c_int32, ctypes.POINTER(lbm_params), _pp, _pp, _pp,
+                                       ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.lbm_batch_size.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+        L.lbm_batch_cavity.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_batch_init_reference.argtypes = [ctypes.c_void_p]
+        L.lbm_batch_step.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.lbm_batch_check.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_batch_nusselt.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.lbm_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_batch_tune.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                     ctypes.POINTER(ctypes.c_int32), _dp]
+        L.lbm_batch_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
+        L.lbm_batch_get_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_batch_synchronize.argtypes = [ctypes.c_void_p]
+        L.lbm_batch_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         _lib = L
     return _lib
 
@@ -304,6 +326,137 @@ class Cavity:
         v = ctypes.c_int64()
         _chk(lib().lbm_device_bytes(self.h, ctypes.byref(v)), "lbm_device_bytes")
         return int(v.value)
+
+
+# ---------------------------------------------------------------------------
+# batches of cavities
+# ---------------------------------------------------------------------------
+class _Member(Cavity):
+    """A member cavity of a Batch: an ordinary handle owned by the batch."""
+
+    def __init__(self, batch, i, h, dim, nx, ny, nz, params, mesh_):
+        self.h = h
+        self.dim, self.nx, self.ny, self.nz = dim, nx, ny, nz
+        self.Q, self.QT = (9, 5) if dim == 2 else (19, 7)
+        self.params, self.mesh = params, mesh_
+        self.storage, self.mode = batch.storage, batch.mode
+        self._batch = batch
+
+    def close(self):  # owned by the batch
+        self.h = None
+
+
+class Batch:
+    """Many independent cavities advanced together (lbm_batch_*).  `specs` is
+    a list of dicts with the Cavity keyword arguments (nx, ny, Ra, Pr, grid,
+    stretch, ...); dim, storage, mode and device are common to all members."""
+
+    def __init__(self, dim, specs, storage="f64", mode="fast", device=0):
+        self.dim, self.storage, self.mode = dim, storage, mode
+        n = len(specs)
+        P = (lbm_params * n)()
+        self._keep = []
+        xs, ys, zs = (_dp * n)(), (_dp * n)(), (_dp * n)()
+        self._meshes = []
+        for i, sp in enumerate(specs):
+            nx, ny = int(sp["nx"]), int(sp["ny"])
+            nz = int(sp.get("nz", 1)) if dim == 3 else 1
+            m = sp.get("coords") or mesh(nx, ny, nz if dim == 3 else 0, sp.get("grid", "tanh"),
+                                         sp.get("stretch", 1.5))
+            self._meshes.append(m)
+            P[i] = lbm_params(dim, nx, ny, nz, float(sp.get("Ra", 1e5)), float(sp.get("Pr", 0.71)),
+                              float(sp.get("Ma", 0.1)), float(sp.get("Thot", 1.0)), float(sp.get("Tcold", 0.0)),
+                              m.dt, m.length_LB, STORE[storage], MODE[mode], int(device), 0)
+            arrs = [np.ascontiguousarray(a) for a in (m.x, m.y)] + ([np.ascontiguousarray(m.z)] if dim == 3 else [])
+            self._keep += arrs
+            xs[i], ys[i] = _p(arrs[0]), _p(arrs[1])
+            if dim == 3:
+                zs[i] = _p(arrs[2])
+        self.specs = specs
+        h = ctypes.c_void_p()
+        _chk(lib().lbm_batch_create(n, P, xs, ys, zs if dim == 3 else None, ctypes.byref(h)), "lbm_batch_create")
+        self.h = h
+        self.n = n
+        self.members = []
+        for i in range(n):
+            hh = ctypes.c_void_p()
+            _chk(lib().lbm_batch_cavity(self.h, i, ctypes.byref(hh)), "lbm_batch_cavity")
+            self.members.append(_Member(self, i, hh, dim, P[i].nx, P[i].ny, P[i].nz, P[i], self._meshes[i]))
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().lbm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nodes(self):
+        return sum(m.nnode for m in self.members)
+
+    def initial(self):
+        _chk(lib().lbm_batch_init_reference(self.h), "lbm_batch_init_reference")
+        return self
+
+    def step(self, n=1):
+        _chk(lib().lbm_batch_step(self.h, int(n)), "lbm_batch_step")
+
+    def synchronize(self):
+        _chk(lib().lbm_batch_synchronize(self.h), "lbm_batch_synchronize")
+
+    def check(self):
+        a, b = np.zeros(self.n), np.zeros(self.n)
+        _chk(lib().lbm_batch_check(self.h, _p(a), _p(b)), "lbm_batch_check")
+        return a, b
+
+    def nusselt(self):
+        a, b = np.zeros(self.n), np.zeros(self.n)
+        _chk(lib().lbm_batch_nusselt(self.h, _p(a), _p(b)), "lbm_batch_nusselt")
+        return a, b
+
+    def run(self, max_steps, check_every=2000, eps=float(np.float32(1e-6))):
+        conv = (ctypes.c_int32 * self.n)()
+        done = (ctypes.c_int64 * self.n)()
+        _chk(lib().lbm_batch_run(self.h, int(max_steps), int(check_every), float(eps), conv, done), "lbm_batch_run")
+        return np.array(conv[:], dtype=bool), np.array(done[:], dtype=np.int64)
+
+    def tune(self, steps=20):
+        t, nb, v = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+        _chk(lib().lbm_batch_tune(self.h, int(steps), ctypes.byref(t), ctypes.byref(nb), ctypes.byref(v)),
+             "lbm_batch_tune")
+        return {"tile": t.value, "nblocks": nb.value, "mlups": v.value}
+
+    def set_option(self, name, value):
+        _chk(lib().lbm_batch_set_option(self.h, BATCH_OPT[name], int(value)), "lbm_batch_set_option")
+
+    def get_option(self, name):
+        v = ctypes.c_int64()
+        _chk(lib().lbm_batch_get_option(self.h, BATCH_OPT[name], ctypes.byref(v)), "lbm_batch_get_option")
+        return int(v.value)
+
+    def stream_ptr(self):
+        s = ctypes.c_void_p()
+        _chk(lib().lbm_batch_stream(self.h, ctypes.byref(s)), "lbm_batch_stream")
+        return int(s.value or 0)
+
+
+def sweep_specs(n=256, seed=0, sides=(64, 96, 128, 192, 256, 384, 512), aspect=(1.0, 4.0),
+                log10_ra=(3.0, 6.0), pr=(0.71, 7.0), stretch=(1.0, 2.0)):
+    """The seeded parameter sweep of differentially heated 2D cavities: width
+    from `sides`, height = width x aspect (tall cavities), Ra log-uniform, Pr
+    and the tanh stretch uniform."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n):
+        nx = int(rng.choice(sides))
+        ny = int(round(nx * rng.uniform(*aspect)))
+        specs.append({"nx": nx, "ny": ny, "Ra": float(10 ** rng.uniform(*log10_ra)), "Pr": float(rng.uniform(*pr)),
+                      "grid": "tanh", "stretch": float(rng.uniform(*stretch))})
+    return specs
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,139 @@
+"""Batches of cavities through the C ABI (lbm_batch_*): every member of a
+batch must evolve exactly as the same cavity run alone (exact mode: bit for
+bit), whatever the tile width, persistent grid, graph replay or launch mode;
+the per-member stop test retires converged members."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [
+    dict(nx=64, ny=80, Ra=1e4, Pr=0.71, grid="tanh", stretch=1.2),
+    dict(nx=96, ny=96, Ra=1e5, Pr=2.0, grid="tanh", stretch=1.7),
+    dict(nx=40, ny=150, Ra=3e3, Pr=7.0, grid="erf", stretch=3.2),
+    dict(nx=130, ny=33, Ra=1e6, Pr=0.71, grid="tanh", stretch=1.0),
+    dict(nx=33, ny=33, Ra=1e5, Pr=0.71, grid="erf", stretch=3.2),
+]
+
+
+def standalone(pkg, sp, steps, mode="exact"):
+    c = pkg.Cavity(2, sp["nx"], sp["ny"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"], stretch=sp["stretch"],
+                   mode=mode, kernel="direct")
+    c.initial()
+    c.step(steps)
+    m = c.macro()
+    c.close()
+    return m
+
+
+@pytest.fixture(scope="module")
+def reference(pkg):
+    return [standalone(pkg, sp, 37) for sp in SPECS]
+
+
+@pytest.mark.parametrize("tile,nblocks,graphs", [(64, 0, 1), (32, 0, 1), (128, 0, 0), (64, 1, 1), (32, 5, 0),
+                                                 (128, 7, 1)])
+def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, graphs):
+    b = pkg.Batch(2, SPECS, mode="exact")
+    b.set_option("tile", tile)
+    b.set_option("nblocks", nblocks)
+    b.set_option("graphs", graphs)
+    b.initial()
+    b.step(20)
+    b.step(17)
+    for m, ref in zip(b.members, reference):
+        got = m.macro()
+        assert m.itc == 37
+        for k in ref:
+            assert np.array_equal(got[k], ref[k]), k
+    b.close()
+
+
+def test_batch_one_launch_per_cavity_matches(pkg, reference):
+    b = pkg.Batch(2, SPECS, mode="exact")
+    b.set_option("persistent", 0)
+    b.initial()
+    b.step(37)
+    for m, ref in zip(b.members, reference):
+        got = m.macro()
+        for k in ref:
+            assert np.array_equal(got[k], ref[k]), k
+    b.close()
+
+
+def test_batch_fast_mode_close_to_standalone(pkg):
+    b = pkg.Batch(2, SPECS, mode="fast")
+    b.initial()
+    b.step(200)
+    for m, sp in zip(b.members, SPECS):
+        ref = standalone(pkg, sp, 200, mode="fast")
+        f_scale = 1.0
+        for k in ref:
+            assert np.abs(m.macro()[k] - ref[k]).max() <= 1e-12 * f_scale, k
+    b.close()
+
+
+def test_batch_check_and_nusselt_per_member(pkg):
+    b = pkg.Batch(2, SPECS, mode="exact")
+    b.initial()
+    b.step(30)
+    eu, et = b.check()
+    nh, nc = b.nusselt()
+    for i, sp in enumerate(SPECS):
+        c = pkg.Cavity(2, sp["nx"], sp["ny"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"], stretch=sp["stretch"],
+                       mode="exact")
+        c.initial()
+        c.step(30)
+        assert (eu[i], et[i]) == c.check()
+        assert (nh[i], nc[i]) == c.nusselt()
+        c.close()
+    b.close()
+
+
+def test_batch_run_retires_converged_members(pkg):
+    specs = [dict(nx=32, ny=32, Ra=1e3, Pr=0.71, grid="tanh", stretch=1.5),
+             dict(nx=48, ny=96, Ra=1e6, Pr=0.71, grid="tanh", stretch=1.5)]
+    b = pkg.Batch(2, specs, mode="fast")
+    b.initial()
+    conv, steps = b.run(max_steps=3000, check_every=100, eps=2e-2)
+    assert conv.dtype == bool and steps.shape == (2,)
+    assert conv[0] and steps[0] < 3000
+    frozen = b.members[0].macro()
+    # the retired member no longer moves while the others continue
+    if not conv[1]:
+        assert steps[1] == 3000
+    b.step(50)
+    # after run() every member is active again
+    moved = b.members[0].macro()
+    assert not np.array_equal(frozen["u"], moved["u"])
+    b.close()
+
+
+def test_batch_tune_picks_a_tile(pkg):
+    b = pkg.Batch(2, pkg.sweep_specs(24, seed=3, sides=(64, 96, 128), aspect=(1.0, 2.0)))
+    b.initial()
+    r = b.tune(steps=6)
+    assert r["tile"] in (32, 64, 128) and r["nblocks"] > 0 and r["mlups"] > 0
+    assert b.get_option("tile") == r["tile"]
+    b.step(4)
+    b.synchronize()
+    b.close()
+
+
+def test_batch_3d_members_match_standalone(pkg):
+    specs = [dict(nx=16, ny=16, nz=12, Ra=1e5, Pr=0.71, grid="tanh", stretch=1.5),
+             dict(nx=20, ny=12, nz=10, Ra=1e4, Pr=2.0, grid="erf", stretch=3.2)]
+    b = pkg.Batch(3, specs, mode="exact")
+    b.initial()
+    b.step(15)
+    for m, sp in zip(b.members, specs):
+        c = pkg.Cavity(3, sp["nx"], sp["ny"], sp["nz"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"],
+                       stretch=sp["stretch"], mode="exact")
+        c.initial()
+        c.step(15)
+        ref = c.macro()
+        got = m.macro()
+        for k in ref:
+            assert np.array_equal(got[k], ref[k]), k
+        c.close()
+    b.close()

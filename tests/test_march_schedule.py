@@ -134,8 +134,7 @@ def check_3d(nx, ny, nz, grid, es):
     replay(nz, ntiles * nz, grid, nodes, check_node)
 
 
-def check_2d(nx, ny, grid, es):
-    TX = 128
+def check_2d(nx, ny, grid, es, TX=128):
     HX = 16 // es
     bx = lambda c: TX + (2 * HX if c else 0)  # noqa: E731
     ntx = -(-nx // TX)
@@ -178,9 +177,10 @@ def test_march3d_schedule_and_indices(shape, es):
 
 @pytest.mark.parametrize("shape", [(2048, 64), (128, 128), (130, 9), (48, 48), (300, 3), (40, 24)])
 @pytest.mark.parametrize("es", [8, 4, 2])
-def test_march2d_schedule_and_indices(shape, es):
+@pytest.mark.parametrize("tx", [32, 64, 128])
+def test_march2d_schedule_and_indices(shape, es, tx):
     nx, ny = shape
-    total = -(-nx // 128) * ny
+    total = -(-nx // tx) * ny
     for grid in sorted({1, 2, 5, 148, 592, total}):
         if grid <= total:
-            check_2d(nx, ny, grid, es)
+            check_2d(nx, ny, grid, es, tx)

@@ -94,6 +94,17 @@ int lbm_mesh(int32_t kind, double stretch, int32_t nx, int32_t ny, int32_t nz,
              double *x, double *y, double *z,
              double *dx0, double *length_LB, double *dt);
 
+/* mesh() generalised to boxes of physical size lx x ly (x lz) with any node
+ * counts (the reference assumes a unit square or cube with nx = ny = nz):
+ * each axis gets the stretched raw grid on [0, l_axis]; the smallest first
+ * spacing over the axes sets the lattice unit (dx0, length_LB = 1/dx0,
+ * dt = dx0*length_LB); every axis is shifted by dx0/2 and scaled by
+ * length_LB as in 2M:113-116.  With lx = ly (= lz) = 1 and equal node counts
+ * this is exactly lbm_mesh. */
+int lbm_mesh_box(int32_t kind, double stretch, int32_t nx, int32_t ny, int32_t nz,
+                 double lx, double ly, double lz, double *x, double *y, double *z,
+                 double *dx0, double *length_LB, double *dt);
+
 /* The parameter block of initial() (2M:151-162, 3M:206-229) for a parameter
  * set: out[0..8] = viscosity_LB, kappa, gbeta, tauf, Snu, Sq, sig_k, dt,
  * length_LB.  Host only. */

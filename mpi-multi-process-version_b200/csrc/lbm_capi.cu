@@ -126,6 +126,43 @@ extern "C" int lbm_mesh(int32_t kind, double stretch, int32_t nx, int32_t ny, in
     return LBM_OK;
 }
 
+extern "C" int lbm_mesh_box(int32_t kind, double stretch, int32_t nx, int32_t ny, int32_t nz, double lx, double ly,
+                            double lz, double *x, double *y, double *z, double *dx0_out, double *length_LB_out,
+                            double *dt_out)
+{
+    if (kind < 0 || kind > 2) return fail(LBM_ERR_PARAM, "lbm_mesh_box: unknown grid kind %d", kind);
+    if (nx < 3 || ny < 3 || (z && nz < 3)) return fail(LBM_ERR_PARAM, "lbm_mesh_box: need >= 3 nodes per axis");
+    if (!x || !y) return fail(LBM_ERR_PARAM, "lbm_mesh_box: x and y are required");
+    if (!(lx > 0) || !(ly > 0) || (z && !(lz > 0))) return fail(LBM_ERR_PARAM, "lbm_mesh_box: lengths must be > 0");
+    if (kind != LBM_GRID_UNIFORM && !(stretch > 0.0)) return fail(LBM_ERR_PARAM, "lbm_mesh_box: stretch must be > 0");
+    grid_raw(kind, nx, stretch, x);
+    grid_raw(kind, ny, stretch, y);
+    if (z) grid_raw(kind, nz, stretch, z);
+    if (lx != 1.0)
+        for (int i = 0; i <= nx + 1; ++i) x[i] = x[i] * lx;
+    if (ly != 1.0)
+        for (int j = 0; j <= ny + 1; ++j) y[j] = y[j] * ly;
+    if (z && lz != 1.0)
+        for (int k = 0; k <= nz + 1; ++k) z[k] = z[k] * lz;
+    // the finest first cell over the axes sets the lattice unit
+    double dx1 = x[1] - x[0];
+    if (y[1] - y[0] < dx1) dx1 = y[1] - y[0];
+    if (z && z[1] - z[0] < dx1) dx1 = z[1] - z[0];
+    const double dx0 = dx1, dt0 = dx0;
+    const double length_LB = 1.0 / dx1;
+    const double dt = dt0 * length_LB;
+    for (int i = 1; i <= nx; ++i) x[i] = x[i] - dx0 / 2.0;
+    for (int j = 1; j <= ny; ++j) y[j] = y[j] - dx0 / 2.0;
+    if (z) for (int k = 1; k <= nz; ++k) z[k] = z[k] - dx0 / 2.0;
+    for (int i = 0; i <= nx + 1; ++i) x[i] = x[i] * length_LB;
+    for (int j = 0; j <= ny + 1; ++j) y[j] = y[j] * length_LB;
+    if (z) for (int k = 0; k <= nz + 1; ++k) z[k] = z[k] * length_LB;
+    if (dx0_out) *dx0_out = dx0;
+    if (length_LB_out) *length_LB_out = length_LB;
+    if (dt_out) *dt_out = dt;
+    return LBM_OK;
+}
+
 static Derived derive(const lbm_params &p)
 {
     // 2M:152-162 and 3M:207-229

@@ -28,7 +28,7 @@ GRID = {"erf": 0, "tanh": 1, "uniform": 2}
 
 # every symbol include/lbm_b200.h declares
 EXPORTS = [
-    "lbm_abi_version", "lbm_error_string", "lbm_last_error", "lbm_mesh", "lbm_derived_params",
+    "lbm_abi_version", "lbm_error_string", "lbm_last_error", "lbm_mesh", "lbm_mesh_box", "lbm_derived_params",
     "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
@@ -74,6 +74,8 @@ def lib():
         L.lbm_last_error.restype = ctypes.c_char_p
         L.lbm_mesh.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                _dp, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_mesh_box.argtypes = [ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
         L.lbm_derived_params.argtypes = [ctypes.POINTER(lbm_params), _dp]
         L.lbm_create.argtypes = [ctypes.POINTER(lbm_params), _dp, _dp, _dp, ctypes.POINTER(ctypes.c_void_p)]
         L.lbm_destroy.argtypes = [ctypes.c_void_p]
@@ -171,6 +173,19 @@ def mesh(nx: int, ny: int, nz: int = 0, grid: str = "erf", stretch: float = 3.2)
     out = np.zeros(3)
     _chk(lib().lbm_mesh(GRID[grid], float(stretch), nx, ny, nz, _p(x), _p(y), _p(z),
                         _p(out[0:1]), _p(out[1:2]), _p(out[2:3])), "lbm_mesh")
+    return Mesh(x, y, z, float(out[0]), float(out[1]), float(out[2]))
+
+
+def mesh_box(nx: int, ny: int, nz: int = 0, lx: float = 1.0, ly: float = 1.0, lz: float = 1.0,
+             grid: str = "tanh", stretch: float = 1.5) -> Mesh:
+    """mesh() for a box of physical size lx x ly (x lz) with any node counts:
+    the finest first cell over the axes sets the lattice unit (lbm_mesh_box).
+    Equal to mesh() for the unit square/cube with equal node counts."""
+    x, y = np.zeros(nx + 2), np.zeros(ny + 2)
+    z = np.zeros(nz + 2) if nz else None
+    out = np.zeros(3)
+    _chk(lib().lbm_mesh_box(GRID[grid], float(stretch), nx, ny, nz, float(lx), float(ly), float(lz), _p(x), _p(y),
+                            _p(z), _p(out[0:1]), _p(out[1:2]), _p(out[2:3])), "lbm_mesh_box")
     return Mesh(x, y, z, float(out[0]), float(out[1]), float(out[2]))
 
 
@@ -349,7 +364,9 @@ class _Member(Cavity):
 class Batch:
     """Many independent cavities advanced together (lbm_batch_*).  `specs` is
     a list of dicts with the Cavity keyword arguments (nx, ny, Ra, Pr, grid,
-    stretch, ...); dim, storage, mode and device are common to all members."""
+    stretch, coords, ...); dim, storage, mode and device are common to all
+    members.  Without `coords` a member gets mesh_box with the physical aspect
+    ny/nx (nz/nx), which is the reference's mesh for square members."""
 
     def __init__(self, dim, specs, storage="f64", mode="fast", device=0):
         self.dim, self.storage, self.mode = dim, storage, mode
@@ -361,8 +378,10 @@ class Batch:
         for i, sp in enumerate(specs):
             nx, ny = int(sp["nx"]), int(sp["ny"])
             nz = int(sp.get("nz", 1)) if dim == 3 else 1
-            m = sp.get("coords") or mesh(nx, ny, nz if dim == 3 else 0, sp.get("grid", "tanh"),
-                                         sp.get("stretch", 1.5))
+            # default: a box of physical size 1 x ny/nx (x nz/nx) -- the reference's
+            # mesh() for square members, well-shaped cells for the others
+            m = sp.get("coords") or mesh_box(nx, ny, nz if dim == 3 else 0, 1.0, ny / nx, nz / nx,
+                                             sp.get("grid", "tanh"), sp.get("stretch", 1.5))
             self._meshes.append(m)
             P[i] = lbm_params(dim, nx, ny, nz, float(sp.get("Ra", 1e5)), float(sp.get("Pr", 0.71)),
                               float(sp.get("Ma", 0.1)), float(sp.get("Thot", 1.0)), float(sp.get("Tcold", 0.0)),
@@ -447,15 +466,18 @@ class Batch:
 def sweep_specs(n=256, seed=0, sides=(64, 96, 128, 192, 256, 384, 512), aspect=(1.0, 4.0),
                 log10_ra=(3.0, 6.0), pr=(0.71, 7.0), stretch=(1.0, 2.0)):
     """The seeded parameter sweep of differentially heated 2D cavities: width
-    from `sides`, height = width x aspect (tall cavities), Ra log-uniform, Pr
-    and the tanh stretch uniform."""
+    from `sides`, height = width x aspect (tall cavities of physical size
+    1 x aspect, mesh_box), Ra log-uniform, Pr and the tanh stretch uniform."""
     rng = np.random.default_rng(seed)
     specs = []
     for _ in range(n):
         nx = int(rng.choice(sides))
-        ny = int(round(nx * rng.uniform(*aspect)))
-        specs.append({"nx": nx, "ny": ny, "Ra": float(10 ** rng.uniform(*log10_ra)), "Pr": float(rng.uniform(*pr)),
-                      "grid": "tanh", "stretch": float(rng.uniform(*stretch))})
+        a = float(rng.uniform(*aspect))
+        ny = int(round(nx * a))
+        b = float(rng.uniform(*stretch))
+        specs.append({"nx": nx, "ny": ny, "aspect": ny / nx, "Ra": float(10 ** rng.uniform(*log10_ra)),
+                      "Pr": float(rng.uniform(*pr)), "grid": "tanh", "stretch": b,
+                      "coords": mesh_box(nx, ny, 0, 1.0, ny / nx, 1.0, "tanh", b)})
     return specs
 
 

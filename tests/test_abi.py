@@ -99,3 +99,20 @@ def test_fortran_e_format(pkg):
     assert pkg.fortran_e(-0.000123456, 13, 6) == "-0.123456E-03"
     assert pkg.fortran_e(0.0, 13, 6) == " 0.000000E+00"
     assert pkg.fortran_e(999.99996, 11, 4) == " 0.1000E+04"
+
+
+def test_mesh_box_reduces_to_mesh_for_unit_square(pkg):
+    for grid, b in (("erf", 3.2), ("tanh", 1.5)):
+        a = pkg.mesh(33, 33, 0, grid, b)
+        m = pkg.mesh_box(33, 33, 0, 1.0, 1.0, 1.0, grid, b)
+        assert np.array_equal(a.x, m.x) and np.array_equal(a.y, m.y) and a.dt == m.dt and a.length_LB == m.length_LB
+
+
+def test_mesh_box_tall_cavity_spacings(pkg):
+    # 1 x 3 cavity with 40 x 120 nodes: every node spacing is at least one
+    # lattice unit and the walls lie half a unit outside the end nodes
+    m = pkg.mesh_box(40, 120, 0, 1.0, 3.0, 1.0, "tanh", 1.5)
+    for c, n in ((m.x, 40), (m.y, 120)):
+        d = np.diff(c[1:n + 1])
+        assert d.min() >= 1.0 - 1e-12
+    assert m.x[1] == pytest.approx(0.5) or m.y[1] == pytest.approx(0.5)

@@ -7,18 +7,25 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-SPECS = [
-    dict(nx=64, ny=80, Ra=1e4, Pr=0.71, grid="tanh", stretch=1.2),
-    dict(nx=96, ny=96, Ra=1e5, Pr=2.0, grid="tanh", stretch=1.7),
-    dict(nx=40, ny=150, Ra=3e3, Pr=7.0, grid="erf", stretch=3.2),
-    dict(nx=130, ny=33, Ra=1e6, Pr=0.71, grid="tanh", stretch=1.0),
-    dict(nx=33, ny=33, Ra=1e5, Pr=0.71, grid="erf", stretch=3.2),
-]
+def _specs():
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    raw = [dict(nx=64, ny=80, Ra=1e4, Pr=0.71, grid="tanh", stretch=1.2),
+           dict(nx=96, ny=96, Ra=1e5, Pr=2.0, grid="tanh", stretch=1.7),
+           dict(nx=40, ny=150, Ra=3e3, Pr=7.0, grid="erf", stretch=3.2),
+           dict(nx=130, ny=33, Ra=1e6, Pr=0.71, grid="tanh", stretch=1.0),
+           dict(nx=33, ny=33, Ra=1e5, Pr=0.71, grid="erf", stretch=3.2)]
+    for sp in raw:  # physical size 1 x ny/nx: cells of similar shape on both axes
+        sp["coords"] = pkg.mesh_box(sp["nx"], sp["ny"], 0, 1.0, sp["ny"] / sp["nx"], 1.0, sp["grid"], sp["stretch"])
+    return raw
+
+
+SPECS = _specs()
 
 
 def standalone(pkg, sp, steps, mode="exact"):
     c = pkg.Cavity(2, sp["nx"], sp["ny"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"], stretch=sp["stretch"],
-                   mode=mode, kernel="direct")
+                   mode=mode, kernel="direct", coords=sp["coords"])
     c.initial()
     c.step(steps)
     m = c.macro()
@@ -44,6 +51,7 @@ def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, g
     for m, ref in zip(b.members, reference):
         got = m.macro()
         assert m.itc == 37
+        assert np.isfinite(got["rho"]).all()
         for k in ref:
             assert np.array_equal(got[k], ref[k]), k
     b.close()
@@ -67,9 +75,9 @@ def test_batch_fast_mode_close_to_standalone(pkg):
     b.step(200)
     for m, sp in zip(b.members, SPECS):
         ref = standalone(pkg, sp, 200, mode="fast")
-        f_scale = 1.0
+        got = m.macro()
         for k in ref:
-            assert np.abs(m.macro()[k] - ref[k]).max() <= 1e-12 * f_scale, k
+            assert np.isfinite(got[k]).all() and np.abs(got[k] - ref[k]).max() <= 1e-12, k
     b.close()
 
 
@@ -81,7 +89,7 @@ def test_batch_check_and_nusselt_per_member(pkg):
     nh, nc = b.nusselt()
     for i, sp in enumerate(SPECS):
         c = pkg.Cavity(2, sp["nx"], sp["ny"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"], stretch=sp["stretch"],
-                       mode="exact")
+                       mode="exact", coords=sp["coords"])
         c.initial()
         c.step(30)
         assert (eu[i], et[i]) == c.check()
@@ -92,7 +100,7 @@ def test_batch_check_and_nusselt_per_member(pkg):
 
 def test_batch_run_retires_converged_members(pkg):
     specs = [dict(nx=32, ny=32, Ra=1e3, Pr=0.71, grid="tanh", stretch=1.5),
-             dict(nx=48, ny=96, Ra=1e6, Pr=0.71, grid="tanh", stretch=1.5)]
+             dict(nx=48, ny=96, Ra=1e5, Pr=0.71, grid="tanh", stretch=1.5)]
     b = pkg.Batch(2, specs, mode="fast")
     b.initial()
     conv, steps = b.run(max_steps=3000, check_every=100, eps=2e-2)
@@ -128,7 +136,7 @@ def test_batch_3d_members_match_standalone(pkg):
     b.step(15)
     for m, sp in zip(b.members, specs):
         c = pkg.Cavity(3, sp["nx"], sp["ny"], sp["nz"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"],
-                       stretch=sp["stretch"], mode="exact")
+                       stretch=sp["stretch"], mode="exact", coords=m.mesh)
         c.initial()
         c.step(15)
         ref = c.macro()

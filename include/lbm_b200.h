@@ -59,6 +59,7 @@ extern "C" {
 #define LBM_OPT_NBLOCKS  2  /* persistent blocks of the march kernel (0 = automatic) */
 #define LBM_OPT_L2PROMO  3  /* L2 fetch promotion of the march kernel's TMA boxes:
                                0 none, 1 64 B, 2 128 B, 3 256 B */
+#define LBM_OPT_GRAPHS   4  /* 1 (default): lbm_step replays captured 2-step CUDA graphs */
 
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */
@@ -137,6 +138,14 @@ int lbm_init_equilibrium(lbm_handle *h, const double *rho, const double *u,
  * collision_T, update (a no-op on one domain), interpolate, bounceback_u,
  * bounceback_T, macro_u, macro_t (2M:309-325, 3M:375-391).  Asynchronous. */
 int lbm_step(lbm_handle *h, int32_t nsteps);
+
+/* The reference's time loop (2M:307-330): lbm_step until, at a check every
+ * check_every iterations (counted from the last init, as itc is), both
+ * residuals of lbm_check are at most eps, or max_steps iterations were done.
+ * Reports the iterations done and the last residuals; returns
+ * LBM_ERR_NONFINITE if a residual sum stops being finite. */
+int lbm_run(lbm_handle *h, int64_t max_steps, int32_t check_every, double eps,
+            int64_t *steps_done, double *errU, double *errT);
 
 /* Iterations done since the last init (the reference's itc). */
 int lbm_itc(const lbm_handle *h, int64_t *itc);

@@ -4,6 +4,8 @@ zzhao0930/MPI-Multi-Process-Version, behind the C ABI in include/lbm_b200.h."""
 from .lbm import (EXPORTS, GRID, MODE, NOALLOC_MAX_NODES, STORE, Batch, Cavity, LBMError, Mesh, check_noalloc,
                   fortran_e, kernel_launches, lbm_params, lib, mesh, mesh_box, output_ascii, run_main, sweep_specs)
 
-__all__ = ["EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Batch", "Cavity", "LBMError", "Mesh",
+from . import studies  # noqa: E402
+
+__all__ = ["studies", "EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Batch", "Cavity", "LBMError", "Mesh",
            "check_noalloc", "sweep_specs", "mesh_box",
            "fortran_e", "kernel_launches", "lbm_params", "lib", "mesh", "output_ascii", "run_main"]

@@ -13,6 +13,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -268,6 +269,7 @@ static int dalloc(lbm_handle *h, T **ptr, size_t bytes)
 
 static void free_all(lbm_handle *h)
 {
+    lbm::drop_graphs(h);
     void *ptrs[] = {h->bufs.pop[0], h->bufs.pop[1], h->bufs.F[0], h->bufs.F[1], h->bufs.rho, h->bufs.u,
                     h->bufs.v, h->bufs.w, h->bufs.T, h->bufs.up, h->bufs.vp, h->bufs.wp, h->bufs.Tp,
                     h->bufs.partials, h->bufs.scal, h->d_wgt[0], h->d_wgt[1], h->d_wgt[2], h->d_coord[0],
@@ -389,6 +391,7 @@ static bool march_supported(const lbm_handle *h)
 
 static int resolve_path(lbm_handle *h)
 {
+    lbm::drop_graphs(h);
     const bool ok = march_supported(h);
     if (h->kernel_opt == 2 && !ok)
         return fail(LBM_ERR_UNSUPPORTED, "march kernel not available for this shape / device");
@@ -623,35 +626,109 @@ int lbm::first_collision(lbm_handle *h)
     return LBM_OK;
 }
 
+// one fused step from buffer `cur` (asynchronous)
+static cudaError_t launch_one(lbm_handle *h, int cur, int wm)
+{
+    const bool ex = h->p.mode == LBM_MODE_EXACT;
+    Bufs &b = h->bufs;
+    const int nxt = 1 - cur;
+    if (h->use_march)
+        return ex ? exact::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
+                                 h->nblocks, h->stream)
+                  : fast::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
+                                h->nblocks, h->stream);
+    return ex ? exact::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream)
+              : fast::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream);
+}
+
+void lbm::drop_graphs(lbm_handle *h)
+{
+    for (auto &g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// a 2-step graph starting from buffer `cur`, captured once per kernel choice
+static int step_graph(lbm_handle *h, int cur, cudaGraphExec_t *out)
+{
+    if (!h->graph[cur]) {
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e1 = launch_one(h, cur, 0);
+        const cudaError_t e2 = launch_one(h, 1 - cur, 0);
+        const cudaError_t e3 = cudaStreamEndCapture(h->stream, &g);
+        lbm::g_launches -= 2;  // counted when replayed
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(LBM_ERR_CUDA, "step graph capture: %s",
+                        cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+        }
+        const cudaError_t e = cudaGraphInstantiate(&h->graph[cur], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "step graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = h->graph[cur];
+    return LBM_OK;
+}
+
 extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
 {
     CHECK_H(h);
     if (nsteps < 0) return fail(LBM_ERR_PARAM, "nsteps < 0");
     if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_step before an init call");
     if (nsteps == 0) return LBM_OK;
-    const bool ex = h->p.mode == LBM_MODE_EXACT;
-    Bufs &b = h->bufs;
     int st = lbm::first_collision(h);
     if (st) return st;
-    for (int s = 0; s < nsteps; ++s) {
-        const int nxt = 1 - h->cur;
-        const int wm = (s == nsteps - 1);
-        if (h->use_march)
-            CU(ex ? exact::march(h->geo, h->p.storage, h->tmaps[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
-                                 h->nblocks, h->stream)
-                  : fast::march(h->geo, h->p.storage, h->tmaps[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
-                                h->nblocks, h->stream));
-        else
-            CU(ex ? exact::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
-                                h->stream)
-                  : fast::step(h->geo, h->p.storage, b.pop[h->cur], b.F[h->cur], b.pop[nxt], b.F[nxt], b, wm,
-                               h->stream));
-        h->cur = nxt;
+    int done = 0;
+    // replay 2-step graphs for all but the last step(s) (small domains are
+    // launch-bound), then the last step writes the macroscopic fields
+    if (h->use_graphs && nsteps > 4) {
+        while (nsteps - done > 2) {
+            cudaGraphExec_t g;
+            if ((st = step_graph(h, h->cur, &g))) return st;
+            CU(cudaGraphLaunch(g, h->stream));
+            lbm::g_launches += 2;
+            done += 2;
+        }
+    }
+    for (; done < nsteps; ++done) {
+        CU(launch_one(h, h->cur, done == nsteps - 1));
+        h->cur = 1 - h->cur;
     }
     h->itc += nsteps;
     return LBM_OK;
 }
 
+extern "C" int lbm_run(lbm_handle *h, int64_t max_steps, int32_t check_every, double eps, int64_t *steps_done,
+                       double *errU, double *errT)
+{
+    CHECK_H(h);
+    if (max_steps < 0 || check_every < 1) return fail(LBM_ERR_PARAM, "need max_steps >= 0 and check_every >= 1");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_run before an init call");
+    // the reference's loop (2M:307-330): iterate while errorU > eps or
+    // errorT > eps, checking every check_every iterations
+    double eu = 100.0, et = 100.0;
+    int64_t done = 0;
+    while ((eu > eps || et > eps) && done < max_steps) {
+        const int64_t k = std::min<int64_t>(check_every - (h->itc % check_every), max_steps - done);
+        int st = lbm_step(h, (int32_t)k);
+        if (st) return st;
+        done += k;
+        if (h->itc % check_every == 0) {
+            st = lbm_check(h, &eu, &et);
+            if (steps_done) *steps_done = done;
+            if (errU) *errU = eu;
+            if (errT) *errT = et;
+            if (st) return st;
+        }
+    }
+    if (steps_done) *steps_done = done;
+    if (errU) *errU = eu;
+    if (errT) *errT = et;
+    return lbm::sync_handle(h);
+}
 extern "C" int lbm_itc(const lbm_handle *h, int64_t *itc)
 {
     if (!h || !itc) return fail(LBM_ERR_PARAM, "NULL argument");
@@ -839,6 +916,10 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         if (value < 0 || value > (1 << 20)) return fail(LBM_ERR_PARAM, "nblocks out of range");
         h->nblocks_opt = (int)value;
         return resolve_path(h);
+    case LBM_OPT_GRAPHS:
+        lbm::drop_graphs(h);
+        h->use_graphs = value != 0;
+        return LBM_OK;
     case LBM_OPT_L2PROMO:
         if (value < 0 || value > 3) return fail(LBM_ERR_PARAM, "L2 promotion must be 0..3");
         CU(cudaStreamSynchronize(h->stream));
@@ -857,6 +938,7 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     case LBM_OPT_KERNEL: *value = h->use_march ? 2 : 1; return LBM_OK;
     case LBM_OPT_NBLOCKS: *value = h->use_march ? h->nblocks : 0; return LBM_OK;
     case LBM_OPT_L2PROMO: *value = h->l2promo; return LBM_OK;
+    case LBM_OPT_GRAPHS: *value = h->use_graphs; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

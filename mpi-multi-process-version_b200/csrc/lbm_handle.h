@@ -42,6 +42,8 @@ struct lbm_handle {
     int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
     int nblocks = 0;             // resolved persistent grid
     int l2promo = 0;             // LBM_OPT_L2PROMO
+    int use_graphs = 1;          // LBM_OPT_GRAPHS
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 2-step graphs from cur = 0 / 1
     int cur = 0;                 // buffer holding the newest populations
     int phase = 0;               // 0: not initialised, 1: pre-collision, 2: post-collision
     int64_t itc = 0;
@@ -59,4 +61,6 @@ bool encode_maps_tx(const lbm_handle *h, int tx, lbm::TmapSet out[2]);
 int first_collision(lbm_handle *h);
 // synchronise h's stream and report a kernel's bounded wait that gave up
 int sync_handle(lbm_handle *h);
+// release the captured step graphs (kernel choice or buffers changed)
+void drop_graphs(lbm_handle *h);
 }  // namespace lbm

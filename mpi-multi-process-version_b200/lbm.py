@@ -29,7 +29,7 @@ GRID = {"erf": 0, "tanh": 1, "uniform": 2}
 # every symbol include/lbm_b200.h declares
 EXPORTS = [
     "lbm_abi_version", "lbm_error_string", "lbm_last_error", "lbm_mesh", "lbm_mesh_box", "lbm_derived_params",
-    "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_itc",
+    "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_run", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
     "lbm_set_option", "lbm_get_option", "lbm_check_noalloc",
@@ -38,7 +38,7 @@ EXPORTS = [
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4}
-OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO = 1, 2, 3
+OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS = 1, 2, 3, 4
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 
@@ -83,6 +83,8 @@ def lib():
         L.lbm_init_equilibrium.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.lbm_step.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.lbm_itc.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
+                              ctypes.POINTER(ctypes.c_int64), _dp, _dp]
         L.lbm_check.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.lbm_nusselt.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.lbm_sums.argtypes = [ctypes.c_void_p, _dp, _dp]
@@ -280,6 +282,14 @@ class Cavity:
 
     def step(self, n: int = 1):
         _chk(lib().lbm_step(self.h, int(n)), "lbm_step")
+
+    def run(self, max_steps: int, check_every: int = 2000, eps: float = float(np.float32(1e-6))):
+        """lbm_run: iterate until both check() residuals are at most eps (tested
+        every check_every iterations) or max_steps.  Returns (steps, errU, errT)."""
+        n, a, b = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        _chk(lib().lbm_run(self.h, int(max_steps), int(check_every), float(eps), ctypes.byref(n), ctypes.byref(a),
+                           ctypes.byref(b)), "lbm_run")
+        return int(n.value), a.value, b.value
 
     @property
     def itc(self) -> int:

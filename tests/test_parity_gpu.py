@@ -267,3 +267,40 @@ def test_gpu_matches_reference_fixture(pkg, path, kernel):
         else:
             assert rel_err(f, d["f"]) <= 1e-12 and rel_err(g, d["g"]) <= 1e-12
         cav.close()
+
+
+@pytest.mark.parametrize("dim,shape,kernel", [(2, (64, 48, 1), "direct"), (2, (300, 40, 1), "march"),
+                                              (3, (40, 18, 12), "march"), (3, (14, 12, 10), "direct")])
+def test_graph_replay_is_bit_identical(pkg, dim, shape, kernel):
+    out = []
+    for graphs in (1, 0):
+        c = pkg.Cavity(dim, *shape, grid="tanh", stretch=1.5, mode="exact", kernel=kernel)
+        c.set_option(pkg.lbm.OPT_GRAPHS, graphs)
+        c.initial()
+        for n in (7, 1, 10, 3):
+            c.step(n)
+        out.append((c.macro(), c.populations()))
+        c.close()
+    for k in out[0][0]:
+        assert np.array_equal(out[0][0][k], out[1][0][k]), k
+    assert np.array_equal(out[0][1][0], out[1][1][0]) and np.array_equal(out[0][1][1], out[1][1][1])
+
+
+def test_run_matches_manual_loop(pkg):
+    a = pkg.Cavity(2, 40, 40, Ra=1e4, grid="tanh", stretch=1.5, mode="exact")
+    a.initial()
+    steps, eu, et = a.run(max_steps=3000, check_every=200, eps=1e-3)
+    b = pkg.Cavity(2, 40, 40, Ra=1e4, grid="tanh", stretch=1.5, mode="exact")
+    b.initial()
+    n, ref = 0, (100.0, 100.0)
+    while (ref[0] > 1e-3 or ref[1] > 1e-3) and n < 3000:
+        b.step(200)
+        n += 200
+        ref = b.check()
+    assert steps == n and (eu, et) == ref
+    assert steps % 200 == 0 and steps < 3000 and eu <= 1e-3 and et <= 1e-3
+    ma, mb = a.macro(), b.macro()
+    for k in ma:
+        assert np.array_equal(ma[k], mb[k])
+    a.close()
+    b.close()

@@ -134,6 +134,17 @@ int lbm_init_reference(lbm_handle *h);
 int lbm_init_equilibrium(lbm_handle *h, const double *rho, const double *u,
                          const double *v, const double *w, const double *T);
 
+/* Warm start (no counterpart in the reference, whose only initial state is
+ * the one of initial()): like lbm_init_equilibrium, plus the first-order
+ * Chapman-Enskog non-equilibrium part of the given fields,
+ *   f_a -= 3 tau_f dt w_a rho (e_a e_a : grad u - div u / 3)
+ *   g_a -= (dt / sig_k) wT_a (e_a . grad T)
+ * with gradients from the slope of the quadratic through each node's
+ * interpolation stencil (one-sided at the walls) on the stretched grid.
+ * Rejects non-finite field values with LBM_ERR_NONFINITE. */
+int lbm_init_warm(lbm_handle *h, const double *rho, const double *u,
+                  const double *v, const double *w, const double *T);
+
 /* Advance nsteps iterations of the reference loop body: collision_U,
  * collision_T, update (a no-op on one domain), interpolate, bounceback_u,
  * bounceback_T, macro_u, macro_t (2M:309-325, 3M:375-391).  Asynchronous. */
@@ -217,6 +228,10 @@ typedef struct lbm_batch lbm_batch;
 #define LBM_BATCH_OPT_NBLOCKS     2  /* persistent blocks (0 = one full wave) */
 #define LBM_BATCH_OPT_PERSISTENT  3  /* 1: one persistent kernel per step, 0: one launch per cavity */
 #define LBM_BATCH_OPT_GRAPHS      4  /* 1: replay steps from CUDA graphs */
+#define LBM_BATCH_OPT_GROWTH      5  /* lbm_batch_run stops a member whose residual is not finite or
+                                        exceeds this factor x its smallest one in the run and reports
+                                        it as converged = -1 (0, the default: off, a non-finite
+                                        residual ends the run with LBM_ERR_NONFINITE) */
 
 /* Create n cavities (same dim, storage, mode and device; any size and
  * parameters).  x[i], y[i], z[i] are the coordinate arrays of cavity i as for
@@ -241,6 +256,12 @@ int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold);
  * steps_done[i] (optional) report each member's outcome. */
 int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps,
                   int32_t *converged, int64_t *steps_done);
+/* lbm_batch_run over the members with mask[i] != 0 only (the others are not
+ * stepped); mask NULL selects every member.  With LBM_BATCH_OPT_GROWTH set,
+ * converged[i] = -1 marks a member stopped for a diverging residual (the
+ * warm-start driver restarts those from the conduction state). */
+int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
+                         double eps, int32_t *converged, int64_t *steps_done);
 /* Time each tile width and grid size on the batch itself (the timed steps
  * advance the members) and keep the fastest; reports the choice. */
 int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups);

@@ -39,6 +39,7 @@ UNITS = [
     ("capi.o", "lbm_capi.cu", []),
     ("noalloc.o", "lbm_noalloc.cu", []),
     ("batch.o", "lbm_batch.cu", []),
+    ("unet.o", "unet_kernels.cu", []),
 ]
 
 HEADERS = ["lbm_internal.h", "lbm_handle.h", "lbm_march.cuh"]
@@ -54,7 +55,8 @@ def _stale(target: str, deps: list[str]) -> bool:
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "lbm_b200.h")]
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", h)
+                                                        for h in ("lbm_b200.h", "lbm_surrogate.h")]
     objs = []
     for obj, src, extra in UNITS:
         o = os.path.join(BUILD, obj)

@@ -48,6 +48,7 @@ struct lbm_batch {
     int nblocks_opt = 0, nblocks = 0;
     int persistent = 1;            // 0: one launch per cavity
     int use_graphs = 1;
+    double growth = 0.0;           // residual growth factor that stops a member in lbm_batch_run (0: off)
     Geo *d_geo = nullptr;
     TmapSet *d_maps = nullptr;
     Bufs *d_bufs = nullptr;
@@ -366,46 +367,69 @@ extern "C" int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold)
     return LBM_OK;
 }
 
-extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps, int32_t *converged,
-                             int64_t *steps_done)
+extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
+                                    double eps, int32_t *converged, int64_t *steps_done)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
     if (max_steps < 0 || check_every < 1) return set_error(LBM_ERR_PARAM, "need max_steps >= 0, check_every >= 1");
-    std::vector<double> eu(b->n), et(b->n);
+    std::vector<double> eu(b->n), et(b->n), best(b->n, INFINITY);
+    std::vector<int> checks(b->n, 0);
+    int remaining = 0;
     for (int i = 0; i < b->n; ++i) {
+        const bool on = !mask || mask[i] != 0;
         if (converged) converged[i] = 0;
         if (steps_done) steps_done[i] = 0;
+        b->active[i] = on ? 1 : 0;
+        remaining += on ? 1 : 0;
     }
-    b->active.assign(b->n, 1);
     b->dirty = true;
     int64_t steps = 0;
-    int remaining = b->n;
+    int st = LBM_OK;
     while (steps < max_steps && remaining > 0) {
         const int k = (int)std::min<int64_t>(check_every, max_steps - steps);
-        int st = lbm_batch_step(b, k);
-        if (st) return st;
+        if ((st = lbm_batch_step(b, k))) break;
         steps += k;
-        st = lbm_batch_synchronize(b);
-        if (st) return st;
+        if ((st = lbm_batch_synchronize(b))) break;
         bool changed = false;
         for (int i = 0; i < b->n; ++i) {
             if (!b->active[i]) continue;
             st = lbm_check(b->cav[i], &eu[i], &et[i]);
-            if (st) return st;
             if (steps_done) steps_done[i] = steps;
-            // the reference keeps iterating while errorU > eps or errorT > eps (2M:307)
-            if (!(eu[i] > eps || et[i] > eps)) {
+            const double r = std::max(eu[i], et[i]);
+            // a member whose residual stops being finite, or grows past growth x
+            // its smallest value in this run, is stopped and reported as -1
+            const bool bad = st == LBM_ERR_NONFINITE || !std::isfinite(r) ||
+                             (b->growth > 0 && checks[i] >= 2 && r > b->growth * best[i]);
+            if (st && st != LBM_ERR_NONFINITE) break;
+            if (st == LBM_ERR_NONFINITE && b->growth <= 0) break;
+            st = LBM_OK;
+            ++checks[i];
+            best[i] = std::min(best[i], r);
+            if (bad) {
+                b->active[i] = 0;
+                if (converged) converged[i] = -1;
+                --remaining;
+                changed = true;
+            } else if (!(eu[i] > eps || et[i] > eps)) {
+                // the reference keeps iterating while errorU > eps or errorT > eps (2M:307)
                 b->active[i] = 0;
                 if (converged) converged[i] = 1;
                 --remaining;
                 changed = true;
             }
         }
+        if (st) break;
         if (changed) b->dirty = true;
     }
     b->active.assign(b->n, 1);
     b->dirty = true;
-    return LBM_OK;
+    return st;
+}
+
+extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps, int32_t *converged,
+                             int64_t *steps_done)
+{
+    return lbm_batch_run_masked(b, nullptr, max_steps, check_every, eps, converged, steps_done);
 }
 
 extern "C" int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
@@ -481,6 +505,10 @@ extern "C" int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value)
     case LBM_BATCH_OPT_GRAPHS:
         b->use_graphs = value != 0;
         break;
+    case LBM_BATCH_OPT_GROWTH:
+        if (value < 0) return set_error(LBM_ERR_PARAM, "growth factor must be >= 0");
+        b->growth = (double)value;
+        break;
     default:
         return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
@@ -496,6 +524,7 @@ extern "C" int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t 
     case LBM_BATCH_OPT_NBLOCKS: *value = b->nblocks; return LBM_OK;
     case LBM_BATCH_OPT_PERSISTENT: *value = b->persistent; return LBM_OK;
     case LBM_BATCH_OPT_GRAPHS: *value = b->use_graphs; return LBM_OK;
+    case LBM_BATCH_OPT_GROWTH: *value = (int64_t)b->growth; return LBM_OK;
     default: return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
 }

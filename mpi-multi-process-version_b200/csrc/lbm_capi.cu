@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <string>
+#include <cmath>
 #include <vector>
 
 #include "../../include/lbm_b200.h"
@@ -537,10 +538,15 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
         if (st_) return st_;                                              \
     } while (0)
 
-static cudaError_t launch_equilibrium(lbm_handle *h, void *pop)
+static cudaError_t launch_equilibrium(lbm_handle *h, void *pop, int neq = 0)
 {
-    return h->p.mode == LBM_MODE_EXACT ? exact::equilibrium(h->geo, h->p.storage, pop, h->bufs, h->stream)
-                                       : fast::equilibrium(h->geo, h->p.storage, pop, h->bufs, h->stream);
+    // first-order non-equilibrium coefficients: 3 tau_f dt and tau_T dt with
+    // tau_T = 1 / sig_k (the relaxation times of the stress and heat-flux moments)
+    const double cf = 3.0 * h->d.tauf * h->p.dt;
+    const double ct = (1.0 / h->d.sig_k) * h->p.dt;
+    return h->p.mode == LBM_MODE_EXACT
+               ? exact::equilibrium(h->geo, h->p.storage, pop, h->bufs, neq, cf, ct, h->stream)
+               : fast::equilibrium(h->geo, h->p.storage, pop, h->bufs, neq, cf, ct, h->stream);
 }
 
 static int reset_run(lbm_handle *h)
@@ -606,6 +612,30 @@ extern "C" int lbm_init_equilibrium(lbm_handle *h, const double *rho, const doub
     int st = upload_macro(h, rho, u, v, w, T);
     if (st) return st;
     CU(launch_equilibrium(h, h->bufs.pop[h->cur]));
+    if ((st = reset_run(h))) return st;
+    CU(cudaStreamSynchronize(h->stream));
+    h->phase = 1;
+    return LBM_OK;
+}
+
+extern "C" int lbm_init_warm(lbm_handle *h, const double *rho, const double *u, const double *v, const double *w,
+                             const double *T)
+{
+    CHECK_H(h);
+    if (!rho || !u || !v || !T) return fail(LBM_ERR_PARAM, "rho, u, v and T are required");
+    const int64_t N = h->geo.nnode;
+    for (int64_t n = 0; n < N; ++n)
+        if (!std::isfinite(rho[n]) || !std::isfinite(u[n]) || !std::isfinite(v[n]) || !std::isfinite(T[n]) ||
+            (w && h->p.dim == 3 && !std::isfinite(w[n])))
+            return fail(LBM_ERR_NONFINITE, "lbm_init_warm: non-finite field value at node %lld", (long long)n);
+    std::vector<double> zero;
+    if (h->p.dim == 3 && !w) {
+        zero.assign((size_t)N, 0.0);
+        w = zero.data();
+    }
+    int st = upload_macro(h, rho, u, v, w, T);
+    if (st) return st;
+    CU(launch_equilibrium(h, h->bufs.pop[h->cur], 1));
     if ((st = reset_run(h))) return st;
     CU(cudaStreamSynchronize(h->stream));
     h->phase = 1;

@@ -55,11 +55,20 @@ struct MarchShape {
 
 enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
 
+// Shifted FP16 storage keeps (f - w*rho0) * 2^12 and (g - w*T0) * 2^12 as
+// binary16.  The power-of-two scale is exact; it lifts the small deviations
+// from the shift (1e-8 .. 1e-3) out of the binary16 subnormal range (below
+// 6.1e-5), where the absolute step is 6e-8, while |f - w| < 16 still fits.
+constexpr float kF16Scale = 4096.0f;
+constexpr float kF16InvScale = 1.0f / 4096.0f;
+
 // kernel launchers; one set per arithmetic mode
 #define LBM_DECLARE_LAUNCHERS(NS)                                                             \
     namespace NS {                                                                            \
-    /* init: equilibrium populations from the macroscopic fields into pop */                  \
-    cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, cudaStream_t s); \
+    /* init: equilibrium populations from the macroscopic fields into pop; neq != 0 adds  */ \
+    /* the first-order non-equilibrium part, cf = 3 tau_f dt, ct = dt / sig_k              */ \
+    cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, int neq, double cf, double ct, \
+                            cudaStream_t s);                                                   \
     /* first collision of a run: pre-collision pop_in -> post-collision pop_out, F_out */     \
     cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out,           \
                         void *F_out, const Bufs &b, cudaStream_t s);                          \

@@ -46,18 +46,18 @@ template <> struct Tr<kF16S> { using S = __half; using C = float; static constex
 
 __device__ __forceinline__ double tocomp(double x) { return x; }
 __device__ __forceinline__ float tocomp(float x) { return x; }
-__device__ __forceinline__ float tocomp(__half x) { return __half2float(x); }
+__device__ __forceinline__ float tocomp(__half x) { return __half2float(x) * kF16InvScale; }
 
 template <class S> __device__ __forceinline__ S fromcomp(double x);
 template <> __device__ __forceinline__ double fromcomp<double>(double x) { return x; }
 template <class S> __device__ __forceinline__ S fromcompf(float x);
 template <> __device__ __forceinline__ float fromcompf<float>(float x) { return x; }
-template <> __device__ __forceinline__ __half fromcompf<__half>(float x) { return __float2half_rn(x); }
+template <> __device__ __forceinline__ __half fromcompf<__half>(float x) { return __float2half_rn(x * kF16Scale); }
 
 template <class S, class C> __device__ __forceinline__ S tostore(C x);
 template <> __device__ __forceinline__ double tostore<double, double>(double x) { return x; }
 template <> __device__ __forceinline__ float tostore<float, float>(float x) { return x; }
-template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x); }
+template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x * kF16Scale); }
 
 // lattice weights used as storage shifts (f - w*rho0, g - w*T0), rho0 = 1
 __device__ __forceinline__ float wU2(int q) { return q == 0 ? 4.0f / 9.0f : (q < 5 ? 1.0f / 9.0f : 1.0f / 36.0f); }
@@ -777,8 +777,47 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 // ---------------------------------------------------------------------------
 // initial equilibrium (2M:227-240, 3M:286-301) and the first collision
 // ---------------------------------------------------------------------------
+// d/dc at c = xm of the quadratic through (xa, qa), (xm, qm), (xb, qb)
+__device__ __forceinline__ double slope3(double xa, double qa, double xm, double qm, double xb, double qb)
+{
+    const double la = (xm - xb) / ((xa - xm) * (xa - xb));
+    const double lm = ((xm - xa) + (xm - xb)) / ((xm - xa) * (xm - xb));
+    const double lb = (xm - xa) / ((xb - xa) * (xb - xm));
+    return (qa * la + qm * lm) + qb * lb;
+}
+
+// gradient of a packed field q at node n = (i, j, k) (0-based) along the
+// three-node interpolation stencil of each axis (one-sided at both ends)
+__device__ __forceinline__ void grad3(const Geo &G, const double *__restrict__ q, int64_t n, int i, int j, int k,
+                                      double out[3])
+{
+    const int64_t sx = 1, sy = G.nx, sz = (int64_t)G.nx * G.ny;
+    const int ii[3] = {i, j, k};
+    const int nn[3] = {G.nx, G.ny, G.nz};
+    const int64_t st[3] = {sx, sy, sz};
+    for (int ax = 0; ax < 3; ++ax) {
+        if (ax == 2 && G.dim != 3) {
+            out[2] = 0.0;
+            break;
+        }
+        const int m = ii[ax] + 1;  // 1-based node of the coordinate table
+        int a, b;
+        if (m == 1) { a = m + 1; b = m + 2; }
+        else if (m == nn[ax]) { a = m - 1; b = m - 2; }
+        else { a = m - 1; b = m + 1; }
+        const double *c = G.coord[ax];
+        out[ax] = slope3(c[a], q[n + (a - m) * st[ax]], c[m], q[n], c[b], q[n + (b - m) * st[ax]]);
+    }
+}
+
+// Equilibrium populations of initial() (2M:227-240 / 3M:286-301) from the
+// macroscopic fields in B; with neq != 0 plus the first-order Chapman-Enskog
+// non-equilibrium part from the fields' gradients (warm starts):
+//   f_a -= (cf w_a rho) (e_a e_a : grad u - div u / 3),  cf = 3 tau_f dt
+//   g_a -= (ct wT_a) (e_a . grad T),                     ct = dt / sig_k
 template <int ST>
-__global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop, const Bufs B)
+__global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop, const Bufs B, int neq, double cf,
+                              double ct)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
@@ -798,15 +837,32 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
         const double wU[9] = {4.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/9.0, 1.0/36.0, 1.0/36.0, 1.0/36.0, 1.0/36.0};
         const double wT[5] = {1.0/2.0, 1.0/8.0, 1.0/8.0, 1.0/8.0, 1.0/8.0};
         const double velocitySquare = u*u+v*v;
+        double gu[3] = {0.0, 0.0, 0.0}, gv[3] = {0.0, 0.0, 0.0}, gT[3] = {0.0, 0.0, 0.0};
+        if (neq) {
+            grad3(G, B.u, n, i, j, k, gu);
+            grad3(G, B.v, n, i, j, k, gv);
+            grad3(G, B.T, n, i, j, k, gT);
+        }
+        const double div = (gu[0] + gv[1]) + 0.0;
         for (int a = 0; a < 9; ++a) {
             const double un = u*ex[a]+v*ey[a];
             double fa = rho*wU[a]*(1.0+3.0*un+4.5*un*un-1.5*velocitySquare);
+            if (neq) {
+                const double exa = ex[a], eya = ey[a];
+                double qq = (exa * exa) * gu[0] + (exa * eya) * (gv[0] + gu[1]) + (eya * eya) * gv[1];
+                qq = qq - div / 3.0;
+                fa = fa - ((cf * wU[a]) * rho) * qq;
+            }
             if (Tr<ST>::kShift) fa -= wU[a];
             pop[a * P + id] = tostore<S, C>(C(fa));
         }
         for (int a = 0; a < 5; ++a) {
             const double un = u*ex[a]+v*ey[a];
             double ga = wT[a]*T*(1.0+4.0*un);
+            if (neq) {
+                const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + 0 * gT[2];
+                ga = ga - (ct * wT[a]) * en;
+            }
             if (Tr<ST>::kShift) ga -= wT[a] * G.T0;
             pop[(9 + a) * P + id] = tostore<S, C>(C(ga));
         }
@@ -815,10 +871,25 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
         const int ey[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
         const int ez[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
         const double us2 = u*u+v*v+w*w;
+        double gu[3] = {0.0, 0.0, 0.0}, gv[3] = {0.0, 0.0, 0.0}, gw[3] = {0.0, 0.0, 0.0}, gT[3] = {0.0, 0.0, 0.0};
+        if (neq) {
+            grad3(G, B.u, n, i, j, k, gu);
+            grad3(G, B.v, n, i, j, k, gv);
+            grad3(G, B.w, n, i, j, k, gw);
+            grad3(G, B.T, n, i, j, k, gT);
+        }
+        const double div = (gu[0] + gv[1]) + gw[2];
         for (int a = 0; a < 19; ++a) {
             const double wa = a == 0 ? 1.0/3.0 : (a < 7 ? 1.0/18.0 : 1.0/36.0);
             const double un = u*ex[a]+v*ey[a]+w*ez[a];
             double fa = wa*rho*(1.0+3.0*un+4.5*un*un-1.5*us2);
+            if (neq) {
+                const double exa = ex[a], eya = ey[a], eza = ez[a];
+                double qq = (exa * exa) * gu[0] + (exa * eya) * (gv[0] + gu[1]) + (eya * eya) * gv[1];
+                qq = ((qq + (eza * eza) * gw[2]) + (exa * eza) * (gw[0] + gu[2])) + (eya * eza) * (gw[1] + gv[2]);
+                qq = qq - div / 3.0;
+                fa = fa - ((cf * wa) * rho) * qq;
+            }
             if (Tr<ST>::kShift) fa -= wa;
             pop[a * P + id] = tostore<S, C>(C(fa));
         }
@@ -826,6 +897,10 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
             const double wa = a == 0 ? 1.0/2.0 : 1.0/12.0;
             const double un = u*ex[a]+v*ey[a]+w*ez[a];
             double ga = wa*T*(1.0+6.0*un);
+            if (neq) {
+                const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + ez[a] * gT[2];
+                ga = ga - (ct * wa) * en;
+            }
             if (Tr<ST>::kShift) ga -= wa * G.T0;
             pop[(19 + a) * P + id] = tostore<S, C>(C(ga));
         }
@@ -931,17 +1006,18 @@ cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void 
 }
 
 template <int ST>
-static cudaError_t launch_eq(const Geo &g, void *pop, const Bufs &b, cudaStream_t s)
+static cudaError_t launch_eq(const Geo &g, void *pop, const Bufs &b, int neq, double cf, double ct, cudaStream_t s)
 {
     const int64_t n = g.nnode;
-    k_equilibrium<ST><<<unsigned((n + 255) / 256), 256, 0, s>>>(g, (typename Tr<ST>::S *)pop, b);
+    k_equilibrium<ST><<<unsigned((n + 255) / 256), 256, 0, s>>>(g, (typename Tr<ST>::S *)pop, b, neq, cf, ct);
     ++g_launches;
     return cudaGetLastError();
 }
 
-cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, cudaStream_t s)
+cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, int neq, double cf, double ct,
+                        cudaStream_t s)
 {
-#define CALL(ST) launch_eq<ST>(g, pop, b, s)
+#define CALL(ST) launch_eq<ST>(g, pop, b, neq, cf, ct, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }

@@ -207,7 +207,7 @@ __global__ void k_aos_to_planes(const Geo G, int q0, int nq, const double *__res
     const double val = aos[e];
     if (ST == kF64) ((double *)pop)[dst] = val;
     else if (ST == kF32) ((float *)pop)[dst] = float(val);
-    else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q)));
+    else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q)) * kF16Scale);
 }
 
 template <int ST>
@@ -221,7 +221,7 @@ __global__ void k_planes_to_aos(const Geo G, int q0, int nq, const void *pop, do
     double val;
     if (ST == kF64) val = ((const double *)pop)[src];
     else if (ST == kF32) val = double(((const float *)pop)[src]);
-    else val = double(__half2float(((const __half *)pop)[src])) + shift_of(G, q);
+    else val = double(__half2float(((const __half *)pop)[src]) * kF16InvScale) + shift_of(G, q);
     aos[e] = val;
 }
 
@@ -261,7 +261,7 @@ __global__ void k_macro_from_pops(const Geo G, const void *pop, const Bufs B)
         const int64_t a = (int64_t)q * G.plane + id;
         if (ST == kF64) return ((const double *)pop)[a];
         if (ST == kF32) return double(((const float *)pop)[a]);
-        return double(__half2float(((const __half *)pop)[a])) + shift_of(G, q);
+        return double(__half2float(((const __half *)pop)[a]) * kF16InvScale) + shift_of(G, q);
     };
     const int ex2[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
     const int ey2[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};

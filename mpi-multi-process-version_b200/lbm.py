@@ -29,15 +29,15 @@ GRID = {"erf": 0, "tanh": 1, "uniform": 2}
 # every symbol include/lbm_b200.h declares
 EXPORTS = [
     "lbm_abi_version", "lbm_error_string", "lbm_last_error", "lbm_mesh", "lbm_mesh_box", "lbm_derived_params",
-    "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_step", "lbm_run", "lbm_itc",
+    "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_init_warm", "lbm_step", "lbm_run", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
     "lbm_set_option", "lbm_get_option", "lbm_check_noalloc",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_size", "lbm_batch_cavity", "lbm_batch_init_reference",
-    "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_tune",
+    "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_run_masked", "lbm_batch_tune",
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
 ]
-BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4}
+BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS = 1, 2, 3, 4
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
@@ -81,6 +81,7 @@ def lib():
         L.lbm_destroy.argtypes = [ctypes.c_void_p]
         L.lbm_init_reference.argtypes = [ctypes.c_void_p]
         L.lbm_init_equilibrium.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.lbm_init_warm.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
         L.lbm_step.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.lbm_itc.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         L.lbm_run.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_double,
@@ -111,6 +112,8 @@ def lib():
         L.lbm_batch_nusselt.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.lbm_batch_run.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                     ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]
+        L.lbm_batch_run_masked.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
         L.lbm_batch_tune.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                      ctypes.POINTER(ctypes.c_int32), _dp]
         L.lbm_batch_set_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64]
@@ -278,6 +281,13 @@ class Cavity:
     def init_equilibrium(self, rho, u, v, w, T):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, w, T)]
         _chk(lib().lbm_init_equilibrium(self.h, *[_p(a) for a in arrs]), "lbm_init_equilibrium")
+        return self
+
+    def init_warm(self, rho, u, v, w, T):
+        """lbm_init_warm: equilibrium of the given fields plus the first-order
+        non-equilibrium part from their gradients (warm starts)."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, v, w, T)]
+        _chk(lib().lbm_init_warm(self.h, *[_p(a) for a in arrs]), "lbm_init_warm")
         return self
 
     def step(self, n: int = 1):
@@ -452,6 +462,17 @@ class Batch:
         done = (ctypes.c_int64 * self.n)()
         _chk(lib().lbm_batch_run(self.h, int(max_steps), int(check_every), float(eps), conv, done), "lbm_batch_run")
         return np.array(conv[:], dtype=bool), np.array(done[:], dtype=np.int64)
+
+    def run_masked(self, mask, max_steps, check_every=2000, eps=float(np.float32(1e-6))):
+        """lbm_batch_run_masked: only members with mask[i] run.  Returns the
+        status per member (1 converged, 0 not converged, -1 stopped for a
+        diverging residual) and the steps each member did."""
+        m = None if mask is None else (ctypes.c_int32 * self.n)(*[int(bool(v)) for v in mask])
+        conv = (ctypes.c_int32 * self.n)()
+        done = (ctypes.c_int64 * self.n)()
+        _chk(lib().lbm_batch_run_masked(self.h, m, int(max_steps), int(check_every), float(eps), conv, done),
+             "lbm_batch_run_masked")
+        return np.array(conv[:], dtype=np.int32), np.array(done[:], dtype=np.int64)
 
     def tune(self, steps=20):
         t, nb, v = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()

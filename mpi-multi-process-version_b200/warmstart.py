@@ -1,0 +1,445 @@
+"""Learned warm start for the differentially heated cavity.
+
+The reference starts every run from the conduction state of initial()
+(natural-convection_2dim_mono.f90:199-240) and iterates until the check()
+residuals fall below 1e-6 (2M:307).  Here a U-Net (surrogate.Net, trained on
+the GPU by this library's own kernels) predicts the steady (u, v, T) field of
+a cavity from (Ra, Pr, grid-coordinate maps); lbm_init_warm turns the
+prediction into populations (equilibrium plus the first-order
+non-equilibrium part), and the solver then runs to the same residual
+criterion as a cold start, so it alone judges the result.  A member whose
+residual diverges is restarted from the conduction state (the cold-start
+fallback).
+
+Representation.  Fields live on the cavity's nodes; the network sees an
+R x R image in index space (node i of n sits at (i + 1/2)/n, pixel r of R at
+(r + 1/2)/R; linear interpolation between the two).  Inputs: the wall-
+normalised physical node coordinates X, Y (which carry the grid stretching),
+(log10 Ra - 4.5)/1.5, (Pr - 3.855)/3.145 and (stretch - 1.5)/0.5.  Outputs:
+u/U0, v/U0 with U0 = Ma/sqrt(3) (the free-fall velocity of the reference's
+parameter choice, 2M:152-162) and (T - Tcold)/(Thot - Tcold), each
+standardised with the training set's mean and deviation.
+"""
+from __future__ import annotations
+
+import functools
+import json
+import time
+
+import numpy as np
+
+from . import lbm as L
+from . import surrogate as S
+
+F32_EPS = float(np.float32(1e-6))   # the reference's epsU/epsT (single-precision literals, 2M:35)
+
+
+# ---------------------------------------------------------------------------
+# index-space resampling
+# ---------------------------------------------------------------------------
+@functools.lru_cache(maxsize=64)
+def _interp_matrix(n_src: int, n_dst: int) -> np.ndarray:
+    xs = (np.arange(n_src) + 0.5) / n_src
+    xd = (np.arange(n_dst) + 0.5) / n_dst
+    W = np.zeros((n_dst, n_src))
+    for k, x in enumerate(xd):
+        j = np.searchsorted(xs, x) - 1
+        if j < 0:
+            W[k, 0] = 1.0
+        elif j >= n_src - 1:
+            W[k, n_src - 1] = 1.0
+        else:
+            t = (x - xs[j]) / (xs[j + 1] - xs[j])
+            W[k, j], W[k, j + 1] = 1.0 - t, t
+    return W
+
+
+def resample(a: np.ndarray, shape) -> np.ndarray:
+    """Bilinear resampling of a (ny, nx) field to `shape` in index space."""
+    a = np.asarray(a, dtype=np.float64)
+    Wy = _interp_matrix(a.shape[0], int(shape[0]))
+    Wx = _interp_matrix(a.shape[1], int(shape[1]))
+    return Wy @ a @ Wx.T
+
+
+def unit_coords(c, n, dt):
+    """Node coordinates 1..n of one axis scaled to [0, 1] between the two
+    halfway bounce-back walls (dt/2 outside the end nodes)."""
+    c = np.asarray(c, dtype=np.float64)
+    lo, hi = c[1] - 0.5 * dt, c[n] + 0.5 * dt
+    return (c[1:n + 1] - lo) / (hi - lo)
+
+
+# ---------------------------------------------------------------------------
+# cases
+# ---------------------------------------------------------------------------
+def sample_cases(n, seed, sizes=(128, 160, 192, 224, 256), log10_ra=(3.0, 6.0), pr=(0.71, 7.0),
+                 stretch=(1.0, 2.0)):
+    """Seeded square cavities: side from `sizes`, Ra log-uniform, Pr and the
+    tanh stretch uniform."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        side = int(rng.choice(sizes))
+        b = float(rng.uniform(*stretch))
+        out.append({"nx": side, "ny": side, "Ra": float(10 ** rng.uniform(*log10_ra)),
+                    "Pr": float(rng.uniform(*pr)), "grid": "tanh", "stretch": b,
+                    "coords": L.mesh_box(side, side, 0, 1.0, 1.0, 1.0, "tanh", b)})
+    return out
+
+
+NF = 8   # feature channels built on the host (the network's input has IN_CH, zero beyond NF)
+
+
+def features(case, R):
+    """(R, R, NF) float32 input image of one case."""
+    m = case["coords"]
+    nx, ny = case["nx"], case["ny"]
+    pix = (np.arange(R) + 0.5) / R
+    X = np.interp(pix, (np.arange(nx) + 0.5) / nx, unit_coords(m.x, nx, m.dt))
+    Y = np.interp(pix, (np.arange(ny) + 0.5) / ny, unit_coords(m.y, ny, m.dt))
+    f = np.zeros((R, R, NF), dtype=np.float32)
+    f[..., 0] = X[None, :]
+    f[..., 1] = Y[:, None]
+    f[..., 2] = (np.log10(case["Ra"]) - 4.5) / 1.5
+    f[..., 3] = (case["Pr"] - 3.855) / 3.145
+    f[..., 4] = (case.get("stretch", 1.5) - 1.5) / 0.5
+    return f
+
+
+def velocity_scale(case):
+    return float(case.get("Ma", 0.1)) / np.sqrt(3.0)
+
+
+def targets(case, fields, R):
+    """(R, R, 3) float32 target image (u/U0, v/U0, theta) of one steady field."""
+    U0 = velocity_scale(case)
+    Th, Tc = float(case.get("Thot", 1.0)), float(case.get("Tcold", 0.0))
+    chans = (fields["u"] / U0, fields["v"] / U0, (fields["T"] - Tc) / (Th - Tc))
+    return np.stack([resample(c, (R, R)) for c in chans], axis=-1).astype(np.float32)
+
+
+def fields_from_image(case, img):
+    """Invert `targets`: (R, R, 3) physical-scale image -> node fields."""
+    U0 = velocity_scale(case)
+    Th, Tc = float(case.get("Thot", 1.0)), float(case.get("Tcold", 0.0))
+    shape = (case["ny"], case["nx"])
+    u = resample(img[..., 0], shape) * U0
+    v = resample(img[..., 1], shape) * U0
+    T = Tc + resample(img[..., 2], shape) * (Th - Tc)
+    return {"rho": np.ones(shape), "u": u, "v": v, "T": T}
+
+
+# ---------------------------------------------------------------------------
+# the model
+# ---------------------------------------------------------------------------
+class WarmStart:
+    """The surrogate network plus its target normalisation."""
+
+    def __init__(self, R=128, device=0, seed=0):
+        self.net = S.Net(R=R, device=device, seed=seed)
+        self.R = R
+        self.mean = np.zeros(3, dtype=np.float32)
+        self.std = np.ones(3, dtype=np.float32)
+        self.history = []
+
+    # -- training ---------------------------------------------------------
+    def fit(self, X, Y, steps=3000, batch=16, lr=2e-3, warmup=100, seed=0, log_every=100, log=None):
+        """Train on inputs X (N, R, R, IN_CH) and targets Y (N, R, R, 3).
+        Adam with linear warm-up and cosine decay; samples drawn with a seeded
+        generator.  Returns the loss history [(step, loss)]."""
+        torch = self.net.torch
+        dev = self.net.dev
+        self.mean = Y.reshape(-1, 3).mean(0).astype(np.float32)
+        self.std = (Y.reshape(-1, 3).std(0) + 1e-6).astype(np.float32)
+        Xd = self._device_inputs(X)
+        Yd = torch.from_numpy(np.ascontiguousarray((Y - self.mean) / self.std, dtype=np.float32)).to(dev)
+        N = X.shape[0]
+        rng = np.random.default_rng(seed)
+        buf = self.net.buffers(batch)
+        tgt = torch.empty(batch * self.R * self.R, 3, dtype=torch.float32, device=dev)
+        hist = []
+        t0 = time.perf_counter()
+        for it in range(steps):
+            idx = torch.from_numpy(rng.integers(0, N, size=batch)).to(dev)
+            buf["x"].copy_(Xd.index_select(0, idx))
+            tgt.copy_(Yd.index_select(0, idx).reshape(-1, 3))
+            self.net.forward(B=batch)
+            loss = self.net.loss(tgt, batch)
+            self.net.backward(batch)
+            frac = it / max(1, steps - 1)
+            lr_t = lr * min(1.0, (it + 1) / warmup) * 0.5 * (1.0 + np.cos(np.pi * frac))
+            self.net.adam(lr_t)
+            if (it + 1) % log_every == 0 or it == steps - 1:
+                val = float(loss.item())
+                hist.append((it + 1, val))
+                if log:
+                    log(f"step {it + 1:6d}  loss {val:.5f}  lr {lr_t:.2e}  {time.perf_counter() - t0:.1f}s")
+        torch.cuda.synchronize(dev)
+        self.history += hist
+        self.train_seconds = time.perf_counter() - t0
+        return hist
+
+    def _device_inputs(self, X):
+        """(N, R, R, IN_CH) bf16 device tensor from host features (N, R, R, <= IN_CH)."""
+        torch = self.net.torch
+        Xd = torch.zeros(X.shape[0], self.R, self.R, S.IN_CH, dtype=torch.bfloat16, device=self.net.dev)
+        for k in range(0, X.shape[0], 256):
+            chunk = torch.from_numpy(np.ascontiguousarray(X[k:k + 256], dtype=np.float32))
+            Xd[k:k + chunk.shape[0], ..., :X.shape[-1]] = chunk.to(self.net.dev).to(torch.bfloat16)
+        return Xd
+
+    # -- inference --------------------------------------------------------
+    def predict_images(self, X, batch=16):
+        """Physical-scale (N, R, R, 3) predictions for inputs X."""
+        out = np.empty((X.shape[0], self.R, self.R, 3), dtype=np.float32)
+        for k in range(0, X.shape[0], batch):
+            xb = self._device_inputs(X[k:k + batch])
+            y = self.net.forward(xb).reshape(xb.shape[0], self.R, self.R, 3)
+            out[k:k + xb.shape[0]] = y.cpu().numpy()
+        return out * self.std + self.mean
+
+    def predict_fields(self, cases):
+        X = np.stack([features(c, self.R) for c in cases])
+        return [fields_from_image(c, img) for c, img in zip(cases, self.predict_images(X))]
+
+    # -- persistence ------------------------------------------------------
+    def save(self, path, meta=None):
+        """Weights as bf16 bit patterns (what the kernels use) plus the
+        normalisation and metadata."""
+        torch = self.net.torch
+        bits = self.net.master.to(torch.bfloat16).view(torch.int16).cpu().numpy()
+        np.savez_compressed(path, weights_bf16=bits, mean=self.mean, std=self.std, R=np.int32(self.R),
+                            meta=np.array(json.dumps(meta or {})))
+
+    @classmethod
+    def load(cls, path, device=0):
+        d = np.load(path, allow_pickle=False)
+        ws = cls(R=int(d["R"]), device=device)
+        torch = ws.net.torch
+        bits = torch.from_numpy(d["weights_bf16"].astype(np.int16))
+        master = bits.view(torch.bfloat16).to(torch.float32).numpy()
+        ws.net.load_state(master)
+        ws.mean, ws.std = d["mean"].astype(np.float32), d["std"].astype(np.float32)
+        ws.meta = json.loads(str(d["meta"]))
+        return ws
+
+
+# ---------------------------------------------------------------------------
+# solving to a steady state
+# ---------------------------------------------------------------------------
+def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
+          growth=100, want_fields=False, device=0, predictions=None):
+    """Run every case to the reference's stop criterion (errorU, errorT <= eps
+    at a check every `check_every` iterations) in one batch.
+
+    init "cold": the conduction state of initial(); "warm": the model's
+    prediction (or `predictions`, a list of node-field dicts) through
+    lbm_init_warm.  Members whose residual diverges (not finite, or growth x
+    above its smallest value) restart cold and their steps add up.
+    Returns a dict of per-case arrays and the wall time."""
+    specs = [{k: v for k, v in c.items()} for c in cases]
+    b = L.Batch(2, specs, storage=storage, device=device)
+    t_pred = 0.0
+    if init == "cold":
+        b.initial()
+    else:
+        t0 = time.perf_counter()
+        preds = predictions if predictions is not None else model.predict_fields(cases)
+        t_pred = time.perf_counter() - t0
+        for mem, f in zip(b.members, preds):
+            mem.init_warm(f["rho"], f["u"], f["v"], None, f["T"])
+    b.set_option("growth", int(growth))
+    b.synchronize()
+    t0 = time.perf_counter()
+    status, steps = b.run_masked(None, max_steps, check_every, eps)
+    fallback = status == -1
+    if fallback.any():
+        for i in np.nonzero(fallback)[0]:
+            b.members[i].initial()
+        st2, steps2 = b.run_masked(fallback, max_steps, check_every, eps)
+        status = np.where(fallback, st2, status)
+        steps = np.where(fallback, steps + steps2, steps)
+    b.synchronize()
+    seconds = time.perf_counter() - t0
+    nu_hot, nu_cold = b.nusselt()
+    out = {"status": status, "steps": steps, "fallback": fallback, "nu_hot": nu_hot, "nu_cold": nu_cold,
+           "seconds": seconds, "predict_seconds": t_pred, "nodes": np.array([m.nnode for m in b.members]),
+           "storage": storage, "init": init}
+    if want_fields:
+        out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
+    b.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# 3D cavities from the 2D model
+# ---------------------------------------------------------------------------
+def fields_3d_from_2d(case3d, model):
+    """Warm-start fields of a 3D cube from the 2D model: the cube is heated
+    along y and gravity points along -z (3M:563, 953-956), so the 2D image's
+    (x, y, u, v) map to the cube's (y, z, v, w); the prediction is extruded
+    along x with u = 0."""
+    m = case3d["coords"]
+    nx, ny, nz = case3d["nx"], case3d["ny"], case3d["nz"]
+    c2 = {"nx": ny, "ny": nz, "Ra": case3d["Ra"], "Pr": case3d["Pr"], "stretch": case3d.get("stretch", 1.5),
+          "coords": L.Mesh(m.y, m.z, None, m.dx0, m.length_LB, m.dt)}
+    f2 = model.predict_fields([c2])[0]                # arrays (nz, ny)
+    shape = (nz, ny, nx)
+    ext = lambda a: np.broadcast_to(a[:, :, None], shape).copy()  # noqa: E731
+    return {"rho": np.ones(shape), "u": np.zeros(shape), "v": ext(f2["u"]), "w": ext(f2["v"]), "T": ext(f2["T"])}
+
+
+# ---------------------------------------------------------------------------
+# the pipeline: solver-generated data -> training -> held-out evaluation
+# ---------------------------------------------------------------------------
+def build_dataset(cases, R, storage="f32", eps=1e-5, max_steps=400_000, log=print):
+    """Steady fields of `cases` from the solver (cold start, one batch) and
+    their (features, targets) images."""
+    t0 = time.perf_counter()
+    res = solve(cases, init="cold", storage=storage, eps=eps, max_steps=max_steps, want_fields=True)
+    X = np.stack([features(c, R) for c in cases])
+    Y = np.stack([targets(c, f, R) for c, f in zip(cases, res["fields"])])
+    if log:
+        log(f"dataset: {len(cases)} cases, {int((res['status'] == 1).sum())} converged to {eps:g}, "
+            f"{int(np.sum(res['steps'] * res['nodes'])) / 1e9:.1f} G lattice updates in "
+            f"{time.perf_counter() - t0:.0f} s")
+    return X, Y, res
+
+
+def step_seconds(sizes, storage="f64", steps=4000):
+    """Measured seconds per iteration of one square cavity of each side
+    (one cavity per launch: the drop-in's time)."""
+    out = {}
+    for n in sizes:
+        c = L.Cavity(2, n, n, Ra=1e5, grid="tanh", stretch=1.5, storage=storage)
+        c.initial()
+        c.step(200)
+        c.synchronize()
+        t0 = time.perf_counter()
+        c.step(steps)
+        c.synchronize()
+        out[int(n)] = (time.perf_counter() - t0) / steps
+        c.close()
+    return out
+
+
+def evaluate(model, cases, max_steps=1_500_000, log=print):
+    """Steps and time to the reference's criterion for FP64 cold (the drop-in)
+    and FP32 warm (mixed precision + batch + warm start), Nu error against the
+    FP64 fixed point (FP64 continued to residual 1e-8), plus the two
+    single-change variants."""
+    rows = {}
+    b = L.Batch(2, [dict(c) for c in cases], storage="f64")
+    b.initial()
+    b.synchronize()
+    t0 = time.perf_counter()
+    st, steps = b.run_masked(None, max_steps, 2000, F32_EPS)
+    b.synchronize()
+    rows["f64_cold"] = {"status": st, "steps": steps, "seconds": time.perf_counter() - t0,
+                        "nu": b.nusselt()[0]}
+    st2, steps2 = b.run_masked(None, max_steps, 2000, 1e-8)
+    rows["f64_ref"] = {"status": st2, "steps": steps + steps2, "nu": b.nusselt()[0]}
+    b.close()
+    if log:
+        log(f"f64 cold: {rows['f64_cold']['seconds']:.1f} s, converged {int((st == 1).sum())}/{len(cases)}")
+    for name, init, storage in (("f32_warm", "warm", "f32"), ("f32_cold", "cold", "f32"), ("f64_warm", "warm", "f64")):
+        r = solve(cases, init=init, model=model, storage=storage, max_steps=max_steps)
+        rows[name] = {"status": r["status"], "steps": r["steps"], "seconds": r["seconds"], "nu": r["nu_hot"],
+                      "fallback": r["fallback"], "predict_seconds": r["predict_seconds"]}
+        if log:
+            log(f"{name}: {r['seconds']:.1f} s (+{r['predict_seconds']:.2f} s prediction), converged "
+                f"{int((r['status'] == 1).sum())}/{len(cases)}, fallbacks {int(r['fallback'].sum())}")
+    return rows
+
+
+def _jsonable(x):
+    if isinstance(x, dict):
+        return {k: _jsonable(v) for k, v in x.items()}
+    if isinstance(x, np.ndarray):
+        return x.tolist()
+    if isinstance(x, (np.floating, np.integer)):
+        return x.item()
+    return x
+
+
+def main(argv=None):
+    """pipeline [--train N] [--test N] [--sizes a,b,..] [--R R] [--steps S]
+    [--data-steps M] [--eval-steps M] [--out DIR]"""
+    import argparse
+    import os
+    import sys
+    ap = argparse.ArgumentParser(prog="warmstart")
+    ap.add_argument("what", choices=["pipeline"])
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--test", type=int, default=200)
+    ap.add_argument("--sizes", default="128,160,192,224,256")
+    ap.add_argument("--R", type=int, default=128)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--data-eps", type=float, default=1e-5)
+    ap.add_argument("--data-steps", type=int, default=400_000)
+    ap.add_argument("--eval-steps", type=int, default=1_500_000)
+    ap.add_argument("--with3d", type=int, default=0, help="side of a 3D cube to evaluate (0: none)")
+    ap.add_argument("--out", default="warmstart_out")
+    a = ap.parse_args(sys.argv[1:] if argv is None else argv)
+    os.makedirs(a.out, exist_ok=True)
+    sizes = tuple(int(s) for s in a.sizes.split(","))
+    logf = open(os.path.join(a.out, "log.txt"), "a")
+
+    def log(msg):
+        print(msg, flush=True)
+        logf.write(msg + "\n")
+        logf.flush()
+
+    train_cases = sample_cases(a.train, seed=1000, sizes=sizes)
+    test_cases = sample_cases(a.test, seed=2000, sizes=sizes)
+    X, Y, _ = build_dataset(train_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
+    Xt, Yt, _ = build_dataset(test_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
+    model = WarmStart(R=a.R, seed=0)
+    model.fit(X, Y, steps=a.steps, batch=a.batch, lr=a.lr, log_every=250, log=log)
+    log(f"training: {a.steps} steps of {a.batch} in {model.train_seconds:.1f} s")
+    pred = model.predict_images(Xt)
+    rel = [float(np.linalg.norm(pred[..., k] - Yt[..., k]) / np.linalg.norm(Yt[..., k] - (k == 2) * 0.0))
+           for k in range(3)]
+    log(f"held-out relative L2 error (u, v, theta): {rel}")
+    meta = {"train": a.train, "test": a.test, "sizes": sizes, "R": a.R, "steps": a.steps, "batch": a.batch,
+            "lr": a.lr, "data_eps": a.data_eps, "data_steps": a.data_steps, "train_seed": 1000, "test_seed": 2000,
+            "heldout_rel_l2": rel, "train_seconds": model.train_seconds}
+    model.save(os.path.join(a.out, "warmstart_unet.npz"), meta)
+    rows = evaluate(model, test_cases, max_steps=a.eval_steps, log=log)
+    tstep = step_seconds(sorted(set(sizes)))
+    side = np.array([c["nx"] for c in test_cases])
+    rows["f64_cold"]["sequential_seconds"] = float(sum(rows["f64_cold"]["steps"][i] * tstep[int(side[i])]
+                                                       for i in range(len(side))))
+    out = {"meta": meta, "cases": [{k: v for k, v in c.items() if k != "coords"} for c in test_cases],
+           "step_seconds_f64_single": tstep, "rows": rows, "history": model.history}
+    if a.with3d:
+        n = a.with3d
+        m3 = L.mesh_box(n, n, n, 1.0, 1.0, 1.0, "tanh", 1.5)
+        c3 = {"nx": n, "ny": n, "nz": n, "Ra": 1e5, "Pr": 0.71, "stretch": 1.5, "coords": m3}
+        res3 = {}
+        for init in ("cold", "warm"):
+            cav = L.Cavity(3, n, n, n, Ra=1e5, Pr=0.71, coords=m3)
+            if init == "cold":
+                cav.initial()
+            else:
+                f = fields_3d_from_2d(c3, model)
+                cav.init_warm(f["rho"], f["u"], f["v"], f["w"], f["T"])
+            cav.synchronize()
+            t0 = time.perf_counter()
+            steps, eu, et = cav.run(a.eval_steps, 2000, F32_EPS)
+            cav.synchronize()
+            res3[init] = {"steps": int(steps), "seconds": time.perf_counter() - t0, "nu": cav.nusselt()[0],
+                          "errU": eu, "errT": et}
+            log(f"3D {n}^3 {init}: {res3[init]}")
+            cav.close()
+        out["cube"] = res3
+    with open(os.path.join(a.out, "eval.json"), "w") as f:
+        json.dump(_jsonable(out), f)
+    log("done")
+
+
+if __name__ == "__main__":
+    main()

@@ -266,6 +266,81 @@ void ora_set_macro(ora_state *s, const double *rho, const double *u, const doubl
     for (long id = 0; id < N; ++id) equilibrium(s, id);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Warm-start initial state (new, no reference counterpart): the equilibrium  */
+/* of 2M:227-240 / 3M:286-301 plus the first-order Chapman-Enskog            */
+/* non-equilibrium part built from gradients of the given fields:            */
+/*   f_a += -3 tau_f dt w_a rho (e_a e_a : grad u - div u / 3)               */
+/*   g_a += -tau_T dt wT_a (e_a . grad T),   tau_T = 1 / sig_k               */
+/* (tau_f relaxes the second-order moments of the MRT set, sig_k the heat    */
+/* flux moments).  Gradients: slope at node m of the quadratic through the   */
+/* three nodes of the interpolation stencil (inter_x order, 2B:246-296).     */
+/* ------------------------------------------------------------------------ */
+
+/* d/dc at c = xm of the quadratic through (xa, qa), (xm, qm), (xb, qb) */
+double ora_slope3(double xa, double qa, double xm, double qm, double xb, double qb)
+{
+    const double la = (xm - xb) / ((xa - xm) * (xa - xb));
+    const double lm = ((xm - xa) + (xm - xb)) / ((xm - xa) * (xm - xb));
+    const double lb = (xm - xa) / ((xb - xa) * (xb - xm));
+    return (qa * la + qm * lm) + qb * lb;
+}
+
+/* stencil partners of node i (1..n) along one axis */
+static void stencil_ab(int i, int n, int *a, int *b)
+{
+    if (i == 1) { *a = i + 1; *b = i + 2; }
+    else if (i == n) { *a = i - 1; *b = i - 2; }
+    else { *a = i - 1; *b = i + 1; }
+}
+
+/* gradient (d/dx, d/dy, d/dz) of field q at node (i, j, k) */
+static void grad3(const ora_state *s, const double *q, int i, int j, int k, double out[3])
+{
+    int a, b;
+    stencil_ab(i, s->nx, &a, &b);
+    out[0] = ora_slope3(s->x[a], q[NID(s, a, j, k)], s->x[i], q[NID(s, i, j, k)], s->x[b], q[NID(s, b, j, k)]);
+    stencil_ab(j, s->ny, &a, &b);
+    out[1] = ora_slope3(s->y[a], q[NID(s, i, a, k)], s->y[j], q[NID(s, i, j, k)], s->y[b], q[NID(s, i, b, k)]);
+    out[2] = 0.0;
+    if (s->dim == 3) {
+        stencil_ab(k, s->nz, &a, &b);
+        out[2] = ora_slope3(s->z[a], q[NID(s, i, j, a)], s->z[k], q[NID(s, i, j, k)], s->z[b], q[NID(s, i, j, b)]);
+    }
+}
+
+void ora_set_macro_neq(ora_state *s, const double *rho, const double *u, const double *v,
+                       const double *w, const double *T)
+{
+    ora_set_macro(s, rho, u, v, w, T);
+    const double cf = 3.0 * s->tauf * s->dt;
+    const double ct = (1.0 / s->sig_k) * s->dt;
+    for (int k = 1; k <= s->nz; ++k)
+        for (int j = 1; j <= s->ny; ++j)
+            for (int i = 1; i <= s->nx; ++i) {
+                const long id = NID(s, i, j, k);
+                double gu[3], gv[3], gw[3] = {0.0, 0.0, 0.0}, gT[3];
+                grad3(s, s->u, i, j, k, gu);
+                grad3(s, s->v, i, j, k, gv);
+                if (s->dim == 3) grad3(s, s->w, i, j, k, gw);
+                grad3(s, s->temp, i, j, k, gT);
+                const double div = (gu[0] + gv[1]) + gw[2];
+                double *f = s->f + id * s->Q, *g = s->g + id * s->QT;
+                for (int a = 0; a < s->Q; ++a) {
+                    const double ex = s->ex[a], ey = s->ey[a], ez = s->ez[a];
+                    double qq = (ex * ex) * gu[0] + (ex * ey) * (gv[0] + gu[1]) + (ey * ey) * gv[1];
+                    if (s->dim == 3)
+                        qq = ((qq + (ez * ez) * gw[2]) + (ex * ez) * (gw[0] + gu[2])) + (ey * ez) * (gw[1] + gv[2]);
+                    qq = qq - div / 3.0;
+                    f[a] = f[a] - ((cf * s->omega_U[a]) * s->rho[id]) * qq;
+                }
+                for (int a = 0; a < s->QT; ++a) {
+                    const double en = (s->ex[a] * gT[0] + s->ey[a] * gT[1]) + s->ez[a] * gT[2];
+                    g[a] = g[a] - (ct * s->omega_T[a]) * en;
+                }
+            }
+}
+
 void ora_destroy(ora_state *s)
 {
     if (!s) return;

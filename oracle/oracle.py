@@ -42,6 +42,9 @@ def lib():
                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.ora_set_macro.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.ora_set_macro_neq.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.ora_slope3.argtypes = [ctypes.c_double] * 6
+        L.ora_slope3.restype = ctypes.c_double
         L.ora_destroy.argtypes = [ctypes.c_void_p]
         L.ora_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.ora_check.argtypes = [ctypes.c_void_p, _dp, _dp]
@@ -141,6 +144,15 @@ class Oracle:
         lib().ora_set_macro(self.h, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]),
                             _p(wa) if wa is not None else None, _p(Ta))
 
+    def set_macro_neq(self, rho, u, v, w, T):
+        """Warm-start state: equilibrium plus the first-order non-equilibrium
+        part from the fields' gradients (ora_set_macro_neq)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).ravel() for a in (rho, u, v)]
+        wa = np.ascontiguousarray(w, dtype=np.float64).ravel() if w is not None else None
+        Ta = np.ascontiguousarray(T, dtype=np.float64).ravel()
+        lib().ora_set_macro_neq(self.h, _p(arrs[0]), _p(arrs[1]), _p(arrs[2]),
+                                _p(wa) if wa is not None else None, _p(Ta))
+
     def step(self, n=1):
         lib().ora_step(self.h, int(n))
 
@@ -172,6 +184,10 @@ class Oracle:
 
 def interpolateF(x0, x1, x2, x, f0, f1, f2):
     return lib().ora_interpolateF(x0, x1, x2, x, f0, f1, f2)
+
+
+def slope3(xa, qa, xm, qm, xb, qb):
+    return lib().ora_slope3(xa, qa, xm, qm, xb, qb)
 
 
 def set_threads(n: int):

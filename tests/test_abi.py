@@ -12,8 +12,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
-    hdr = open(os.path.join(ROOT, "include", "lbm_b200.h")).read()
+def declared_symbols(header="lbm_b200.h"):
+    hdr = open(os.path.join(ROOT, "include", header)).read()
     hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
     return sorted(set(re.findall(r"\b(lbm_[a-z0-9_]+)\s*\(", hdr)))
 
@@ -25,6 +25,21 @@ def test_library_exports_every_declared_symbol(pkg):
     for s in syms:
         assert hasattr(L, s), f"{s} declared in lbm_b200.h but not exported"
     assert sorted(pkg.EXPORTS) == syms
+
+
+def test_library_exports_every_surrogate_symbol(pkg):
+    L = pkg.lib()
+    syms = declared_symbols("lbm_surrogate.h")
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(L, s), f"{s} declared in lbm_surrogate.h but not exported"
+    assert sorted(pkg.surrogate.NN_EXPORTS) == syms
+    pkg.surrogate.nn()  # every signature binds
+
+
+def test_include_headers_are_covered():
+    # every header of the C ABI is checked by one of the export tests above
+    assert sorted(os.listdir(os.path.join(ROOT, "include"))) == ["lbm_b200.h", "lbm_surrogate.h"]
 
 
 def test_abi_version(pkg):

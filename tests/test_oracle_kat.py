@@ -111,3 +111,58 @@ def test_nusselt_of_linear_conduction_profile(ora):
         vol = (hi - lo) ** dim
         assert mass == pytest.approx(vol, rel=1e-12)
         assert energy == pytest.approx(0.5 * vol, rel=1e-9)
+
+
+def test_slope3_exact_on_quadratics(ora):
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        x = rng.uniform(0, 10, 3)
+        if min(abs(x[0] - x[1]), abs(x[0] - x[2]), abs(x[1] - x[2])) < 1e-2:
+            continue
+        a, b, c = rng.normal(size=3)
+        q = lambda t: a * t * t + b * t + c  # noqa: E731
+        got = ora.slope3(x[0], q(x[0]), x[1], q(x[1]), x[2], q(x[2]))
+        assert got == pytest.approx(2 * a * x[1] + b, rel=1e-9, abs=1e-9)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_warm_start_non_equilibrium_moments(ora, dim):
+    # Linear fields have exact stencil gradients.  The added part must carry
+    # no mass and no momentum, its second moment must be the Chapman-Enskog
+    # stress -tau_f dt rho / 3 (du_a/dx_b + du_b/dx_a), and its thermal first
+    # moment the diffusive flux -(dt / sig_k) cs_T^2 grad T.
+    n = 9
+    o = ora.Oracle(dim, n, n + 2, n + 1 if dim == 3 else 1, grid="tanh", stretch=1.5, Ra=1e4)
+    shape = o.shape
+    ax = [o.coords(a) for a in ("x", "y", "z")[:dim]]
+    grids = np.meshgrid(*[c[1:-1] for c in ax[::-1]], indexing="ij")[::-1]  # x, y(, z) arrays of `shape`
+    rng = np.random.default_rng(3)
+    G = rng.normal(scale=1e-4, size=(dim, dim))  # G[a, b] = d u_b / d x_a
+    gT = rng.normal(scale=1e-3, size=dim)
+    vel = [sum(G[a, b] * grids[a] for a in range(dim)) for b in range(dim)]
+    T = 0.5 + sum(gT[a] * grids[a] for a in range(dim))
+    rho = np.full(shape, 1.02)
+    w = vel[2] if dim == 3 else None
+    o.set_macro(rho, vel[0], vel[1], w, T)
+    f0, g0 = o.pops("f"), o.pops("g")
+    o.set_macro_neq(rho, vel[0], vel[1], w, T)
+    df, dg = o.pops("f") - f0, o.pops("g") - g0
+    p = o.params()
+    ex = np.array([[0, 1, 0, -1, 0, 1, -1, -1, 1], [0, 0, 1, 0, -1, 1, 1, -1, -1]]) if dim == 2 else np.array([
+        [0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0],
+        [0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1],
+        [0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1]])
+    QT = 5 if dim == 2 else 7
+    assert np.abs(df.sum(-1)).max() < 1e-15
+    for a in range(dim):
+        assert np.abs((df * ex[a]).sum(-1)).max() < 1e-15
+        for b in range(dim):
+            pi = (df * ex[a] * ex[b]).sum(-1)
+            expect = -p["tauf"] * o.dt * 1.02 / 3.0 * (G[a, b] + G[b, a])
+            assert np.abs(pi - expect).max() <= 1e-10 * max(abs(expect), 1e-9), (a, b)
+    cs2T = 0.25 if dim == 2 else 1.0 / 6.0
+    assert np.abs(dg.sum(-1)).max() < 1e-15
+    for a in range(dim):
+        flux = (dg * ex[a][:QT]).sum(-1)
+        expect = -(o.dt / p["sig_k"]) * cs2T * gT[a]
+        assert np.abs(flux - expect).max() <= 1e-10 * abs(expect), a  # cancellation in g - g_eq

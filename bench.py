@@ -173,10 +173,53 @@ def dist_setup():
     return world, rank, local
 
 
+def run_reference_batch(args):
+    """batch256 on the CPU: the C restatement advances the first cavities of
+    the same seeded sweep, one iteration of each per step (a bounded sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    oracle.set_threads(os.cpu_count() or 1)
+    specs = pkg.sweep_specs(256, seed=0)[:8]
+    orc = []
+    for sp in specs:
+        m = sp["coords"]
+        o = oracle.Oracle(2, sp["nx"], sp["ny"], 1, x=m.x, y=m.y, dt=m.dt, length_LB=m.length_LB, Ra=sp["Ra"],
+                          Pr=sp["Pr"])
+        orc.append(o)
+    for _ in range(args.warmup):
+        for o in orc:
+            o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for o in orc:
+            o.step(1)
+    dt = time.perf_counter() - t0
+    nodes = sum(sp["nx"] * sp["ny"] for sp in specs)
+    v = nodes * args.steps / dt / 1e6
+    line = {"impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batch256", "sample": "first 8 cavities of the seed-0 sweep, one iteration each "
+                                                         "per step", "nodes": nodes},
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
+                             "sample": f"{args.steps} iterations of 8 sweep cavities ({nodes} nodes)"},
+            "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
-    wl = WORKLOADS[args.workload]
     if rank != 0:
         return
+    if args.workload == "batch256":
+        return run_reference_batch(args)
+    if args.workload == "steady":
+        print(json.dumps({"impl": "reference", "unavailable": "time to a steady state of the CPU restatement is "
+                          "hours at these sizes (10^5-10^6 iterations per cavity); its per-iteration rate is the "
+                          "reference arm of the cavity workloads"}), flush=True)
+        return
+    wl = WORKLOADS[args.workload]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
@@ -227,15 +270,41 @@ def add_kernel_config(cfg, cav, pkg):
     return cfg
 
 
+def _reduce(x: float, world: int, op: str) -> float:
+    """max / sum of a host scalar over ranks (NCCL; identity on one rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
 def run_batch(args, world, rank, local):
     """The seeded sweep of 256 2D cavities (widths 64..512, aspect 1-4, Ra
     1e3..1e6, Pr 0.71..7, tanh stretch 1..2) through one persistent kernel per
-    step, against stepping each cavity with its own launch (FP64)."""
+    step, against stepping each cavity with its own launch (same precision).
+    On N ranks each rank advances its own seeded sweep (seed = rank: weak
+    scaling), or with --batch-shard one sweep split by LPT over node counts
+    (strong scaling); no data crosses ranks while stepping."""
     import torch
     torch.cuda.set_device(local)
     from __graft_entry__ import load_package
     pkg = load_package()
-    specs = pkg.sweep_specs(256, seed=0)
+    if args.batch_shard:
+        all_specs = pkg.sweep_specs(256, seed=0)
+        idx, specs = pkg.sharding.my_share(all_specs, world, rank)
+        n_total, scaling = len(all_specs), "strong"
+    else:
+        specs = pkg.sweep_specs(256, seed=rank)
+        idx, n_total, scaling = list(range(rank * 256, rank * 256 + 256)), 256 * world, "weak"
     b = pkg.Batch(2, specs, storage=args.storage, mode=args.mode, device=local)
     b.initial()
     tuned = b.tune(steps=6)
@@ -243,13 +312,15 @@ def run_batch(args, world, rank, local):
 
     def timed(nsteps, reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        _barrier(world)
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(reps):
             b.step(nsteps)
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        _barrier(world)
+        return _reduce(e0.elapsed_time(e1), world, "max")
 
     for _ in range(args.warmup):
         b.step(args.inner)
@@ -265,14 +336,15 @@ def run_batch(args, world, rank, local):
     launches = pkg.kernel_launches() - l0
     clocks = sampler.stop() if sampler else None
     nodes = b.nodes
+    nodes_all = _reduce(float(nodes), world, "sum")
     iters = args.steps * args.inner
-    value = world * nodes * iters / (ms / 1e3) / 1e6
+    value = nodes_all * iters / (ms / 1e3) / 1e6
     # one launch per cavity per step, same batch and precision
     b.set_option("persistent", 0)
     b.step(2)
     base_steps = max(2, args.inner // 10)
     ms_base = timed(base_steps, 2)
-    baseline = nodes * base_steps * 2 / (ms_base / 1e3) / 1e6
+    baseline = nodes_all * base_steps * 2 / (ms_base / 1e3) / 1e6
     b.set_option("persistent", 1)
     bpl = bytes_per_lup(2, args.storage)
     peak, peak_kind = measured_peak()
@@ -284,32 +356,39 @@ def run_batch(args, world, rank, local):
         big = max(m.nnode for m in b.members)
         pin = {k: torch.zeros(big, dtype=torch.float64, pin_memory=True).numpy() for k in ("rho", "u", "v", "T")}
         pin["rho"][:] = 1.0
+        reps = max(1, args.steps // 4)
+        _barrier(world)
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
-        for _ in range(max(1, args.steps // 4)):
+        for _ in range(reps):
             for m in b.members:
                 nn = m.nnode
                 m.init_equilibrium(*(pin[k][:nn].reshape(m.shape) for k in ("rho", "u", "v")), None,
                                    pin["T"][:nn].reshape(m.shape))
             b.step(args.inner)
-            b.nusselt()
+            nu_hot, _ = b.nusselt()
         f1.record(stream)
         torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1)
-        reps = max(1, args.steps // 4)
-        e2e = {"value": world * nodes * args.inner * reps / (ems / 1e3) / 1e6, "unit": "MLUPS",
+        _barrier(world)
+        ems = _reduce(f0.elapsed_time(f1), world, "max")
+        e2e = {"value": nodes_all * args.inner * reps / (ems / 1e3) / 1e6, "unit": "MLUPS",
                "h2d_bytes_per_step": 4 * nodes * 8, "d2h_bytes_per_step": 2 * 8 * len(specs),
                "path": "lbm_init_equilibrium per member (pinned host fields) + lbm_batch_step + lbm_batch_nusselt"}
+        # the one collective of the data path: every cavity's result to every rank
+        got = pkg.sharding.gather_by_index(idx, {"nu_hot": nu_hot}, n_total)
+        e2e["nusselt_gathered"] = int(np.isfinite(got["nu_hot"]).sum())
     if rank == 0:
         line = {
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": scaling,
             "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-            "config": {"workload": "batch256", "cavities": len(specs), "nodes": nodes, "lattice": "D2Q9+D2Q5",
-                       "sweep": "widths {64..512}, aspect 1-4, Ra 1e3-1e6 log, Pr 0.71-7, tanh stretch 1-2, seed 0",
+            "config": {"workload": "batch256", "cavities": n_total, "nodes": int(nodes_all), "lattice": "D2Q9+D2Q5",
+                       "sweep": "widths {64..512}, aspect 1-4, Ra 1e3-1e6 log, Pr 0.71-7, tanh stretch 1-2, "
+                                + ("seed 0 split over ranks by LPT" if args.batch_shard else "seed = rank"),
                        "storage": args.storage, "mode": args.mode, "iterations_per_step": args.inner,
                        "tile": tuned["tile"], "blocks": tuned["nblocks"], "graphs": True,
+                       "l2": "state larger than L2 (%.1f GB per GPU)" % (nodes * bpl / 2 / 1e9),
                        "one_launch_per_cavity_mlups": baseline,
                        "speedup_vs_one_launch_per_cavity": value / baseline if baseline else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -318,6 +397,100 @@ def run_batch(args, world, rank, local):
         }
         print(json.dumps(line), flush=True)
     b.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+MODEL_PATH = os.path.join(ROOT, "mpi-multi-process-version_b200", "warmstart_unet.npz")
+
+
+def run_steady(args, world, rank, local):
+    """Time to a steady state on held-out cavities (square, sides 128..256,
+    Ra 1e3..1e6 log-uniform, Pr 0.71..7, tanh stretch 1..2; the first
+    --cases of the held-out seed the warm-start model never saw): the FP64
+    drop-in from the conduction state, one cavity per launch, against FP32
+    storage + one persistent batch + the learned warm start.  Both run to the
+    reference's stop criterion (errorU, errorT <= 1e-6 at a check every 2000
+    iterations, 2M:307); the metric is the mixed arm's wall time for all
+    cases (lower is better), with the Nusselt agreement between the arms.
+    On N ranks the cases are split by LPT over node counts."""
+    import torch
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    W = pkg.warmstart
+    model = W.WarmStart.load(MODEL_PATH, device=local)
+    all_cases = W.sample_cases(200, seed=2000)[:args.cases]
+    idx, cases = pkg.sharding.my_share(all_cases, world, rank)
+    max_steps = args.max_steps
+    # FP64 cold, one cavity at a time (the drop-in's time to solution)
+    steps_cold, nu_cold, t_cold = [], [], 0.0
+    for c in cases:
+        cav = pkg.Cavity(2, c["nx"], c["ny"], Ra=c["Ra"], Pr=c["Pr"], coords=c["coords"], storage="f64",
+                         device=local)
+        cav.initial()
+        cav.synchronize()
+        t0 = time.perf_counter()
+        n, _, _ = cav.run(max_steps, 2000, W.F32_EPS)
+        cav.synchronize()
+        t_cold += time.perf_counter() - t0
+        steps_cold.append(n)
+        nu_cold.append(cav.nusselt()[0])
+        cav.close()
+    # mixed: FP32 storage, one batch, warm start (prediction time included)
+    sampler = None
+    if not args.no_clocks and rank == 0:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        sampler = ClockSampler(vis.split(",")[local] if vis else str(local))
+        sampler.start()
+        time.sleep(0.3)
+    l0 = pkg.kernel_launches()
+    _barrier(world)
+    r = W.solve(cases, init="warm", model=model, storage="f32", max_steps=max_steps, device=local)
+    launches = pkg.kernel_launches() - l0
+    clocks = sampler.stop() if sampler else None
+    t_mixed = _reduce(r["seconds"] + r["predict_seconds"], world, "max")
+    t_cold = _reduce(t_cold, world, "max")
+    got = pkg.sharding.gather_by_index(idx, {"steps_cold": steps_cold, "nu_cold": nu_cold, "steps_mixed": r["steps"],
+                                             "nu_mixed": r["nu_hot"], "status": r["status"],
+                                             "nodes": [c["nx"] * c["ny"] for c in cases]}, len(all_cases))
+    if rank == 0:
+        err = np.abs(got["nu_mixed"] - got["nu_cold"]) / np.abs(got["nu_cold"])
+        conv = got["status"] == 1
+        lups = float(np.sum(got["steps_mixed"] * got["nodes"]))
+        bpl = bytes_per_lup(2, "f32")
+        peak, peak_kind = measured_peak()
+        achieved = bpl * lups / t_mixed / 1e9
+        line = {
+            "metric": "time_to_steady_s", "value": t_mixed, "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
+            "ms_per_step": t_mixed * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32 storage (FP64 residual / Nu sums)", "data": "synthetic",
+            "config": {"workload": "steady", "cases": len(all_cases), "sides": "128..256", "criterion":
+                       "errorU, errorT <= float32(1e-6) every 2000 iterations", "max_steps": max_steps,
+                       "model": os.path.basename(MODEL_PATH), "baseline_arm": "FP64, conduction start, one cavity "
+                       "per launch"},
+            "time_to_steady": {"fp64_cold_seconds": t_cold, "mixed_warm_seconds": t_mixed,
+                               "speedup": t_cold / t_mixed, "fp64_cold_steps": int(got["steps_cold"].sum()),
+                               "mixed_warm_steps": int(got["steps_mixed"].sum()),
+                               "converged_mixed": int(conv.sum()),
+                               "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()),
+                               "max_nu_rel_err": float(err.max()), "fallbacks": int(np.sum(r["fallback"]))},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind, "bytes_per_lup": bpl,
+                         "kernel": "k_march2d_batch (FP32), wall time incl. host checks"},
+            "cpu_baseline": None,
+            "e2e": {"value": t_mixed, "unit": "s", "h2d_bytes_per_step": int(4 * 8 * got["nodes"].sum()),
+                    "d2h_bytes_per_step": 16 * len(all_cases),
+                    "path": "host prediction + lbm_init_warm per member + lbm_batch_run_masked + lbm_batch_nusselt"},
+            "gpu_launches": launches, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -327,7 +500,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--inner", type=int, default=100, help="LBM iterations per bench step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS) + ["batch256"])
+    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS) + ["batch256", "steady"])
+    ap.add_argument("--cases", type=int, default=16, help="steady: held-out cavities")
+    ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")
     ap.add_argument("--storage", default="f64", choices=["f64", "f32", "f16s"])
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -336,6 +511,8 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "march"])
     ap.add_argument("--nblocks", type=int, default=0, help="persistent blocks of the march kernel (0 = auto)")
     ap.add_argument("--l2promo", type=int, default=-1, help="TMA L2 promotion 0..3 (-1 = library default)")
+    ap.add_argument("--batch-shard", action="store_true",
+                    help="batch256 on N GPUs: split one sweep by LPT (strong scaling) instead of one sweep per rank")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -347,6 +524,8 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "batch256":
         return run_batch(args, world, rank, local)
+    if args.workload == "steady":
+        return run_steady(args, world, rank, local)
 
     import torch
     torch.cuda.set_device(local)

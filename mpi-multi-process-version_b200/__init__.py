@@ -5,9 +5,10 @@ from .lbm import (EXPORTS, GRID, MODE, NOALLOC_MAX_NODES, STORE, Batch, Cavity, 
                   fortran_e, kernel_launches, lbm_params, lib, mesh, mesh_box, output_ascii, run_main, sweep_specs)
 
 from . import studies  # noqa: E402
+from . import sharding  # noqa: E402
 from . import surrogate  # noqa: E402
 from . import warmstart  # noqa: E402
 
-__all__ = ["studies", "surrogate", "warmstart", "EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Batch", "Cavity", "LBMError", "Mesh",
+__all__ = ["studies", "sharding", "surrogate", "warmstart", "EXPORTS", "GRID", "MODE", "NOALLOC_MAX_NODES", "STORE", "Batch", "Cavity", "LBMError", "Mesh",
            "check_noalloc", "sweep_specs", "mesh_box",
            "fortran_e", "kernel_launches", "lbm_params", "lib", "mesh", "output_ascii", "run_main"]

@@ -229,7 +229,7 @@ class WarmStart:
 # solving to a steady state
 # ---------------------------------------------------------------------------
 def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
-          growth=100, want_fields=False, device=0, predictions=None):
+          growth=100, want_fields=False, device=0, predictions=None, field_fn=None):
     """Run every case to the reference's stop criterion (errorU, errorT <= eps
     at a check every `check_every` iterations) in one batch.
 
@@ -268,6 +268,8 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
            "storage": storage, "init": init}
     if want_fields:
         out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
+    if field_fn is not None:
+        out["field_out"] = [field_fn(i, m.macro()) for i, m in enumerate(b.members)]
     b.close()
     return out
 
@@ -297,9 +299,10 @@ def build_dataset(cases, R, storage="f32", eps=1e-5, max_steps=400_000, log=prin
     """Steady fields of `cases` from the solver (cold start, one batch) and
     their (features, targets) images."""
     t0 = time.perf_counter()
-    res = solve(cases, init="cold", storage=storage, eps=eps, max_steps=max_steps, want_fields=True)
+    res = solve(cases, init="cold", storage=storage, eps=eps, max_steps=max_steps,
+                field_fn=lambda i, f: targets(cases[i], f, R))
     X = np.stack([features(c, R) for c in cases])
-    Y = np.stack([targets(c, f, R) for c, f in zip(cases, res["fields"])])
+    Y = np.stack(res.pop("field_out"))
     if log:
         log(f"dataset: {len(cases)} cases, {int((res['status'] == 1).sum())} converged to {eps:g}, "
             f"{int(np.sum(res['steps'] * res['nodes'])) / 1e9:.1f} G lattice updates in "
@@ -353,6 +356,29 @@ def evaluate(model, cases, max_steps=1_500_000, log=print):
     return rows
 
 
+def summarize(rows):
+    """Headline numbers of an evaluation: time and steps of each variant
+    against FP64 cold, and the Nusselt error against the FP64 fixed point."""
+    ref = np.asarray(rows["f64_ref"]["nu"])
+    base = rows["f64_cold"]
+    out = {"cases": int(len(ref)), "f64_cold_converged": int((np.asarray(base["status"]) == 1).sum()),
+           "f64_cold_batched_seconds": base["seconds"], "f64_cold_sequential_seconds": base.get("sequential_seconds"),
+           "f64_cold_steps": int(np.sum(base["steps"]))}
+    for name in ("f32_warm", "f32_cold", "f64_warm", "f64_cold"):
+        r = rows[name]
+        ok = np.asarray(r["status"]) == 1
+        err = np.abs(np.asarray(r["nu"]) - ref) / np.abs(ref)
+        secs = r["seconds"] + r.get("predict_seconds", 0.0)
+        out[name] = {"seconds": secs, "steps": int(np.sum(r["steps"])), "converged": int(ok.sum()),
+                     "nu_within_1e-4": int((ok & (err <= 1e-4)).sum()),
+                     "max_nu_rel_err_converged": float(err[ok].max()) if ok.any() else None,
+                     "step_ratio_vs_f64_cold": float(np.sum(base["steps"]) / max(1, np.sum(r["steps"]))),
+                     "speedup_vs_f64_cold_sequential": (base.get("sequential_seconds") or 0.0) / secs,
+                     "speedup_vs_f64_cold_batched": base["seconds"] / secs,
+                     "fallbacks": int(np.sum(r.get("fallback", 0)))}
+    return out
+
+
 def _jsonable(x):
     if isinstance(x, dict):
         return {k: _jsonable(v) for k, v in x.items()}
@@ -375,7 +401,7 @@ def main(argv=None):
     ap.add_argument("--test", type=int, default=200)
     ap.add_argument("--sizes", default="128,160,192,224,256")
     ap.add_argument("--R", type=int, default=128)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=8000)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--data-eps", type=float, default=1e-5)
@@ -436,6 +462,8 @@ def main(argv=None):
             log(f"3D {n}^3 {init}: {res3[init]}")
             cav.close()
         out["cube"] = res3
+    out["summary"] = summarize(rows)
+    log(f"summary: {json.dumps(_jsonable(out['summary']))}")
     with open(os.path.join(a.out, "eval.json"), "w") as f:
         json.dump(_jsonable(out), f)
     log("done")

@@ -409,6 +409,9 @@ def main(argv=None):
     ap.add_argument("--eval-steps", type=int, default=1_500_000)
     ap.add_argument("--with3d", type=int, default=0, help="side of a 3D cube to evaluate (0: none)")
     ap.add_argument("--out", default="warmstart_out")
+    ap.add_argument("--phase", default="all", choices=["all", "train", "eval"],
+                    help="train: data + training + held-out image error; eval: time to steady state with --model")
+    ap.add_argument("--model", default=None, help="eval phase: a saved model (.npz)")
     a = ap.parse_args(sys.argv[1:] if argv is None else argv)
     os.makedirs(a.out, exist_ok=True)
     sizes = tuple(int(s) for s in a.sizes.split(","))
@@ -421,26 +424,34 @@ def main(argv=None):
 
     train_cases = sample_cases(a.train, seed=1000, sizes=sizes)
     test_cases = sample_cases(a.test, seed=2000, sizes=sizes)
-    X, Y, _ = build_dataset(train_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
-    Xt, Yt, _ = build_dataset(test_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
-    model = WarmStart(R=a.R, seed=0)
-    model.fit(X, Y, steps=a.steps, batch=a.batch, lr=a.lr, log_every=250, log=log)
-    log(f"training: {a.steps} steps of {a.batch} in {model.train_seconds:.1f} s")
-    pred = model.predict_images(Xt)
-    rel = [float(np.linalg.norm(pred[..., k] - Yt[..., k]) / np.linalg.norm(Yt[..., k] - (k == 2) * 0.0))
-           for k in range(3)]
-    log(f"held-out relative L2 error (u, v, theta): {rel}")
-    meta = {"train": a.train, "test": a.test, "sizes": sizes, "R": a.R, "steps": a.steps, "batch": a.batch,
-            "lr": a.lr, "data_eps": a.data_eps, "data_steps": a.data_steps, "train_seed": 1000, "test_seed": 2000,
-            "heldout_rel_l2": rel, "train_seconds": model.train_seconds}
-    model.save(os.path.join(a.out, "warmstart_unet.npz"), meta)
+    if a.phase in ("all", "train"):
+        X, Y, _ = build_dataset(train_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
+        Xt, Yt, _ = build_dataset(test_cases, a.R, eps=a.data_eps, max_steps=a.data_steps, log=log)
+        model = WarmStart(R=a.R, seed=0)
+        model.fit(X, Y, steps=a.steps, batch=a.batch, lr=a.lr, log_every=250, log=log)
+        log(f"training: {a.steps} steps of {a.batch} in {model.train_seconds:.1f} s")
+        pred = model.predict_images(Xt)
+        rel = [float(np.linalg.norm(pred[..., k] - Yt[..., k]) / np.linalg.norm(Yt[..., k])) for k in range(3)]
+        log(f"held-out relative L2 error (u, v, theta): {rel}")
+        meta = {"train": a.train, "test": a.test, "sizes": sizes, "R": a.R, "steps": a.steps, "batch": a.batch,
+                "lr": a.lr, "data_eps": a.data_eps, "data_steps": a.data_steps, "train_seed": 1000,
+                "test_seed": 2000, "heldout_rel_l2": rel, "train_seconds": model.train_seconds,
+                "history": model.history}
+        model.save(os.path.join(a.out, "warmstart_unet.npz"), meta)
+        del X, Y
+        if a.phase == "train":
+            log("done")
+            return
+    else:
+        model = WarmStart.load(a.model)
+        meta = model.meta
     rows = evaluate(model, test_cases, max_steps=a.eval_steps, log=log)
     tstep = step_seconds(sorted(set(sizes)))
     side = np.array([c["nx"] for c in test_cases])
     rows["f64_cold"]["sequential_seconds"] = float(sum(rows["f64_cold"]["steps"][i] * tstep[int(side[i])]
                                                        for i in range(len(side))))
     out = {"meta": meta, "cases": [{k: v for k, v in c.items() if k != "coords"} for c in test_cases],
-           "step_seconds_f64_single": tstep, "rows": rows, "history": model.history}
+           "step_seconds_f64_single": tstep, "rows": rows}
     if a.with3d:
         n = a.with3d
         m3 = L.mesh_box(n, n, n, 1.0, 1.0, 1.0, "tanh", 1.5)

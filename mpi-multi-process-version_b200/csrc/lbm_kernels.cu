@@ -40,9 +40,12 @@ namespace LBM_NS {
 // storage traits
 // ---------------------------------------------------------------------------
 template <int ST> struct Tr;
-template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false; };
-template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = false; };
-template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true; };
+// kShift: flow populations stored and computed as f - w (deviation form);
+// kShiftG: thermal populations stored as g - w*T0 (FP16 only: in FP32 the
+// unshifted g, proportional to T in [Tcold, Thot], is the better conditioned)
+template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false, kShiftG = false; };
+template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = true, kShiftG = false; };
+template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true, kShiftG = true; };
 
 __device__ __forceinline__ double tocomp(double x) { return x; }
 __device__ __forceinline__ float tocomp(float x) { return x; }
@@ -59,7 +62,15 @@ template <> __device__ __forceinline__ double tostore<double, double>(double x) 
 template <> __device__ __forceinline__ float tostore<float, float>(float x) { return x; }
 template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x * kF16Scale); }
 
-// lattice weights used as storage shifts (f - w*rho0, g - w*T0), rho0 = 1
+// Reduced-precision storage (FP32, shifted FP16) keeps f - w*rho0 (rho0 = 1;
+// FP16 also g - w*T0).  The flow populations stay in that deviation form
+// through streaming and collision (the interpolation weights sum to one and
+// bounce-back pairs directions of equal weight, so both commute with the
+// shift; the collision subtracts the rest state's moments): velocities are
+// small differences of O(w) populations, and in FP32 arithmetic on the full
+// populations their rounding (~1e-8) would hold the check() residual above
+// ~1e-5.  The thermal populations are shifted back on load.
+// lattice weights used as storage shifts
 __device__ __forceinline__ float wU2(int q) { return q == 0 ? 4.0f / 9.0f : (q < 5 ? 1.0f / 9.0f : 1.0f / 36.0f); }
 __device__ __forceinline__ float wT2(int q) { return q == 0 ? 0.5f : 0.125f; }
 __device__ __forceinline__ float wU3(int q) { return q == 0 ? 1.0f / 3.0f : (q < 7 ? 1.0f / 18.0f : 1.0f / 36.0f); }
@@ -96,8 +107,9 @@ __device__ __forceinline__ int off_b(int i, int n) { return i == 0 ? 2 : (i == n
 // 2D: D2Q9 MRT + D2Q5
 // ---------------------------------------------------------------------------
 
-// collision_U (2M:431-520) and collision_T (2M:522-569) at one node.
-template <class C>
+// collision_U (2M:431-520) and collision_T (2M:522-569) at one node.  DEV:
+// f and fp are deviations from the rest state (rho is still the full density).
+template <class C, bool DEV = false>
 __device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C u, C v, C T,
                                           const Geo &G, C fp[9], C gp[5], C &Fy)
 {
@@ -122,6 +134,12 @@ __device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C 
     meq[6] = -rho*v;
     meq[7] = rho*(u*u-v*v);
     meq[8] = rho*(u*v);
+    if (DEV) {
+        // minus the rest state's moments (1, -2, 1, 0, ...): rho - 1 = m[0]
+        meq[0] = m[0];
+        meq[1] = -C(2.0)*m[0]+C(3.0)*rho*(u*u+v*v);
+        meq[2] = m[0]-C(3.0)*rho*(u*u+v*v);
+    }
 
     Fy = gbeta*T*rho;
 #if LBM_EXACT
@@ -217,7 +235,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 
     auto LD = [&](int q, int64_t off) -> C {
         C val = tocomp(__ldg(src + q * P + id + off));
-        if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        if (Tr<ST>::kShiftG && q >= 9) val += C(wT2(q - 9)) * C(G.T0);
         return val;
     };
     // y-interpolation of plane q on the column at x-offset c
@@ -262,7 +280,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     // that produced src
     const C Fy0 = Fin[id];
     const C dt = C(G.dt);
-    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+    const C rho = (Tr<ST>::kShift ? C(1.0) : C(0.0)) + (f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]);
 #if LBM_EXACT
     const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
     const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
@@ -279,7 +297,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     }
 
     auto ST_ = [&](int q, C val) {
-        if (Tr<ST>::kShift) val -= (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        if (Tr<ST>::kShiftG && q >= 9) val -= C(wT2(q - 9)) * C(G.T0);
         dst[q * P + id] = tostore<S, C>(val);
     };
     if (KIND == 1) {
@@ -291,7 +309,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     }
 
     C fp[9], gp[5], Fy;
-    collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, Fy);
     Fout[id] = Fy;
 #pragma unroll
     for (int q = 0; q < 9; ++q) ST_(q, fp[q]);
@@ -303,8 +321,9 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 // 3D: D3Q19 MRT + D3Q7
 // ---------------------------------------------------------------------------
 
-// collision_U (3M:445-669) and collision_T (3M:671-730) at one node.
-template <class C>
+// collision_U (3M:445-669) and collision_T (3M:671-730) at one node.  DEV:
+// f and fp are deviations from the rest state (rho is still the full density).
+template <class C, bool DEV = false>
 __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C u, C v, C w, C T,
                                           const Geo &G, C fp[19], C gp[7], C &Fz)
 {
@@ -347,6 +366,12 @@ __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C
     meq[13]=rho*u*v;
     meq[14]=rho*v*w;
     meq[15]=rho*u*w;
+    if (DEV) {
+        // minus the rest state's moments (1, -11, 3, 0, ...): rho - 1 = m[0]
+        meq[0]=m[0];
+        meq[1]=-C(11.0)*m[0]+C(19.0)*rho*Vsquare;
+        meq[2]=C(3.0)*m[0]-C(5.5)*rho*Vsquare;
+    }
 
     Fz = gbeta*T*rho;
 #if LBM_EXACT
@@ -465,7 +490,7 @@ __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C
 // transform groups the +- symmetric populations; ~45 % fewer FP64 operations
 // and shorter dependency chains.  Fz0 is the force carried from the previous
 // collision (macro_u's half-force term).  Writes rho, u, v, w, T.
-template <class C>
+template <class C, bool DEV = false>
 __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7],
                                             C &Fz, C &rho, C &u, C &v, C &w, C &T)
 {
@@ -505,8 +530,8 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
     m[17] = yz_y - xy_y;
     m[18] = xz_z - yz_z;
 
-    // macro_u / macro_t (3M:988-1025)
-    rho = m[0];
+    // macro_u / macro_t (3M:988-1025); DEV: m[0] = rho - 1
+    rho = DEV ? C(1.0) + m[0] : m[0];
     const C rinv = C(1.0) / rho;
     u = m[3] * rinv;
     v = m[5] * rinv;
@@ -524,8 +549,10 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
     const C e11 = rho * (vv - ww);
     C mp[19];
     mp[0] = m[0];
-    mp[1] = m[1] - Snu * (m[1] - (C(-11.0) * rho + C(19.0) * rho * Vs)) + (C(38.0) - C(19.0) * Snu) * wF;
-    mp[2] = m[2] - Snu * (m[2] - (C(3.0) * rho - C(5.5) * rho * Vs)) - (C(11.0) - C(5.5) * Snu) * wF;
+    // DEV: the equilibria minus the rest state's moments (1, -11, 3, 0, ...)
+    const C r1 = DEV ? m[0] : rho;
+    mp[1] = m[1] - Snu * (m[1] - (C(-11.0) * r1 + C(19.0) * rho * Vs)) + (C(38.0) - C(19.0) * Snu) * wF;
+    mp[2] = m[2] - Snu * (m[2] - (C(3.0) * r1 - C(5.5) * rho * Vs)) - (C(11.0) - C(5.5) * Snu) * wF;
     mp[3] = m[3];
     mp[4] = m[4] - Sq * (m[4] - C(-2.0 / 3.0) * ru);
     mp[5] = m[5];
@@ -618,12 +645,12 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
 #endif
 
 // macro_u / macro_t (3M:988-1025) in the reference's operation order
-template <class C>
+template <class C, bool DEV = false>
 __device__ __forceinline__ void macro3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C &rho, C &u, C &v,
                                         C &w, C &T)
 {
     const C dt = C(G.dt);
-    rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
+    rho = (DEV ? C(1.0) : C(0.0)) + f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
 #if LBM_EXACT
     u = (f[1]-f[2]+f[7]-f[8]+f[9]-f[10]+f[11]-f[12]+f[13]-f[14])/rho;
     v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])/rho;
@@ -639,15 +666,15 @@ __device__ __forceinline__ void macro3d(const C f[19], const C gg[7], C Fz0, con
 
 // macro + collision of one node: the reference's order in the exact build,
 // the shared-subexpression form in the fast build
-template <class C>
+template <class C, bool DEV = false>
 __device__ __forceinline__ void node3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7], C &Fz,
                                        C &rho, C &u, C &v, C &w, C &T)
 {
 #if LBM_EXACT
-    macro3d<C>(f, gg, Fz0, G, rho, u, v, w, T);
-    collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+    macro3d<C, DEV>(f, gg, Fz0, G, rho, u, v, w, T);
+    collide3d<C, DEV>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
 #else
-    node3d_fast<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+    node3d_fast<C, DEV>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
 #endif
 }
 
@@ -675,7 +702,7 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 
     auto LD = [&](int q, int64_t off) -> C {
         C val = tocomp(__ldg(src + q * P + id + off));
-        if (Tr<ST>::kShift) val += (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+        if (Tr<ST>::kShiftG && q >= 19) val += C(wT3(q - 19)) * C(G.T0);
         return val;
     };
     auto YI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + ya), LD(q, c), LD(q, c + yb)); };
@@ -746,10 +773,10 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     const C Fz0 = Fin[id];
     C rho, u, v, w, T, fp[19], gp[7], Fz;
     if (LBM_EXACT || KIND == 1) {
-        macro3d<C>(f, gg, Fz0, G, rho, u, v, w, T);
-        if (KIND == 0) collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+        macro3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, rho, u, v, w, T);
+        if (KIND == 0) collide3d<C, Tr<ST>::kShift>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
     } else {
-        node3d<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+        node3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
     }
     if (write_macro || KIND == 1) {
         const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
@@ -757,7 +784,7 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
         B.w[mid] = double(w); B.T[mid] = double(T);
     }
     auto ST_ = [&](int q, C val) {
-        if (Tr<ST>::kShift) val -= (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+        if (Tr<ST>::kShiftG && q >= 19) val -= C(wT3(q - 19)) * C(G.T0);
         dst[q * P + id] = tostore<S, C>(val);
     };
     if (KIND == 1) {
@@ -863,7 +890,7 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
                 const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + 0 * gT[2];
                 ga = ga - (ct * wT[a]) * en;
             }
-            if (Tr<ST>::kShift) ga -= wT[a] * G.T0;
+            if (Tr<ST>::kShiftG) ga -= wT[a] * G.T0;
             pop[(9 + a) * P + id] = tostore<S, C>(C(ga));
         }
     } else {
@@ -901,7 +928,7 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
                 const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + ez[a] * gT[2];
                 ga = ga - (ct * wa) * en;
             }
-            if (Tr<ST>::kShift) ga -= wa * G.T0;
+            if (Tr<ST>::kShiftG) ga -= wa * G.T0;
             pop[(19 + a) * P + id] = tostore<S, C>(C(ga));
         }
     }
@@ -924,20 +951,21 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
     const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
     const int64_t P = G.plane;
     const int Q = G.dim == 2 ? 9 : 19, QT = G.dim == 2 ? 5 : 7;
+    // the flow populations stay deviations (see the storage note above)
     auto shift = [&](int q) -> C {
-        if (!Tr<ST>::kShift) return C(0);
-        if (G.dim == 2) return q < 9 ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
-        return q < 19 ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+        if (!Tr<ST>::kShiftG) return C(0);
+        if (G.dim == 2) return q < 9 ? C(0) : C(wT2(q - 9)) * C(G.T0);
+        return q < 19 ? C(0) : C(wT3(q - 19)) * C(G.T0);
     };
     C f[19], gg[7], fp[19], gp[7], F;
     for (int q = 0; q < Q; ++q) f[q] = tocomp(in[q * P + id]) + shift(q);
     for (int q = 0; q < QT; ++q) gg[q] = tocomp(in[(Q + q) * P + id]) + shift(Q + q);
     const C rho = C(B.rho[n]), u = C(B.u[n]), v = C(B.v[n]), T = C(B.T[n]);
     if (G.dim == 2) {
-        collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, F);
+        collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, F);
     } else {
         const C w = C(B.w[n]);
-        collide3d<C>(f, gg, rho, u, v, w, T, G, fp, gp, F);
+        collide3d<C, Tr<ST>::kShift>(f, gg, rho, u, v, w, T, G, fp, gp, F);
     }
     Fout[id] = F;
     for (int q = 0; q < Q; ++q) out[q * P + id] = tostore<S, C>(fp[q] - shift(q));

@@ -302,7 +302,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 const C zp[3] = {C(wz[0]), C(wz[1]), C(wz[2])}, zm[3] = {C(wz[3]), C(wz[4]), C(wz[5])};
                 auto SV = [&](const unsigned char *box, int idx, int q) -> C {
                     C val = tocomp(((const S *)box)[idx]);
-                    if (Tr<ST>::kShift) val += (q < 19) ? C(wU3(q)) : C(wT3(q - 19)) * C(G.T0);
+                    if (Tr<ST>::kShiftG && q >= 19) val += C(wT3(q - 19)) * C(G.T0);
                     return val;
                 };
                 auto ZB = [&](int zi, int s) -> const unsigned char * { return sm + (s & 3) * L::zslot() + L::zoff(zi); };
@@ -388,7 +388,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 
                 // macro_u / macro_t (3M:988-1025) and the collision
                 C rho, u, v, w, T, fp[19], gp[7], Fz;
-                node3d<C>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+                node3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
                 if (write_macro) {
                     const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
                     B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
@@ -397,14 +397,12 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 Fout[id] = Fz;
 #pragma unroll
                 for (int q = 0; q < 19; ++q) {
-                    C val = fp[q];
-                    if (Tr<ST>::kShift) val -= C(wU3(q));
-                    dst[q * P + id] = tostore<S, C>(val);
+                    dst[q * P + id] = tostore<S, C>(fp[q]);
                 }
 #pragma unroll
                 for (int q = 0; q < 7; ++q) {
                     C val = gp[q];
-                    if (Tr<ST>::kShift) val -= C(wT3(q)) * C(G.T0);
+                    if (Tr<ST>::kShiftG) val -= C(wT3(q)) * C(G.T0);
                     dst[(19 + q) * P + id] = tostore<S, C>(val);
                 }
             }
@@ -502,7 +500,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
     auto SV = [&](const unsigned char *box, int idx, int q) -> C {
         C val = tocomp(((const S *)box)[idx]);
-        if (Tr<ST>::kShift) val += (q < 9) ? C(wU2(q)) : C(wT2(q - 9)) * C(G.T0);
+        if (Tr<ST>::kShiftG && q >= 9) val += C(wT2(q - 9)) * C(G.T0);
         return val;
     };
     auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
@@ -552,7 +550,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     }
 
     const C dt = C(G.dt);
-    const C rho = f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8];
+    const C rho = (Tr<ST>::kShift ? C(1.0) : C(0.0)) + (f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]);
 #if LBM_EXACT
     const C u = ( f[1]-f[3]+f[5]-f[6]-f[7]+f[8]+C(0.5)*dt*C(0.0))/rho;
     const C v = ( f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)/rho;
@@ -567,18 +565,14 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
         B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
     }
     C fp[9], gp[5], Fy;
-    collide2d<C>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, Fy);
     Fout[id] = Fy;
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-        C val = fp[q];
-        if (Tr<ST>::kShift) val -= C(wU2(q));
-        dst[q * P + id] = tostore<S, C>(val);
-    }
+    for (int q = 0; q < 9; ++q) dst[q * P + id] = tostore<S, C>(fp[q]);
 #pragma unroll
     for (int q = 0; q < 5; ++q) {
         C val = gp[q];
-        if (Tr<ST>::kShift) val -= C(wT2(q)) * C(G.T0);
+        if (Tr<ST>::kShiftG) val -= C(wT2(q)) * C(G.T0);
         dst[(9 + q) * P + id] = tostore<S, C>(val);
     }
 }

@@ -188,6 +188,12 @@ __device__ __forceinline__ double shift_of(const Geo &G, int q)
     return (q == 19 ? 0.5 : 1.0 / 12.0) * G.T0;
 }
 
+// FP32 storage shifts the flow populations only
+__device__ __forceinline__ double shift_f32(const Geo &G, int q)
+{
+    return q < (G.dim == 2 ? 9 : 19) ? shift_of(G, q) : 0.0;
+}
+
 __device__ __forceinline__ int64_t pidx(const Geo &G, int64_t n)
 {
     const int i = int(n % G.nx);
@@ -206,7 +212,7 @@ __global__ void k_aos_to_planes(const Geo G, int q0, int nq, const double *__res
     const int64_t dst = (int64_t)q * G.plane + pidx(G, n);
     const double val = aos[e];
     if (ST == kF64) ((double *)pop)[dst] = val;
-    else if (ST == kF32) ((float *)pop)[dst] = float(val);
+    else if (ST == kF32) ((float *)pop)[dst] = float(val - shift_f32(G, q));
     else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q)) * kF16Scale);
 }
 
@@ -220,7 +226,7 @@ __global__ void k_planes_to_aos(const Geo G, int q0, int nq, const void *pop, do
     const int64_t src = (int64_t)q * G.plane + pidx(G, n);
     double val;
     if (ST == kF64) val = ((const double *)pop)[src];
-    else if (ST == kF32) val = double(((const float *)pop)[src]);
+    else if (ST == kF32) val = double(((const float *)pop)[src]) + shift_f32(G, q);
     else val = double(__half2float(((const __half *)pop)[src]) * kF16InvScale) + shift_of(G, q);
     aos[e] = val;
 }
@@ -260,7 +266,7 @@ __global__ void k_macro_from_pops(const Geo G, const void *pop, const Bufs B)
     auto ld = [&](int q) -> double {
         const int64_t a = (int64_t)q * G.plane + id;
         if (ST == kF64) return ((const double *)pop)[a];
-        if (ST == kF32) return double(((const float *)pop)[a]);
+        if (ST == kF32) return double(((const float *)pop)[a]) + shift_f32(G, q);
         return double(__half2float(((const __half *)pop)[a]) * kF16InvScale) + shift_of(G, q);
     };
     const int ex2[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};

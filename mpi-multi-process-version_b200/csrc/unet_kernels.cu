@@ -543,6 +543,246 @@ int launched(const char *what, int count = 1)
 
 bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
+// ---------------------------------------------------------------------------
+// 3x3 convolution on the 5th-generation tensor cores (tcgen05, TMEM)
+// ---------------------------------------------------------------------------
+// Same implicit GEMM as k_conv3x3 (M = pixels, N = Cout, K = 9 Cin), with the
+// accumulator tile (128 pixels x BN channels, FP32) held in tensor memory:
+//   * 4 warps gather the im2col tile and the weight tile of each K chunk (one
+//     tap, 32 input channels) with cp.async into a 4-stage ring, in the
+//     no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
+//     matrix; K-adjacent core matrices 128 B apart, 8-row groups 512 B apart);
+//   * after a generic-to-async proxy fence and a CTA barrier, one thread issues
+//     two tcgen05.mma (K = 16 each) and commits them to the stage's mbarrier,
+//     which frees the stage for the copy of chunk kc + 3;
+//   * the epilogue reads the accumulators back with tcgen05.ld (warp w owns
+//     TMEM lanes 32w..32w+31, i.e. pixels 32w..32w+31 of the tile).
+// Every mbarrier wait is bounded; on timeout the CTA counts the event in
+// g_nn_timeouts (read by lbm_nn_timeouts), waits (bounded) for its own MMAs,
+// frees its tensor memory and returns.
+constexpr int TBM = 128, TBK = 32, TSTAGES = 4, TTHREADS = 128;
+constexpr long long kNnWaitCycles = 2000000000LL;  // ~1 s at 1.9 GHz
+__device__ int g_nn_timeouts;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void nn_mbar_init(uint64_t *b, uint32_t n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ bool nn_mbar_test(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool nn_mbar_wait(uint64_t *b, uint32_t parity)
+{
+    if (nn_mbar_test(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!nn_mbar_test(b, parity))
+        if (clock64() - t0 > kNnWaitCycles) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// shared-memory matrix descriptor: start address, leading / stride byte
+// offsets (>> 4), descriptor version 1, base offset 0, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, bf16 A and B, both
+// K-major, N = BN, M = 128
+template <int BN>
+__host__ __device__ constexpr uint32_t umma_idesc()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TBM >> 4) << 24);
+}
+
+template <int BN>
+struct TcLayout {
+    static constexpr int A_BYTES = TBM * TBK * 2;  // 8 KB
+    static constexpr int B_BYTES = BN * TBK * 2;
+    static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr int BAR = TSTAGES * STAGE;    // mbarriers, then the TMEM address
+    static constexpr int SMEM = BAR + 64 + 1024;   // + alignment slack
+    // byte offset of element (row r, 16-byte piece q) in a K-major no-swizzle tile
+    __device__ static int off(int r, int q) { return (r >> 3) * 512 + q * 128 + (r & 7) * 16; }
+};
+
+template <int BN>
+__global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int desc_swap)
+{
+    using Lt = TcLayout<BN>;
+    extern __shared__ unsigned char tc_raw[];
+    unsigned char *sm = tc_raw + ((1024u - (smem_u32(tc_raw) & 1023u)) & 1023u);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + Lt::BAR);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + TSTAGES);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t M = (int64_t)a.B * a.H * a.W;
+    const int64_t m0 = (int64_t)blockIdx.x * TBM;
+    const int n0 = blockIdx.y * BN;
+    const int cchunks = a.Cin / TBK;
+    const int nk = 9 * cchunks;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < TSTAGES; ++s) nn_mbar_init(&bars[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    // the four A pieces of this thread: rows r = (tid + 128 i) / 4, 16-byte piece q
+    int ab[4], ay[4], ax[4];
+    bool av[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = (tid + i * TTHREADS) >> 2;
+        const int64_t m = m0 + r;
+        av[i] = m < M;
+        const int64_t mm = av[i] ? m : 0;
+        ax[i] = int(mm % a.W);
+        ay[i] = int((mm / a.W) % a.H);
+        ab[i] = int(mm / ((int64_t)a.W * a.H));
+    }
+    auto load = [&](int kc) {
+        unsigned char *st = sm + (kc % TSTAGES) * Lt::STAGE;
+        const int tap = kc / cchunks, c0 = (kc % cchunks) * TBK;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int v = tid + i * TTHREADS, r = v >> 2, q = v & 3;
+            const int yy = ay[i] + dy, xx = ax[i] + dx;
+            const bool ok = av[i] && yy >= 0 && yy < a.H && xx >= 0 && xx < a.W;
+            const bf16 *src = ok ? a.x + ((int64_t)(ab[i] * a.H + yy) * a.W + xx) * a.xs + a.xo + c0 + q * 8 : a.x;
+            cp_async16(st + Lt::off(r, q), src, ok ? 16 : 0);
+        }
+#pragma unroll
+        for (int i = 0; i < BN / 32; ++i) {
+            const int v = tid + i * TTHREADS, r = v >> 2, q = v & 3;
+            const int n = n0 + r;
+            const bool ok = n < a.Cout;
+            const bf16 *src = ok ? a.w + ((int64_t)n * 9 + tap) * a.Cin + c0 + q * 8 : a.w;
+            cp_async16(st + Lt::A_BYTES + Lt::off(r, q), src, ok ? 16 : 0);
+        }
+    };
+
+    // K-direction core matrices 128 B apart, 8-row groups 512 B apart
+    const uint32_t lbo = desc_swap ? 512u : 128u, sbo = desc_swap ? 128u : 512u;
+    constexpr uint32_t idesc = umma_idesc<BN>();
+    bool fail = false;
+    int issued = 0;  // K chunks whose MMAs were issued (uniform over the CTA)
+    for (int kc = 0; kc < TSTAGES - 1; ++kc) {
+        if (kc < nk) load(kc);
+        cp_commit();
+    }
+    for (int kc = 0; kc < nk; ++kc) {
+        // refill the stage chunk kc-1 used once its MMAs are done
+        const int nxt = kc + TSTAGES - 1;
+        if (nxt < nk) {
+            if (kc >= 1 && !nn_mbar_wait(&bars[(kc - 1) % TSTAGES], uint32_t(((kc - 1) / TSTAGES) & 1))) fail = true;
+            if (!fail) load(nxt);
+        }
+        cp_commit();
+        cp_wait<TSTAGES - 1>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        if (__syncthreads_or(fail)) {
+            fail = true;
+            break;
+        }
+        tc_fence_after();
+        if (tid == 0) {
+            const uint32_t base = smem_u32(sm + (kc % TSTAGES) * Lt::STAGE);
+#pragma unroll
+            for (int ks = 0; ks < TBK; ks += 16) {
+                const uint64_t da = umma_desc(base + (ks / 8) * 128, lbo, sbo);
+                const uint64_t db = umma_desc(base + Lt::A_BYTES + (ks / 8) * 128, lbo, sbo);
+                const uint32_t accum = (kc > 0 || ks > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(accum)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bars[kc % TSTAGES]))
+                         : "memory");
+        }
+        ++issued;
+    }
+    // every MMA of this CTA is complete once the commit of the last issued
+    // chunk arrives (bounded: also on the failure path, before the tensor
+    // memory is freed)
+    bool done = true;
+    if (issued > 0) done = nn_mbar_wait(&bars[(issued - 1) % TSTAGES], uint32_t(((issued - 1) / TSTAGES) & 1));
+    cp_wait<0>();
+    tc_fence_after();
+    if (__syncthreads_or(fail || !done)) {
+        if (tid == 0) atomicAdd(&g_nn_timeouts, 1);
+    } else {
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(taddr)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int64_t m = m0 + warp * 32 + lane;
+            if (m < M) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n >= a.Cout) break;
+                    float z = __uint_as_float(r[j]);
+                    if (a.bias) z += a.bias[n];
+                    if (a.of) {
+                        float *p = a.of + m * a.os + a.oo + n;
+                        *p = a.acc ? *p + z : z;
+                    }
+                    if (a.oa) a.oa[m * a.as + a.ao + n] = __float2bfloat16_rn(a.act ? silu(z) : z);
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+int g_use_tc = 1;          // 1: 3x3 convolutions on tcgen05 (the default), 0: mma.sync (lbm_nn_set_tensor_path)
+int g_desc_swap = 0;       // layout probe only: swap the two descriptor strides
+
 }  // namespace
 
 #define NN_REQUIRE(cond, ...)                                         \
@@ -568,6 +808,21 @@ extern "C" int lbm_nn_conv3x3(const void *x, int64_t xs, int32_t xo, const void 
                (bf16 *)oa, as, ao, act};
     const int64_t M = (int64_t)B * H * W;
     cudaStream_t s = (cudaStream_t)stream;
+    if (g_use_tc) {
+        const int bn = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : 128);
+        dim3 grid(unsigned((M + TBM - 1) / TBM), unsigned((Cout + bn - 1) / bn));
+        if (bn == 32) {
+            cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<32>::SMEM);
+            k_conv3x3_tc<32><<<grid, TTHREADS, TcLayout<32>::SMEM, s>>>(a, g_desc_swap);
+        } else if (bn == 64) {
+            cudaFuncSetAttribute(k_conv3x3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<64>::SMEM);
+            k_conv3x3_tc<64><<<grid, TTHREADS, TcLayout<64>::SMEM, s>>>(a, g_desc_swap);
+        } else {
+            cudaFuncSetAttribute(k_conv3x3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<128>::SMEM);
+            k_conv3x3_tc<128><<<grid, TTHREADS, TcLayout<128>::SMEM, s>>>(a, g_desc_swap);
+        }
+        return launched("lbm_nn_conv3x3 (tcgen05)");
+    }
     if (Cout <= 32) {
         dim3 grid(unsigned((M + CBM - 1) / CBM), unsigned((Cout + 31) / 32));
         k_conv3x3<32><<<grid, kThreads, 0, s>>>(a);
@@ -752,4 +1007,29 @@ extern "C" int lbm_nn_to_bf16(const float *x, void *y, int64_t n, void *stream)
     NN_REQUIRE(x && y && n > 0, "lbm_nn_to_bf16: bad arguments");
     k_to_bf16<<<blocks_for(n), kThreads, 0, (cudaStream_t)stream>>>(x, (bf16 *)y, n);
     return launched("lbm_nn_to_bf16");
+}
+
+extern "C" int lbm_nn_set_tensor_path(int32_t path)
+{
+    NN_REQUIRE(path == 0 || path == 1 || path == 2, "lbm_nn_set_tensor_path: path must be 0 (mma.sync), 1 (tcgen05)"
+                                                    " or 2 (tcgen05, strides swapped: layout probe)");
+    g_use_tc = path != 0;
+    g_desc_swap = path == 2;
+    return LBM_OK;
+}
+
+extern "C" int lbm_nn_get_tensor_path(void) { return g_use_tc ? (g_desc_swap ? 2 : 1) : 0; }
+
+extern "C" int lbm_nn_timeouts(int32_t *count, int32_t reset)
+{
+    NN_REQUIRE(count, "lbm_nn_timeouts: count is NULL");
+    int v = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_nn_timeouts, sizeof v);
+    if (e == cudaSuccess && reset) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_nn_timeouts, &zero, sizeof zero);
+    }
+    if (e != cudaSuccess) return lbm::set_error(LBM_ERR_CUDA, "lbm_nn_timeouts: %s", cudaGetErrorString(e));
+    *count = v;
+    return LBM_OK;
 }

@@ -55,8 +55,26 @@ _SIGS = {
     "lbm_nn_mse": [_dp, _dp, _dp, _i64, _i32, _dp, _dp, _i64, _dp, _dp],
     "lbm_nn_adam": [_dp, _dp, _dp, _dp, _dp, _i64, _f32, _f32, _f32, _f32, _f32, _f32, _f32, _dp],
     "lbm_nn_to_bf16": [_dp, _dp, _i64, _dp],
+    "lbm_nn_set_tensor_path": [_i32],
+    "lbm_nn_get_tensor_path": [],
+    "lbm_nn_timeouts": [_dp, _i32],
 }
 NN_EXPORTS = list(_SIGS)
+
+
+def set_tensor_path(path):
+    """0: mma.sync convolutions; 1: tcgen05 (TMEM accumulators); 2: layout probe."""
+    _chk(nn().lbm_nn_set_tensor_path(int(path)), "lbm_nn_set_tensor_path")
+
+
+def tensor_path():
+    return int(nn().lbm_nn_get_tensor_path())
+
+
+def timeouts(reset=False):
+    c = ctypes.c_int32()
+    _chk(nn().lbm_nn_timeouts(ctypes.byref(c), int(bool(reset))), "lbm_nn_timeouts")
+    return int(c.value)
 
 _bound = False
 

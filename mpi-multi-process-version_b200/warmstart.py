@@ -228,16 +228,7 @@ class WarmStart:
 # ---------------------------------------------------------------------------
 # solving to a steady state
 # ---------------------------------------------------------------------------
-def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
-          growth=100, want_fields=False, device=0, predictions=None, field_fn=None):
-    """Run every case to the reference's stop criterion (errorU, errorT <= eps
-    at a check every `check_every` iterations) in one batch.
-
-    init "cold": the conduction state of initial(); "warm": the model's
-    prediction (or `predictions`, a list of node-field dicts) through
-    lbm_init_warm.  Members whose residual diverges (not finite, or growth x
-    above its smallest value) restart cold and their steps add up.
-    Returns a dict of per-case arrays and the wall time."""
+def _prepare(cases, init, storage, model, predictions, device, growth):
     specs = [{k: v for k, v in c.items()} for c in cases]
     b = L.Batch(2, specs, storage=storage, device=device)
     t_pred = 0.0
@@ -251,7 +242,12 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
             mem.init_warm(f["rho"], f["u"], f["v"], None, f["T"])
     b.set_option("growth", int(growth))
     b.synchronize()
-    t0 = time.perf_counter()
+    return b, t_pred
+
+
+def _run(b, eps, max_steps, check_every):
+    """lbm_batch_run_masked with the cold-start fallback for members stopped
+    for a diverging residual."""
     status, steps = b.run_masked(None, max_steps, check_every, eps)
     fallback = status == -1
     if fallback.any():
@@ -260,12 +256,46 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
         st2, steps2 = b.run_masked(fallback, max_steps, check_every, eps)
         status = np.where(fallback, st2, status)
         steps = np.where(fallback, steps + steps2, steps)
+    return status, steps, fallback
+
+
+def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
+          growth=100, want_fields=False, device=0, predictions=None, field_fn=None, switch_eps=1e-5):
+    """Run every case to the reference's stop criterion (errorU, errorT <= eps
+    at a check every `check_every` iterations) in one batch.
+
+    init "cold": the conduction state of initial(); "warm": the model's
+    prediction (or `predictions`, a list of node-field dicts) through
+    lbm_init_warm.  Members whose residual diverges (not finite, or growth x
+    above its smallest value) restart cold and their steps add up.
+    storage "f64" / "f32" / "f16s", or "mixed": FP32 storage until the
+    residuals reach `switch_eps`, then the populations move to an FP64 batch
+    (lbm_get_populations / lbm_set_populations) that runs to `eps`, so the
+    result is the FP64 fixed point.
+    Returns a dict of per-case arrays and the wall time."""
+    first = "f32" if storage == "mixed" else storage
+    b, t_pred = _prepare(cases, init, first, model, predictions, device, growth)
+    t0 = time.perf_counter()
+    status, steps, fallback = _run(b, switch_eps if storage == "mixed" else eps, max_steps, check_every)
+    steps_low = steps.copy()
+    if storage == "mixed":
+        b64 = L.Batch(2, [{k: v for k, v in c.items()} for c in cases], storage="f64", device=device)
+        b64.set_option("growth", int(growth))
+        for m32, m64 in zip(b.members, b64.members):
+            f, g = m32.populations()
+            m64.initial()
+            m64.set_populations(f, g)
+        b.close()
+        b = b64
+        status, steps2, fb2 = _run(b, eps, max_steps, check_every)
+        steps = steps + steps2
+        fallback = fallback | fb2
     b.synchronize()
     seconds = time.perf_counter() - t0
     nu_hot, nu_cold = b.nusselt()
     out = {"status": status, "steps": steps, "fallback": fallback, "nu_hot": nu_hot, "nu_cold": nu_cold,
            "seconds": seconds, "predict_seconds": t_pred, "nodes": np.array([m.nnode for m in b.members]),
-           "storage": storage, "init": init}
+           "storage": storage, "init": init, "steps_low_precision": steps_low if storage == "mixed" else None}
     if want_fields:
         out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
     if field_fn is not None:
@@ -329,9 +359,10 @@ def step_seconds(sizes, storage="f64", steps=4000):
 
 def evaluate(model, cases, max_steps=1_500_000, log=print):
     """Steps and time to the reference's criterion for FP64 cold (the drop-in)
-    and FP32 warm (mixed precision + batch + warm start), Nu error against the
-    FP64 fixed point (FP64 continued to residual 1e-8), plus the two
-    single-change variants."""
+    and the mixed-precision warm start (FP32 to residual 1e-5, then FP64; one
+    batch; the model's prediction), Nu error against the FP64 fixed point
+    (FP64 continued to residual 1e-8), plus single-change variants (FP64 warm,
+    mixed cold) and FP32 alone."""
     rows = {}
     b = L.Batch(2, [dict(c) for c in cases], storage="f64")
     b.initial()
@@ -346,10 +377,12 @@ def evaluate(model, cases, max_steps=1_500_000, log=print):
     b.close()
     if log:
         log(f"f64 cold: {rows['f64_cold']['seconds']:.1f} s, converged {int((st == 1).sum())}/{len(cases)}")
-    for name, init, storage in (("f32_warm", "warm", "f32"), ("f32_cold", "cold", "f32"), ("f64_warm", "warm", "f64")):
+    for name, init, storage in (("mixed_warm", "warm", "mixed"), ("f64_warm", "warm", "f64"),
+                                ("mixed_cold", "cold", "mixed"), ("f32_warm", "warm", "f32")):
         r = solve(cases, init=init, model=model, storage=storage, max_steps=max_steps)
         rows[name] = {"status": r["status"], "steps": r["steps"], "seconds": r["seconds"], "nu": r["nu_hot"],
-                      "fallback": r["fallback"], "predict_seconds": r["predict_seconds"]}
+                      "fallback": r["fallback"], "predict_seconds": r["predict_seconds"],
+                      "steps_low_precision": r["steps_low_precision"]}
         if log:
             log(f"{name}: {r['seconds']:.1f} s (+{r['predict_seconds']:.2f} s prediction), converged "
                 f"{int((r['status'] == 1).sum())}/{len(cases)}, fallbacks {int(r['fallback'].sum())}")
@@ -364,7 +397,7 @@ def summarize(rows):
     out = {"cases": int(len(ref)), "f64_cold_converged": int((np.asarray(base["status"]) == 1).sum()),
            "f64_cold_batched_seconds": base["seconds"], "f64_cold_sequential_seconds": base.get("sequential_seconds"),
            "f64_cold_steps": int(np.sum(base["steps"]))}
-    for name in ("f32_warm", "f32_cold", "f64_warm", "f64_cold"):
+    for name in [k for k in ("mixed_warm", "f64_warm", "mixed_cold", "f32_warm", "f32_cold", "f64_cold") if k in rows]:
         r = rows[name]
         ok = np.asarray(r["status"]) == 1
         err = np.abs(np.asarray(r["nu"]) - ref) / np.abs(ref)

@@ -351,3 +351,24 @@ def test_init_warm_rejects_non_finite(pkg):
     with pytest.raises(pkg.LBMError):
         cav.init_warm(one, bad, zero, None, zero)
     cav.close()
+
+
+@pytest.mark.parametrize("dim,shape,Ra", [(2, (48, 48, 1), 1e3), (2, (40, 56, 1), 1e4)])
+def test_fp32_storage_reaches_the_reference_criterion(pkg, dim, shape, Ra):
+    # FP32 storage keeps the flow populations as deviations from the rest
+    # state, so its check() residual falls below the reference's 1e-6 like
+    # FP64's, in about as many iterations, to a Nusselt number within 1e-4
+    eps = float(np.float32(1e-6))
+    out = {}
+    for st in ("f64", "f32"):
+        c = pkg.Cavity(dim, *shape, Ra=Ra, grid="tanh", stretch=1.5, storage=st,
+                       coords=pkg.mesh_box(shape[0], shape[1], 0, 1.0, shape[1] / shape[0], 1.0, "tanh", 1.5))
+        c.initial()
+        steps, eu, et = c.run(400000, 2000, eps)
+        out[st] = (steps, eu, et, c.nusselt()[0])
+        c.close()
+    s64, s32 = out["f64"][0], out["f32"][0]
+    assert s64 < 400000 and s32 < 400000
+    assert out["f32"][1] <= eps and out["f32"][2] <= eps
+    assert s32 <= 1.5 * s64 + 4000
+    assert abs(out["f32"][3] - out["f64"][3]) <= 1e-4 * abs(out["f64"][3])

@@ -114,10 +114,20 @@ def _close(a, b, rel):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("path", [0, 1])
 @pytest.mark.parametrize("Cin,Cout,xs,xo", [(32, 48, 32, 0), (64, 128, 96, 32), (96, 32, 96, 0)])
-def test_conv3x3_forward_and_data_gradient(pkg, Cin, Cout, xs, xo):
+def test_conv3x3_forward_and_data_gradient(pkg, Cin, Cout, xs, xo, path):
     torch, dev = _dev()
     lib = pkg.surrogate.nn()
+    pkg.surrogate.set_tensor_path(path)
+    try:
+        _conv_forward_and_data_gradient(torch, dev, lib, Cin, Cout, xs, xo)
+    finally:
+        pkg.surrogate.set_tensor_path(1)
+    assert pkg.surrogate.timeouts(reset=True) == 0
+
+
+def _conv_forward_and_data_gradient(torch, dev, lib, Cin, Cout, xs, xo):
     rng = np.random.default_rng(Cin + Cout)
     B, H, W = 2, 12, 20
     xfull = U.bf16_round(rng.normal(size=(B, H, W, xs)))
@@ -275,21 +285,25 @@ def test_head_loss_and_adam(pkg):
 
 @pytest.mark.gpu
 def test_network_forward_and_gradients_match_oracle(pkg):
-    # the whole U-Net on the device against the oracle with the same bf16
-    # rounding points: outputs and every parameter gradient
+    # the whole U-Net on the device (mma.sync convolutions) against the oracle
+    # with the same bf16 rounding points: outputs and every parameter gradient
     torch, dev = _dev()
     S = pkg.surrogate
     rng = np.random.default_rng(7)
     params = U.init_params(3)
     params = {k: (w, rng.normal(0, 0.05, size=b.shape).astype(np.float32)) for k, (w, b) in params.items()}
-    net = S.Net(R=32, params=params)
     B = 2
     x = U.bf16_round(rng.normal(size=(B, 32, 32, U.IN_CH)))
-    y = net.forward(_bf16(torch, dev, x))
     dy = rng.normal(size=(B * 32 * 32, U.OUT_CH)).astype(np.float32)
-    net.buffers(B)["dy"].copy_(_f32(torch, dev, dy))
-    net.backward(B)
-    torch.cuda.synchronize()
+    S.set_tensor_path(0)
+    try:
+        net = S.Net(R=32, params=params)
+        y = net.forward(_bf16(torch, dev, x))
+        net.buffers(B)["dy"].copy_(_f32(torch, dev, dy))
+        net.backward(B)
+        torch.cuda.synchronize()
+    finally:
+        S.set_tensor_path(1)
     yr, cache = U.forward({k: (np.asarray(w, np.float64), np.asarray(b, np.float64)) for k, (w, b) in params.items()},
                           x, bf16=True)
     assert np.linalg.norm(_np(y) - yr.reshape(-1, 3)) <= 1e-2 * np.linalg.norm(yr)
@@ -321,3 +335,73 @@ def test_training_reduces_loss(pkg):
     assert hist[-1][1] < 0.1 * hist[0][1]
     pred = ws.predict_images(X)
     assert np.sqrt(((pred - Y) ** 2).mean()) < 0.3 * Y.std()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("Cin,Cout,H,W", [(32, 32, 16, 24), (64, 64, 12, 20), (96, 128, 8, 40), (128, 256, 9, 15),
+                                          (32, 48, 17, 13)])
+def test_tcgen05_convolution_matches_oracle(pkg, Cin, Cout, H, W):
+    # the tcgen05 path (accumulators in tensor memory) against the oracle and
+    # against the mma.sync path, forward with bias + SiLU and accumulate mode
+    torch, dev = _dev()
+    S = pkg.surrogate
+    lib = S.nn()
+    rng = np.random.default_rng(Cin * Cout + H)
+    B = 2
+    x = U.bf16_round(rng.normal(size=(B, H, W, Cin)))
+    w = U.bf16_round(rng.normal(0, 0.1, size=(Cout, 9, Cin)))
+    bias = rng.normal(size=Cout).astype(np.float32).astype(np.float64)
+    xd, wd, bd = _bf16(torch, dev, x), _bf16(torch, dev, w), _f32(torch, dev, bias)
+    outs = {}
+    S.timeouts(reset=True)
+    try:
+        for path in (0, 1):
+            S.set_tensor_path(path)
+            z = torch.zeros(B, H, W, Cout, dtype=torch.float32, device=dev)
+            a = torch.zeros(B, H, W, Cout, dtype=torch.bfloat16, device=dev)
+            assert lib.lbm_nn_conv3x3(xd.data_ptr(), Cin, 0, wd.data_ptr(), bd.data_ptr(), B, H, W, Cin, Cout,
+                                      z.data_ptr(), Cout, 0, 0, a.data_ptr(), Cout, 0, 1, None) == 0
+            acc = torch.ones(B, H, W, Cout, dtype=torch.float32, device=dev)
+            assert lib.lbm_nn_conv3x3(xd.data_ptr(), Cin, 0, wd.data_ptr(), None, B, H, W, Cin, Cout,
+                                      acc.data_ptr(), Cout, 0, 1, None, 0, 0, 0, None) == 0
+            torch.cuda.synchronize()
+            outs[path] = (_np(z), _np(a), _np(acc))
+    finally:
+        S.set_tensor_path(1)
+    assert S.timeouts(reset=True) == 0
+    zr = U.conv3x3(x, w, bias)
+    z1, a1, acc1 = outs[1]
+    assert _close(z1, zr, 1e-5)
+    assert np.abs(a1 - U.bf16_round(U.silu(z1))).max() <= 2 ** -7 * np.abs(a1).max()
+    assert _close(acc1 - 1.0, zr - bias, 1e-5)
+    assert _close(z1, outs[0][0], 1e-5)
+
+
+@pytest.mark.gpu
+def test_network_gradients_on_tcgen05_path(pkg):
+    # the whole U-Net's gradients with the tcgen05 convolutions, against the oracle
+    torch, dev = _dev()
+    S = pkg.surrogate
+    rng = np.random.default_rng(9)
+    params = {k: (w, rng.normal(0, 0.05, size=b.shape).astype(np.float32)) for k, (w, b) in U.init_params(4).items()}
+    S.set_tensor_path(1)
+    try:
+        net = S.Net(R=32, params=params)
+        x = U.bf16_round(rng.normal(size=(2, 32, 32, U.IN_CH)))
+        y = net.forward(_bf16(torch, dev, x))
+        dy = rng.normal(size=(2 * 32 * 32, U.OUT_CH)).astype(np.float32)
+        net.buffers(2)["dy"].copy_(_f32(torch, dev, dy))
+        net.backward(2)
+        torch.cuda.synchronize()
+    finally:
+        S.set_tensor_path(1)
+    assert S.timeouts(reset=True) == 0
+    yr, cache = U.forward({k: (np.asarray(w, np.float64), np.asarray(b, np.float64)) for k, (w, b) in params.items()},
+                          x)
+    assert np.linalg.norm(_np(y) - yr.reshape(-1, 3)) <= 1e-2 * np.linalg.norm(yr)
+    gr = U.backward(cache, dy.reshape(yr.shape).astype(np.float64))
+    gd = net.get_params("grad")
+    for name in gr:
+        for k in range(2):
+            err = np.linalg.norm(gd[name][k] - gr[name][k]) / max(np.linalg.norm(gr[name][k]), 1e-30)
+            assert err <= 2e-2, (name, k, err)

@@ -1,0 +1,75 @@
+"""The learned warm start on the GPU: what the trained network gains over the
+reference's conduction start, on held-out cavities the model never saw
+(seed 2000; the training set used seed 1000), with the solver judging both by
+the reference's criterion; the mixed-precision path's result against FP64; and
+the cold-start fallback when a warm start diverges."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MODEL = os.path.join(ROOT, "mpi-multi-process-version_b200", "warmstart_unet.npz")
+
+
+def _cases(pkg, n=3):
+    # held-out cases of the smallest side and moderate Ra, so the test runs in seconds
+    cs = [c for c in pkg.warmstart.sample_cases(60, seed=2000) if c["nx"] == 128 and c["Ra"] < 3e4]
+    return cs[:n]
+
+
+@pytest.fixture(scope="module")
+def model(pkg):
+    return pkg.warmstart.WarmStart.load(MODEL)
+
+
+def test_model_file_describes_its_training(model):
+    assert model.meta["train"] >= 1000 and model.meta["train_seed"] != model.meta["test_seed"]
+    assert max(model.meta["heldout_rel_l2"]) < 0.2
+
+
+def test_warm_start_needs_fewer_iterations_than_cold(pkg, model):
+    W = pkg.warmstart
+    cases = _cases(pkg)
+    assert len(cases) == 3
+    cold = W.solve(cases, init="cold", storage="f64", max_steps=800000)
+    warm = W.solve(cases, init="warm", model=model, storage="f64", max_steps=800000)
+    assert (cold["status"] == 1).all() and (warm["status"] == 1).all()
+    assert not warm["fallback"].any()
+    # the trained network's gain: at least 1.5x fewer iterations over the set
+    assert warm["steps"].sum() * 1.5 <= cold["steps"].sum(), (warm["steps"], cold["steps"])
+    # both runs end at the same FP64 fixed point
+    err = np.abs(warm["nu_hot"] - cold["nu_hot"]) / cold["nu_hot"]
+    assert err.max() <= 1e-4, err
+
+
+def test_mixed_precision_reaches_fp64_nusselt(pkg, model):
+    W = pkg.warmstart
+    cases = _cases(pkg, 2)
+    ref = W.solve(cases, init="cold", storage="f64", max_steps=800000)
+    mixed = W.solve(cases, init="warm", model=model, storage="mixed", max_steps=800000)
+    assert (mixed["status"] == 1).all()
+    assert (mixed["steps_low_precision"] > 0).all()
+    err = np.abs(mixed["nu_hot"] - ref["nu_hot"]) / ref["nu_hot"]
+    assert err.max() <= 1e-4, err
+
+
+def test_diverging_warm_start_falls_back_to_cold(pkg):
+    # a prediction far outside the low-Mach regime blows up; the member is
+    # stopped (residual not finite or growing) and restarted from the
+    # conduction state, then converges like a cold start
+    W = pkg.warmstart
+    cases = _cases(pkg, 2)
+    bad = []
+    for c in cases:
+        shape = (c["ny"], c["nx"])
+        rng = np.random.default_rng(0)
+        bad.append({"rho": np.ones(shape), "u": rng.uniform(-0.5, 0.5, shape), "v": rng.uniform(-0.5, 0.5, shape),
+                    "T": rng.uniform(-5.0, 5.0, shape)})
+    good = W.solve(cases[:1], init="cold", storage="f64", max_steps=800000)
+    res = W.solve(cases, init="warm", predictions=bad, storage="f64", max_steps=800000)
+    assert res["fallback"].all()
+    assert (res["status"] == 1).all()
+    assert abs(res["nu_hot"][0] - good["nu_hot"][0]) <= 1e-4 * good["nu_hot"][0]

@@ -120,6 +120,8 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
         cudaStreamDestroy(h->stream);
         h->stream = b->stream;
         h->owns_stream = false;
+        h->resident_opt = 0;  // members step one iteration per launch (or in the batch kernel)
+        h->resident = 0;
         b->cav.push_back(h);
     }
     b->active.assign(n, 1);

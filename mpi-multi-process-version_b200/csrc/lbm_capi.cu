@@ -275,7 +275,7 @@ static void free_all(lbm_handle *h)
                     h->bufs.v, h->bufs.w, h->bufs.T, h->bufs.up, h->bufs.vp, h->bufs.wp, h->bufs.Tp,
                     h->bufs.partials, h->bufs.scal, h->d_wgt[0], h->d_wgt[1], h->d_wgt[2], h->d_coord[0],
                     h->d_coord[1], h->d_coord[2], h->d_cellw[0], h->d_cellw[1], h->d_cellw[2], h->staging,
-                    h->aos, h->bufs.err};
+                    h->aos, h->bufs.err, h->d_bar};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->stream && h->owns_stream) cudaStreamDestroy(h->stream);
@@ -426,6 +426,14 @@ static int resolve_path(lbm_handle *h)
                 h->nblocks = slots;
         }
     }
+    // small 2D domains: every iteration of an lbm_step call in one resident
+    // cooperative launch (the per-iteration launch gap dominates there)
+    h->resident = 0;
+    if (!h->use_march && h->p.dim == 2 && h->resident_opt && h->owns_stream && h->d_bar) {
+        const int nb = h->p.mode == LBM_MODE_EXACT ? exact::resident_blocks(h->geo, h->p.storage, h->device)
+                                                   : fast::resident_blocks(h->geo, h->p.storage, h->device);
+        if (nb > 0 && (int64_t)nb * 256 >= h->geo.nnode) h->resident = nb;
+    }
     return LBM_OK;
 }
 
@@ -519,6 +527,9 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
         (st = dalloc(h, &b.partials, 592 * 4 * 8)) || (st = dalloc(h, &b.scal, 16 * 8)))
         return bail(st);
     if ((st = dalloc(h, &b.err, 16))) return bail(st);
+    if ((st = dalloc(h, &h->d_bar, 2 * sizeof(unsigned)))) return bail(st);
+    if (cudaMemset(h->d_bar, 0, 2 * sizeof(unsigned)) != cudaSuccess)
+        return bail(fail(LBM_ERR_CUDA, "memset failed"));
     if (cudaMemset(b.F[0], 0, fb) != cudaSuccess || cudaMemset(b.F[1], 0, fb) != cudaSuccess ||
         cudaMemset(b.w, 0, mb) != cudaSuccess || cudaMemset(b.wp, 0, mb) != cudaSuccess ||
         cudaMemset(b.err, 0, 16) != cudaSuccess || cudaMemset(b.pop[0], 0, popb) != cudaSuccess ||
@@ -712,6 +723,17 @@ extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
     int st = lbm::first_collision(h);
     if (st) return st;
     int done = 0;
+    if (h->resident && nsteps > 4) {
+        const bool ex = h->p.mode == LBM_MODE_EXACT;
+        CU(cudaMemsetAsync(h->d_bar, 0, 2 * sizeof(unsigned), h->stream));
+        CU(ex ? exact::steps_resident(h->geo, h->p.storage, h->bufs.pop, h->bufs.F, h->bufs, h->cur, nsteps, h->d_bar,
+                                      h->bufs.err, h->resident, h->stream)
+              : fast::steps_resident(h->geo, h->p.storage, h->bufs.pop, h->bufs.F, h->bufs, h->cur, nsteps, h->d_bar,
+                                     h->bufs.err, h->resident, h->stream));
+        h->cur = (h->cur + nsteps) & 1;
+        h->itc += nsteps;
+        return LBM_OK;
+    }
     // replay 2-step graphs for all but the last step(s) (small domains are
     // launch-bound), then the last step writes the macroscopic fields
     if (h->use_graphs && nsteps > 4) {
@@ -950,6 +972,9 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         lbm::drop_graphs(h);
         h->use_graphs = value != 0;
         return LBM_OK;
+    case LBM_OPT_RESIDENT:
+        h->resident_opt = value != 0;
+        return resolve_path(h);
     case LBM_OPT_L2PROMO:
         if (value < 0 || value > 3) return fail(LBM_ERR_PARAM, "L2 promotion must be 0..3");
         CU(cudaStreamSynchronize(h->stream));
@@ -969,6 +994,7 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     case LBM_OPT_NBLOCKS: *value = h->use_march ? h->nblocks : 0; return LBM_OK;
     case LBM_OPT_L2PROMO: *value = h->l2promo; return LBM_OK;
     case LBM_OPT_GRAPHS: *value = h->use_graphs; return LBM_OK;
+    case LBM_OPT_RESIDENT: *value = h->resident > 0; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

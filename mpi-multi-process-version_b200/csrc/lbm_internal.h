@@ -20,6 +20,27 @@ struct Geo {
     const double *cellw[3];  // per axis: cell widths of nodes 1..n
 };
 
+// The conduction profile between the isothermal walls along the heated axis
+// (x in 2D, y in 3D; the walls lie dt/2 outside the end nodes): linear in the
+// physical coordinate, Tc = Thot at the hot wall and Tcold at the cold one.
+// Reduced-precision storage keeps the thermal populations as g - wT * Tc.
+__host__ __device__ inline double tc_gradient(const Geo &G)
+{
+    const int ax = G.dim == 2 ? 0 : 1;
+    const int n = ax == 0 ? G.nx : G.ny;
+    const double *c = G.coord[ax];
+    const double lo = c[1] - 0.5 * G.dt, hi = c[n] + 0.5 * G.dt;
+    return (G.Tcold - G.Thot) / (hi - lo);
+}
+
+// Tc at node m (0-based) of the heated axis
+__host__ __device__ inline double tc_value(const Geo &G, int m)
+{
+    const double *c = G.coord[G.dim == 2 ? 0 : 1];
+    return G.Thot + tc_gradient(G) * (c[m + 1] - (c[1] - 0.5 * G.dt));
+}
+
+
 // Device buffers of one cavity.
 struct Bufs {
     void *pop[2];          // ping-pong population buffers, (Q+QT) planes each
@@ -69,6 +90,13 @@ constexpr float kF16InvScale = 1.0f / 4096.0f;
     /* the first-order non-equilibrium part, cf = 3 tau_f dt, ct = dt / sig_k              */ \
     cudaError_t equilibrium(const Geo &g, int store, void *pop, const Bufs &b, int neq, double cf, double ct, \
                             cudaStream_t s);                                                   \
+    /* nsteps 2D fused steps in one cooperative launch (domains of one wave); bar: two    */ \
+    /* zeroed unsigned of device memory, err: device flag set on a barrier timeout        */ \
+    cudaError_t steps_resident(const Geo &g, int store, void *const pop[2], void *const F[2], \
+                               const Bufs &b, int cur, int nsteps, unsigned *bar, int *err,    \
+                               int nblocks, cudaStream_t s);                                   \
+    /* resident grid of steps_resident for this domain (0: not available) */                  \
+    int resident_blocks(const Geo &g, int store, int device);                                  \
     /* first collision of a run: pre-collision pop_in -> post-collision pop_out, F_out */     \
     cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out,           \
                         void *F_out, const Bufs &b, cudaStream_t s);                          \

@@ -41,11 +41,11 @@ namespace LBM_NS {
 // ---------------------------------------------------------------------------
 template <int ST> struct Tr;
 // kShift: flow populations stored and computed as f - w (deviation form);
-// kShiftG: thermal populations stored as g - w*T0 (FP16 only: in FP32 the
-// unshifted g, proportional to T in [Tcold, Thot], is the better conditioned)
-template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false, kShiftG = false; };
-template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = true, kShiftG = false; };
-template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true, kShiftG = true; };
+// kDevT: thermal populations stored and computed as g - wT*Tc, Tc the
+// conduction profile (tc_value)
+template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false, kDevT = false; };
+template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = true, kDevT = true; };
+template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true, kDevT = true; };
 
 __device__ __forceinline__ double tocomp(double x) { return x; }
 __device__ __forceinline__ float tocomp(float x) { return x; }
@@ -62,14 +62,20 @@ template <> __device__ __forceinline__ double tostore<double, double>(double x) 
 template <> __device__ __forceinline__ float tostore<float, float>(float x) { return x; }
 template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x * kF16Scale); }
 
-// Reduced-precision storage (FP32, shifted FP16) keeps f - w*rho0 (rho0 = 1;
-// FP16 also g - w*T0).  The flow populations stay in that deviation form
-// through streaming and collision (the interpolation weights sum to one and
-// bounce-back pairs directions of equal weight, so both commute with the
-// shift; the collision subtracts the rest state's moments): velocities are
-// small differences of O(w) populations, and in FP32 arithmetic on the full
-// populations their rounding (~1e-8) would hold the check() residual above
-// ~1e-5.  The thermal populations are shifted back on load.
+// Reduced-precision storage (FP32, shifted FP16) keeps f - w*rho0 (rho0 = 1)
+// and g - wT*Tc (Tc: the linear conduction profile between the isothermal
+// walls), and both stay in that deviation form through streaming and
+// collision:
+//   * velocities are small differences of O(w) populations: in FP32
+//     arithmetic on the full populations their rounding (~1e-8) would hold the
+//     check() residual above ~1e-5.  The interpolation weights sum to one and
+//     bounce-back pairs directions of equal weight, so both commute with the
+//     shift; the collision subtracts the rest state's moments;
+//   * the wall Nusselt number amplifies temperature errors next to the wall
+//     by ~L_LB/Nu (~400), so ~1e-7 of absolute rounding in T ~ 1 would bias
+//     Nu by 1e-4.  Quadratic interpolation is exact on the linear profile, so
+//     streaming the deviation only adds -wT e.grad(Tc) dt per direction; the
+//     walls and the collision take Tc into their equilibria.
 // lattice weights used as storage shifts
 __device__ __forceinline__ float wU2(int q) { return q == 0 ? 4.0f / 9.0f : (q < 5 ? 1.0f / 9.0f : 1.0f / 36.0f); }
 __device__ __forceinline__ float wT2(int q) { return q == 0 ? 0.5f : 0.125f; }
@@ -109,7 +115,7 @@ __device__ __forceinline__ int off_b(int i, int n) { return i == 0 ? 2 : (i == n
 
 // collision_U (2M:431-520) and collision_T (2M:522-569) at one node.  DEV:
 // f and fp are deviations from the rest state (rho is still the full density).
-template <class C, bool DEV = false>
+template <class C, bool DEV = false, bool DEVT = false>
 __device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C u, C v, C T,
                                           const Geo &G, C fp[9], C gp[5], C &Fy)
 {
@@ -200,10 +206,12 @@ __device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C 
 #pragma unroll
     for (int a = 0; a < 5; ++a) np[a] = n[a]-Qr[a]*(n[a]-neq[a]);
 #else
-    np[0] = T;  // n(0) - 1*(n(0) - T)
+    // DEVT: gg are deviations from wT*Tc, whose moments are (Tc, 0, 0, Tc/2, 0)
+    const C Tn = DEVT ? n[0] : T;
+    np[0] = Tn;  // n(0) - 1*(n(0) - T)
     np[1] = n[1]-sig_k*(n[1]-T*u);
     np[2] = n[2]-sig_k*(n[2]-T*v);
-    np[3] = n[3]-C(1.9)*(n[3]-T*C(0.5));
+    np[3] = n[3]-C(1.9)*(n[3]-Tn*C(0.5));
     np[4] = n[4]-C(1.9)*n[4];
 #endif
     gp[0] = np[0]-np[3];
@@ -213,18 +221,17 @@ __device__ __forceinline__ void collide2d(const C f[9], const C gg[5], C rho, C 
     gp[4] = -DV(np[2],2.0)+DV(np[3],4.0)-DV(np[4],4.0);
 }
 
-// KIND 0: fused step; KIND 1: stream + walls + macro only
-template <int ST, int KIND>
-__global__ void __launch_bounds__(256)
-k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename Tr<ST>::C *__restrict__ Fin,
-         typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
-         int write_macro)
+// One node (i, j) of the fused 2D step.  KIND 0: fused step; KIND 1: stream
+// + walls + macro only.  COHERENT: read the source through L2 (ld.global.cg)
+// instead of the read-only path, for a kernel that wrote it itself earlier.
+template <int ST, int KIND, bool COHERENT = false>
+__device__ __forceinline__ void step2d_node(const Geo &G, const typename Tr<ST>::S *__restrict__ src,
+                                            const typename Tr<ST>::C *__restrict__ Fin,
+                                            typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout,
+                                            const Bufs &B, int write_macro, int i, int j)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= G.nx || j >= G.ny) return;
     const int64_t P = G.plane;
     const int64_t id = (int64_t)j * G.pitch + i;
     const int xa = off_a(i, G.nx), xb = off_b(i, G.nx);
@@ -234,9 +241,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     load_w(G.wgt[1], j, yp, ym);
 
     auto LD = [&](int q, int64_t off) -> C {
-        C val = tocomp(__ldg(src + q * P + id + off));
-        if (Tr<ST>::kShiftG && q >= 9) val += C(wT2(q - 9)) * C(G.T0);
-        return val;
+        return tocomp(COHERENT ? __ldcg(src + q * P + id + off) : __ldg(src + q * P + id + off));
     };
     // y-interpolation of plane q on the column at x-offset c
     auto YI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + ya), LD(q, c), LD(q, c + yb)); };
@@ -256,16 +261,25 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     gg[2] = ip(yp, LD(11, ya), LD(11, 0), LD(11, yb));
     gg[3] = ip(xm, LD(12, xa), LD(12, 0), LD(12, xb));
     gg[4] = ip(ym, LD(13, ya), LD(13, 0), LD(13, yb));
+    // deviation from the conduction profile: the departure point of g1 / g3
+    // lies dt behind / ahead along x
+    C Tc = C(0.0);
+    if (Tr<ST>::kDevT) {
+        Tc = C(tc_value(G, i));
+        const C sT = C(0.125 * G.dt * tc_gradient(G));
+        gg[1] -= sT;
+        gg[3] += sT;
+    }
 
     // walls: bounceback_u (2B:731-768), bounceback_T (2B:770-801)
     const C two_wT = C(2.0) * C(0.125);
     if (i == 0) {
         f[1] = LD(3, 0); f[5] = LD(7, 0); f[8] = LD(6, 0);
-        gg[1] = -LD(12, 0) + two_wT * C(G.Thot);
+        gg[1] = -LD(12, 0) + two_wT * (Tr<ST>::kDevT ? C(G.Thot) - Tc : C(G.Thot));
     }
     if (i == G.nx - 1) {
         f[3] = LD(1, 0); f[6] = LD(8, 0); f[7] = LD(5, 0);
-        gg[3] = -LD(10, 0) + two_wT * C(G.Tcold);
+        gg[3] = -LD(10, 0) + two_wT * (Tr<ST>::kDevT ? C(G.Tcold) - Tc : C(G.Tcold));
     }
     if (j == G.ny - 1) {
         f[4] = LD(2, 0); f[7] = LD(5, 0); f[8] = LD(6, 0);
@@ -278,7 +292,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 
     // macro_u / macro_t (2M:726-753); the force is the one of the collision
     // that produced src
-    const C Fy0 = Fin[id];
+    const C Fy0 = COHERENT ? __ldcg(Fin + id) : Fin[id];
     const C dt = C(G.dt);
     const C rho = (Tr<ST>::kShift ? C(1.0) : C(0.0)) + (f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]);
 #if LBM_EXACT
@@ -289,7 +303,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
     const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
 #endif
-    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+    const C T = Tr<ST>::kDevT ? Tc + (gg[0]+gg[1]+gg[2]+gg[3]+gg[4]) : gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
 
     if (write_macro || KIND == 1) {
         const int64_t mid = (int64_t)j * G.nx + i;
@@ -297,7 +311,6 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     }
 
     auto ST_ = [&](int q, C val) {
-        if (Tr<ST>::kShiftG && q >= 9) val -= C(wT2(q - 9)) * C(G.T0);
         dst[q * P + id] = tostore<S, C>(val);
     };
     if (KIND == 1) {
@@ -309,12 +322,83 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     }
 
     C fp[9], gp[5], Fy;
-    collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    collide2d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, T, G, fp, gp, Fy);
     Fout[id] = Fy;
 #pragma unroll
     for (int q = 0; q < 9; ++q) ST_(q, fp[q]);
 #pragma unroll
     for (int q = 0; q < 5; ++q) ST_(9 + q, gp[q]);
+}
+
+template <int ST, int KIND>
+__global__ void __launch_bounds__(256)
+k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename Tr<ST>::C *__restrict__ Fin,
+         typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
+         int write_macro)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= G.nx || j >= G.ny) return;
+    step2d_node<ST, KIND>(G, src, Fin, dst, Fout, B, write_macro, i, j);
+}
+
+// Bounded grid-wide barrier for a cooperative launch (every block resident):
+// sense by generation count.  False (and *err set) if the other blocks did
+// not arrive within kGridWaitCycles.
+static constexpr long long kGridWaitCycles = 2000000000LL;  // ~1 s
+
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned nblocks, int *err)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        const unsigned g0 = *(volatile unsigned *)gen;
+        __threadfence();
+        ok = 1;
+        if (atomicAdd(count, 1u) + 1u == nblocks) {
+            *(volatile unsigned *)count = 0u;
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*(volatile unsigned *)gen == g0)
+                if (clock64() - t0 > kGridWaitCycles) {
+                    atomicExch(err, 1);
+                    ok = 0;
+                    break;
+                }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// nsteps fused 2D steps in one cooperative launch for domains that fit one
+// wave (the per-step launch gap dominates there): step s reads buffer
+// (cur + s) & 1, writes the other, and every block waits at the grid barrier
+// before the next step reads what its neighbours wrote.  The macroscopic
+// fields are written by the last step.
+template <int ST>
+__global__ void __launch_bounds__(256)
+k_steps2d_resident(const Geo G, typename Tr<ST>::S *p0, typename Tr<ST>::S *p1, typename Tr<ST>::C *F0,
+                   typename Tr<ST>::C *F1, const Bufs B, int cur, int nsteps, unsigned *bar, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int64_t nn = (int64_t)G.nx * G.ny;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int s = 0; s < nsteps; ++s) {
+        const int c = (cur + s) & 1;
+        const S *src = c ? p1 : p0;
+        S *dst = c ? p0 : p1;
+        const C *Fin = c ? F1 : F0;
+        C *Fout = c ? F0 : F1;
+        const int wm = s == nsteps - 1;
+        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += stride)
+            step2d_node<ST, 0, true>(G, src, Fin, dst, Fout, B, wm, int(n % G.nx), int(n / G.nx));
+        if (s + 1 < nsteps && !grid_barrier(bar, bar + 1, gridDim.x, err)) return;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -323,7 +407,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 
 // collision_U (3M:445-669) and collision_T (3M:671-730) at one node.  DEV:
 // f and fp are deviations from the rest state (rho is still the full density).
-template <class C, bool DEV = false>
+template <class C, bool DEV = false, bool DEVT = false>
 __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C u, C v, C w, C T,
                                           const Geo &G, C fp[19], C gp[7], C &Fz)
 {
@@ -465,11 +549,13 @@ __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C
 #pragma unroll
     for (int a = 0; a < 7; ++a) np[a] = n[a]-Qr[a]*(n[a]-neq[a]);
 #else
-    np[0] = T;
+    // DEVT: gg are deviations from wT*Tc, whose moments are (Tc, 0, 0, 0, Tc/2, 0, 0)
+    const C Tn = DEVT ? n[0] : T;
+    np[0] = Tn;
     np[1] = n[1]-sig_k*(n[1]-T*u);
     np[2] = n[2]-sig_k*(n[2]-T*v);
     np[3] = n[3]-sig_k*(n[3]-T*w);
-    np[4] = n[4]-C(1.2)*(n[4]-T*C(0.5));
+    np[4] = n[4]-C(1.2)*(n[4]-Tn*C(0.5));
     np[5] = n[5]-C(1.2)*n[5];
     np[6] = n[6]-C(1.2)*n[6];
 #endif
@@ -490,9 +576,9 @@ __device__ __forceinline__ void collide3d(const C f[19], const C gg[7], C rho, C
 // transform groups the +- symmetric populations; ~45 % fewer FP64 operations
 // and shorter dependency chains.  Fz0 is the force carried from the previous
 // collision (macro_u's half-force term).  Writes rho, u, v, w, T.
-template <class C, bool DEV = false>
+template <class C, bool DEV = false, bool DEVT = false>
 __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7],
-                                            C &Fz, C &rho, C &u, C &v, C &w, C &T)
+                                            C &Fz, C &rho, C &u, C &v, C &w, C &T, C Tc = C(0.0))
 {
     const C Snu = C(G.Snu), Sq = C(G.Sq), dt = C(G.dt), gbeta = C(G.gbeta), sig_k = C(G.sig_k);
     // pairwise sums / differences
@@ -536,7 +622,8 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
     u = m[3] * rinv;
     v = m[5] * rinv;
     w = (m[7] + C(0.5) * dt * Fz0) * rinv;
-    T = gg[0] + (gg[1] + gg[2]) + (gg[3] + gg[4]) + (gg[5] + gg[6]);
+    const C Tn = gg[0] + (gg[1] + gg[2]) + (gg[3] + gg[4]) + (gg[5] + gg[6]);  // DEVT: T - Tc
+    T = DEVT ? Tc + Tn : Tn;
 
     // equilibria and relaxation (3M:522-587)
     const C uu = u * u, vv = v * v, ww = w * w;
@@ -625,9 +712,9 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
     const C np1 = n1 - sig_k * (n1 - T * u);
     const C np2 = n2 - sig_k * (n2 - T * v);
     const C np3 = n3 - sig_k * (n3 - T * w);
-    const C np4 = n4 - C(1.2) * (n4 - T * C(0.5));
+    const C np4 = n4 - C(1.2) * (n4 - Tn * C(0.5));
     const C np5 = C(-0.2) * n5, np6 = C(-0.2) * n6;
-    gp[0] = T - np4;
+    gp[0] = Tn - np4;
     const C t4 = np4 * C(1.0 / 6.0), t5 = np5 * C(1.0 / 6.0), t6 = np6 * C(1.0 / 6.0);
     {
         const C c = t4 + t5 + t6, o = np1 * C(0.5);
@@ -645,9 +732,9 @@ __device__ __forceinline__ void node3d_fast(const C f[19], const C gg[7], C Fz0,
 #endif
 
 // macro_u / macro_t (3M:988-1025) in the reference's operation order
-template <class C, bool DEV = false>
+template <class C, bool DEV = false, bool DEVT = false>
 __device__ __forceinline__ void macro3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C &rho, C &u, C &v,
-                                        C &w, C &T)
+                                        C &w, C &T, C Tc = C(0.0))
 {
     const C dt = C(G.dt);
     rho = (DEV ? C(1.0) : C(0.0)) + f[0]+f[1]+f[2]+f[3]+f[4]+f[5]+f[6]+f[7]+f[8]+f[9]+f[10]+f[11]+f[12]+f[13]+f[14]+f[15]+f[16]+f[17]+f[18];
@@ -661,20 +748,20 @@ __device__ __forceinline__ void macro3d(const C f[19], const C gg[7], C Fz0, con
     v = (f[3]-f[4]+f[7]+f[8]-f[9]-f[10]+f[15]-f[16]+f[17]-f[18])*rinv;
     w = (f[5]-f[6]+f[11]+f[12]-f[13]-f[14]+f[15]+f[16]-f[17]-f[18]+C(0.5)*dt*Fz0)*rinv;
 #endif
-    T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
+    T = DEVT ? Tc + (gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6]) : gg[0]+gg[1]+gg[2]+gg[3]+gg[4]+gg[5]+gg[6];
 }
 
 // macro + collision of one node: the reference's order in the exact build,
 // the shared-subexpression form in the fast build
-template <class C, bool DEV = false>
+template <class C, bool DEV = false, bool DEVT = false>
 __device__ __forceinline__ void node3d(const C f[19], const C gg[7], C Fz0, const Geo &G, C fp[19], C gp[7], C &Fz,
-                                       C &rho, C &u, C &v, C &w, C &T)
+                                       C &rho, C &u, C &v, C &w, C &T, C Tc = C(0.0))
 {
 #if LBM_EXACT
-    macro3d<C, DEV>(f, gg, Fz0, G, rho, u, v, w, T);
-    collide3d<C, DEV>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+    macro3d<C, DEV, DEVT>(f, gg, Fz0, G, rho, u, v, w, T, Tc);
+    collide3d<C, DEV, DEVT>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
 #else
-    node3d_fast<C, DEV>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+    node3d_fast<C, DEV, DEVT>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T, Tc);
 #endif
 }
 
@@ -702,7 +789,6 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 
     auto LD = [&](int q, int64_t off) -> C {
         C val = tocomp(__ldg(src + q * P + id + off));
-        if (Tr<ST>::kShiftG && q >= 19) val += C(wT3(q - 19)) * C(G.T0);
         return val;
     };
     auto YI = [&](int q, const C w[3], int64_t c) -> C { return ip(w, LD(q, c + ya), LD(q, c), LD(q, c + yb)); };
@@ -741,16 +827,24 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     gg[4] = ip(ym, LD(23, ya), LD(23, 0), LD(23, yb));
     gg[5] = ip(zp, LD(24, za), LD(24, 0), LD(24, zb));
     gg[6] = ip(zm, LD(25, za), LD(25, 0), LD(25, zb));
+    // deviation from the conduction profile along y (the heated axis)
+    C Tc = C(0.0);
+    if (Tr<ST>::kDevT) {
+        Tc = C(tc_value(G, j));
+        const C sT = C((1.0 / 12.0) * G.dt * tc_gradient(G));
+        gg[3] -= sT;
+        gg[4] += sT;
+    }
 
     // walls: bounceback_u (3B:1053-1136), bounceback_T (3B:1138-1197)
     const C two_wT = C(2.0) * (C(1.0) / C(12.0));
     if (j == 0) {
         f[3] = LD(4, 0); f[7] = LD(10, 0); f[8] = LD(9, 0); f[15] = LD(18, 0); f[17] = LD(16, 0);
-        gg[3] = -LD(23, 0) + two_wT * C(G.Thot);
+        gg[3] = -LD(23, 0) + two_wT * (Tr<ST>::kDevT ? C(G.Thot) - Tc : C(G.Thot));
     }
     if (j == G.ny - 1) {
         f[4] = LD(3, 0); f[9] = LD(8, 0); f[10] = LD(7, 0); f[16] = LD(17, 0); f[18] = LD(15, 0);
-        gg[4] = -LD(22, 0) + two_wT * C(G.Tcold);
+        gg[4] = -LD(22, 0) + two_wT * (Tr<ST>::kDevT ? C(G.Tcold) - Tc : C(G.Tcold));
     }
     if (i == 0) {
         f[1] = LD(2, 0); f[9] = LD(8, 0); f[7] = LD(10, 0); f[13] = LD(12, 0); f[11] = LD(14, 0);
@@ -773,10 +867,10 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     const C Fz0 = Fin[id];
     C rho, u, v, w, T, fp[19], gp[7], Fz;
     if (LBM_EXACT || KIND == 1) {
-        macro3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, rho, u, v, w, T);
-        if (KIND == 0) collide3d<C, Tr<ST>::kShift>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
+        macro3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, Fz0, G, rho, u, v, w, T, Tc);
+        if (KIND == 0) collide3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, w, T, G, fp, gp, Fz);
     } else {
-        node3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+        node3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T, Tc);
     }
     if (write_macro || KIND == 1) {
         const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
@@ -784,7 +878,6 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
         B.w[mid] = double(w); B.T[mid] = double(T);
     }
     auto ST_ = [&](int q, C val) {
-        if (Tr<ST>::kShiftG && q >= 19) val -= C(wT3(q - 19)) * C(G.T0);
         dst[q * P + id] = tostore<S, C>(val);
     };
     if (KIND == 1) {
@@ -890,7 +983,7 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
                 const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + 0 * gT[2];
                 ga = ga - (ct * wT[a]) * en;
             }
-            if (Tr<ST>::kShiftG) ga -= wT[a] * G.T0;
+            if (Tr<ST>::kDevT) ga -= wT[a] * tc_value(G, i);
             pop[(9 + a) * P + id] = tostore<S, C>(C(ga));
         }
     } else {
@@ -928,7 +1021,7 @@ __global__ void k_equilibrium(const Geo G, typename Tr<ST>::S *__restrict__ pop,
                 const double en = (ex[a] * gT[0] + ey[a] * gT[1]) + ez[a] * gT[2];
                 ga = ga - (ct * wa) * en;
             }
-            if (Tr<ST>::kShiftG) ga -= wa * G.T0;
+            if (Tr<ST>::kDevT) ga -= wa * tc_value(G, j);
             pop[(19 + a) * P + id] = tostore<S, C>(C(ga));
         }
     }
@@ -951,21 +1044,17 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
     const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
     const int64_t P = G.plane;
     const int Q = G.dim == 2 ? 9 : 19, QT = G.dim == 2 ? 5 : 7;
-    // the flow populations stay deviations (see the storage note above)
-    auto shift = [&](int q) -> C {
-        if (!Tr<ST>::kShiftG) return C(0);
-        if (G.dim == 2) return q < 9 ? C(0) : C(wT2(q - 9)) * C(G.T0);
-        return q < 19 ? C(0) : C(wT3(q - 19)) * C(G.T0);
-    };
+    // populations stay deviations (see the storage note above)
+    auto shift = [&](int q) -> C { return C(0) * C(q); };
     C f[19], gg[7], fp[19], gp[7], F;
     for (int q = 0; q < Q; ++q) f[q] = tocomp(in[q * P + id]) + shift(q);
     for (int q = 0; q < QT; ++q) gg[q] = tocomp(in[(Q + q) * P + id]) + shift(Q + q);
     const C rho = C(B.rho[n]), u = C(B.u[n]), v = C(B.v[n]), T = C(B.T[n]);
     if (G.dim == 2) {
-        collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, F);
+        collide2d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, T, G, fp, gp, F);
     } else {
         const C w = C(B.w[n]);
-        collide3d<C, Tr<ST>::kShift>(f, gg, rho, u, v, w, T, G, fp, gp, F);
+        collide3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, w, T, G, fp, gp, F);
     }
     Fout[id] = F;
     for (int q = 0; q < Q; ++q) out[q * P + id] = tostore<S, C>(fp[q] - shift(q));
@@ -1023,6 +1112,45 @@ cudaError_t step(const Geo &g, int store, const void *pop_in, const void *F_in, 
 #define CALL(ST) launch_step<ST>(g, pop_in, F_in, pop_out, F_out, b, write_macro, 0, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
+}
+
+template <int ST>
+static cudaError_t launch_resident(const Geo &g, void *const pop[2], void *const F[2], const Bufs &b, int cur,
+                                   int nsteps, unsigned *bar, int *err, int nblocks, cudaStream_t s)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    S *p0 = (S *)pop[0], *p1 = (S *)pop[1];
+    C *F0 = (C *)F[0], *F1 = (C *)F[1];
+    Geo gg = g;
+    Bufs bb = b;
+    void *args[] = {&gg, &p0, &p1, &F0, &F1, &bb, &cur, &nsteps, &bar, &err};
+    ++g_launches;
+    return cudaLaunchCooperativeKernel((const void *)k_steps2d_resident<ST>, dim3(nblocks), dim3(256), args, 0, s);
+}
+
+cudaError_t steps_resident(const Geo &g, int store, void *const pop[2], void *const F[2], const Bufs &b, int cur,
+                           int nsteps, unsigned *bar, int *err, int nblocks, cudaStream_t s)
+{
+#define CALL(ST) launch_resident<ST>(g, pop, F, b, cur, nsteps, bar, err, nblocks, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+int resident_blocks(const Geo &g, int store, int device)
+{
+    int bps = 0, sms = 0;
+    cudaError_t e = cudaErrorNotSupported;
+    switch (store) {
+    case kF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF64>, 256, 0); break;
+    case kF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF32>, 256, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF16S>, 256, 0); break;
+    }
+    if (e != cudaSuccess || bps <= 0) return 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    const int64_t need = ((int64_t)g.nx * g.ny + 255) / 256;
+    const int64_t cap = (int64_t)bps * sms;
+    return (int)(need < cap ? need : cap);
 }
 
 cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in, void *pop_out,

@@ -618,7 +618,11 @@ struct TcLayout {
     static constexpr int B_BYTES = BN * TBK * 2;
     static constexpr int STAGE = A_BYTES + B_BYTES;
     static constexpr int BAR = TSTAGES * STAGE;    // mbarriers, then the TMEM address
+    static_assert(BAR >= TBM * 33 * 4, "the epilogue stages 128 x 33 floats in the ring");
+    static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "TMEM allocations are powers of two >= 32");
     static constexpr int SMEM = BAR + 64 + 1024;   // + alignment slack
+    // shared memory bounds the CTAs per SM, so their TMEM columns fit the SM's 512
+    static_assert((228 * 1024 / SMEM) * BN <= 512, "TMEM oversubscription");
     // byte offset of element (row r, 16-byte piece q) in a K-major no-swizzle tile
     __device__ static int off(int r, int q) { return (r >> 3) * 512 + q * 128 + (r & 7) * 16; }
 };
@@ -743,6 +747,10 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
     if (__syncthreads_or(fail || !done)) {
         if (tid == 0) atomicAdd(&g_nn_timeouts, 1);
     } else {
+        // the ring is free now: stage each 32-column slice of the accumulator
+        // (thread = pixel row) and write it out row by row with the lanes on
+        // consecutive channels, so every store instruction is coalesced
+        float *stg = reinterpret_cast<float *>(sm);   // 128 x 33 floats, fits the ring
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 32) {
             uint32_t r[32];
@@ -758,14 +766,19 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
                 : "r"(taddr)
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const int64_t m = m0 + warp * 32 + lane;
-            if (m < M) {
+            const int row = warp * 32 + lane;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int n = n0 + c0 + j;
-                    if (n >= a.Cout) break;
-                    float z = __uint_as_float(r[j]);
-                    if (a.bias) z += a.bias[n];
+            for (int j = 0; j < 32; ++j) stg[row * 33 + j] = __uint_as_float(r[j]);
+            __syncthreads();
+            const int n = n0 + c0 + lane;
+            if (n < a.Cout) {
+                const float bia = a.bias ? a.bias[n] : 0.0f;
+#pragma unroll 4
+                for (int rr = 0; rr < 32; ++rr) {
+                    const int rl = warp * 32 + rr;
+                    const int64_t m = m0 + rl;
+                    if (m >= M) break;
+                    const float z = stg[rl * 33 + lane] + bia;
                     if (a.of) {
                         float *p = a.of + m * a.os + a.oo + n;
                         *p = a.acc ? *p + z : z;
@@ -773,6 +786,7 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
                     if (a.oa) a.oa[m * a.as + a.ao + n] = __float2bfloat16_rn(a.act ? silu(z) : z);
                 }
             }
+            __syncthreads();
         }
     }
     tc_fence_before();
@@ -809,7 +823,7 @@ extern "C" int lbm_nn_conv3x3(const void *x, int64_t xs, int32_t xo, const void 
     const int64_t M = (int64_t)B * H * W;
     cudaStream_t s = (cudaStream_t)stream;
     if (g_use_tc) {
-        const int bn = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : 128);
+        const int bn = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : (Cout <= 128 ? 128 : 256));
         dim3 grid(unsigned((M + TBM - 1) / TBM), unsigned((Cout + bn - 1) / bn));
         if (bn == 32) {
             cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<32>::SMEM);
@@ -817,9 +831,14 @@ extern "C" int lbm_nn_conv3x3(const void *x, int64_t xs, int32_t xo, const void 
         } else if (bn == 64) {
             cudaFuncSetAttribute(k_conv3x3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<64>::SMEM);
             k_conv3x3_tc<64><<<grid, TTHREADS, TcLayout<64>::SMEM, s>>>(a, g_desc_swap);
-        } else {
+        } else if (bn == 128) {
             cudaFuncSetAttribute(k_conv3x3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<128>::SMEM);
             k_conv3x3_tc<128><<<grid, TTHREADS, TcLayout<128>::SMEM, s>>>(a, g_desc_swap);
+        } else {
+            // 256 TMEM columns per CTA; its 97 KB of shared memory keep at most
+            // two CTAs on an SM, within the SM's 512 columns
+            cudaFuncSetAttribute(k_conv3x3_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<256>::SMEM);
+            k_conv3x3_tc<256><<<grid, TTHREADS, TcLayout<256>::SMEM, s>>>(a, g_desc_swap);
         }
         return launched("lbm_nn_conv3x3 (tcgen05)");
     }

@@ -38,7 +38,7 @@ EXPORTS = [
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5}
-OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS = 1, 2, 3, 4
+OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 

@@ -372,3 +372,35 @@ def test_fp32_storage_reaches_the_reference_criterion(pkg, dim, shape, Ra):
     assert out["f32"][1] <= eps and out["f32"][2] <= eps
     assert s32 <= 1.5 * s64 + 4000
     assert abs(out["f32"][3] - out["f64"][3]) <= 1e-4 * abs(out["f64"][3])
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("shape", [(40, 24), (128, 128), (100, 37)])
+def test_resident_multistep_launch_is_bit_identical(pkg, shape, mode):
+    # small 2D domains run an lbm_step call's iterations in one cooperative
+    # launch; the result is the per-iteration path's, bit for bit
+    out = []
+    for resident in (1, 0):
+        c = pkg.Cavity(2, *shape, Ra=1e4, grid="tanh", stretch=1.5, mode=mode,
+                       coords=pkg.mesh_box(shape[0], shape[1], 0, 1.0, shape[1] / shape[0], 1.0, "tanh", 1.5))
+        c.set_option(pkg.lbm.OPT_RESIDENT, resident)
+        assert c.get_option(pkg.lbm.OPT_RESIDENT) == resident
+        c.initial()
+        c.step(37)
+        c.step(101)
+        f, g = c.populations()
+        out.append((f, g, c.macro()))
+        c.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for k in FIELDS2:
+        assert np.array_equal(out[0][2][k], out[1][2][k]), k
+
+
+def test_resident_path_matches_oracle_in_exact_mode(pkg, ora):
+    cav, o = pair(pkg, ora, 2, 48, 48, grid="tanh", stretch=1.5, Ra=1e4, mode="exact")
+    assert cav.get_option(pkg.lbm.OPT_RESIDENT) == 1
+    cav.step(200)
+    o.step(200)
+    f, g = cav.populations()
+    assert np.array_equal(f, o.pops("f")) and np.array_equal(g, o.pops("g"))
+    cav.close()

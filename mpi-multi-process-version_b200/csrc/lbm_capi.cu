@@ -490,6 +490,7 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
     g.Snu = h->d.Snu; g.Sq = h->d.Sq; g.sig_k = h->d.sig_k; g.gbeta = h->d.gbeta;
     g.dt = p->dt; g.Thot = p->Thot; g.Tcold = p->Tcold; g.T0 = 0.5 * (p->Thot + p->Tcold);
     g.length_LB = p->length_LB;
+    tc_setup(g, c[p->dim == 2 ? 0 : 1]);
 
     // coordinates, weights, cell widths
     for (int a = 0; a < 3; ++a) {

@@ -15,6 +15,7 @@ struct Geo {
     int64_t plane;   // elements between population planes
     int64_t nnode;   // nx*ny*nz: packed macro arrays, x fastest
     double Snu, Sq, sig_k, gbeta, dt, Thot, Tcold, T0, length_LB;
+    double tc_lo, tc_grad;   // conduction profile: hot wall position and dTc per lattice unit (tc_setup)
     const double *wgt[3];    // per axis: weights [n][2 signs][3], sign 0 = +1, 1 = -1
     const double *coord[3];  // per axis: coordinates c(0:n+1)
     const double *cellw[3];  // per axis: cell widths of nodes 1..n
@@ -24,20 +25,20 @@ struct Geo {
 // (x in 2D, y in 3D; the walls lie dt/2 outside the end nodes): linear in the
 // physical coordinate, Tc = Thot at the hot wall and Tcold at the cold one.
 // Reduced-precision storage keeps the thermal populations as g - wT * Tc.
-__host__ __device__ inline double tc_gradient(const Geo &G)
+// tc_setup fills the two Geo fields from the host copy of the coordinates.
+inline void tc_setup(Geo &G, const double *c_heated)
 {
-    const int ax = G.dim == 2 ? 0 : 1;
-    const int n = ax == 0 ? G.nx : G.ny;
-    const double *c = G.coord[ax];
-    const double lo = c[1] - 0.5 * G.dt, hi = c[n] + 0.5 * G.dt;
-    return (G.Tcold - G.Thot) / (hi - lo);
+    const int n = G.dim == 2 ? G.nx : G.ny;
+    G.tc_lo = c_heated[1] - 0.5 * G.dt;
+    G.tc_grad = (G.Tcold - G.Thot) / ((c_heated[n] + 0.5 * G.dt) - G.tc_lo);
 }
+
+__host__ __device__ inline double tc_gradient(const Geo &G) { return G.tc_grad; }
 
 // Tc at node m (0-based) of the heated axis
 __host__ __device__ inline double tc_value(const Geo &G, int m)
 {
-    const double *c = G.coord[G.dim == 2 ? 0 : 1];
-    return G.Thot + tc_gradient(G) * (c[m + 1] - (c[1] - 0.5 * G.dt));
+    return G.Thot + G.tc_grad * (G.coord[G.dim == 2 ? 0 : 1][m + 1] - G.tc_lo);
 }
 
 

@@ -1044,11 +1044,10 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
     const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
     const int64_t P = G.plane;
     const int Q = G.dim == 2 ? 9 : 19, QT = G.dim == 2 ? 5 : 7;
-    // populations stay deviations (see the storage note above)
-    auto shift = [&](int q) -> C { return C(0) * C(q); };
     C f[19], gg[7], fp[19], gp[7], F;
-    for (int q = 0; q < Q; ++q) f[q] = tocomp(in[q * P + id]) + shift(q);
-    for (int q = 0; q < QT; ++q) gg[q] = tocomp(in[(Q + q) * P + id]) + shift(Q + q);
+    // reduced-precision storage: the populations stay deviations (see the storage note above)
+    for (int q = 0; q < Q; ++q) f[q] = tocomp(in[q * P + id]);
+    for (int q = 0; q < QT; ++q) gg[q] = tocomp(in[(Q + q) * P + id]);
     const C rho = C(B.rho[n]), u = C(B.u[n]), v = C(B.v[n]), T = C(B.T[n]);
     if (G.dim == 2) {
         collide2d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, T, G, fp, gp, F);
@@ -1057,8 +1056,8 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
         collide3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, w, T, G, fp, gp, F);
     }
     Fout[id] = F;
-    for (int q = 0; q < Q; ++q) out[q * P + id] = tostore<S, C>(fp[q] - shift(q));
-    for (int q = 0; q < QT; ++q) out[(Q + q) * P + id] = tostore<S, C>(gp[q] - shift(Q + q));
+    for (int q = 0; q < Q; ++q) out[q * P + id] = tostore<S, C>(fp[q]);
+    for (int q = 0; q < QT; ++q) out[(Q + q) * P + id] = tostore<S, C>(gp[q]);
 }
 
 #include "lbm_march.cuh"

@@ -271,9 +271,14 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
         const bool active = i < G.nx && j < G.ny;
         C xp[3], xm[3], yp[3], ym[3];
         int xa = 0, xb = 0, ya = 0, yb = 0;
+        C Tcn = C(0.0), sTc = C(0.0);  // conduction profile at the node's y and its streaming shift
         if (active) {
             load_w(G.wgt[0], i, xp, xm);
             load_w(G.wgt[1], j, yp, ym);
+            if (Tr<ST>::kDevT) {
+                Tcn = C(tc_value(G, j));
+                sTc = C((1.0 / 12.0) * G.dt * tc_gradient(G));
+            }
             xa = off_a(i, G.nx); xb = off_b(i, G.nx);
             ya = off_a(j, G.ny); yb = off_b(j, G.ny);
         }
@@ -301,9 +306,8 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 const double *wz = (const double *)(nslot_k + L::wo());
                 const C zp[3] = {C(wz[0]), C(wz[1]), C(wz[2])}, zm[3] = {C(wz[3]), C(wz[4]), C(wz[5])};
                 auto SV = [&](const unsigned char *box, int idx, int q) -> C {
-                    C val = tocomp(((const S *)box)[idx]);
-                    if (Tr<ST>::kShiftG && q >= 19) val += C(wT3(q - 19)) * C(G.T0);
-                    return val;
+                    (void)q;
+                    return tocomp(((const S *)box)[idx]);
                 };
                 auto ZB = [&](int zi, int s) -> const unsigned char * { return sm + (s & 3) * L::zslot() + L::zoff(zi); };
                 auto NB = [&](int ni) -> const unsigned char * {
@@ -356,6 +360,11 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 f[18] = ip(ym, Zc(9, 18, zm, 2, 0, ya), Zc(9, 18, zm, 2, 0, 0), Zc(9, 18, zm, 2, 0, yb));
                 gg[5] = Zc(10, 24, zp, 0, 0, 0);
                 gg[6] = Zc(11, 25, zm, 0, 0, 0);
+                // deviation from the conduction profile along y (the heated axis)
+                if (Tr<ST>::kDevT) {
+                    gg[3] -= sTc;
+                    gg[4] += sTc;
+                }
 
                 // walls: bounceback_u / bounceback_T (3B:1053-1197), centre values of slice k
                 auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0, 0), q); };
@@ -363,11 +372,11 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 const C two_wT = C(2.0) * (C(1.0) / C(12.0));
                 if (j == 0) {
                     f[3] = CN(4, 4); f[7] = CN(8, 10); f[8] = CN(7, 9); f[15] = CZ(9, 18); f[17] = CZ(7, 16);
-                    gg[3] = -CN(13, 23) + two_wT * C(G.Thot);
+                    gg[3] = -CN(13, 23) + two_wT * (Tr<ST>::kDevT ? C(G.Thot) - Tcn : C(G.Thot));
                 }
                 if (j == G.ny - 1) {
                     f[4] = CN(3, 3); f[9] = CN(6, 8); f[10] = CN(5, 7); f[16] = CZ(8, 17); f[18] = CZ(6, 15);
-                    gg[4] = -CN(12, 22) + two_wT * C(G.Tcold);
+                    gg[4] = -CN(12, 22) + two_wT * (Tr<ST>::kDevT ? C(G.Tcold) - Tcn : C(G.Tcold));
                 }
                 if (i == 0) {
                     f[1] = CN(2, 2); f[9] = CN(6, 8); f[7] = CN(8, 10); f[13] = CZ(3, 12); f[11] = CZ(5, 14);
@@ -388,7 +397,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 
                 // macro_u / macro_t (3M:988-1025) and the collision
                 C rho, u, v, w, T, fp[19], gp[7], Fz;
-                node3d<C, Tr<ST>::kShift>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T);
+                node3d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, Fz0, G, fp, gp, Fz, rho, u, v, w, T, Tcn);
                 if (write_macro) {
                     const int64_t mid = ((int64_t)k * G.ny + j) * G.nx + i;
                     B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v);
@@ -401,9 +410,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 }
 #pragma unroll
                 for (int q = 0; q < 7; ++q) {
-                    C val = gp[q];
-                    if (Tr<ST>::kShiftG) val -= C(wT3(q)) * C(G.T0);
-                    dst[(19 + q) * P + id] = tostore<S, C>(val);
+                    dst[(19 + q) * P + id] = tostore<S, C>(gp[q]);
                 }
             }
             __syncthreads();
@@ -499,9 +506,8 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     const double *wy = (const double *)(nslot_j + L::wo());
     const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
     auto SV = [&](const unsigned char *box, int idx, int q) -> C {
-        C val = tocomp(((const S *)box)[idx]);
-        if (Tr<ST>::kShiftG && q >= 9) val += C(wT2(q - 9)) * C(G.T0);
-        return val;
+        (void)q;
+        return tocomp(((const S *)box)[idx]);
     };
     auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
     auto NB = [&](int ni) -> const unsigned char * { return nslot_j + L::noff(ni); };
@@ -527,6 +533,14 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     gg[2] = YI(6, 11, yp, 0);
     gg[3] = ip(xm, SV(NB(5), ix(1, xa), 12), SV(NB(5), ix(1, 0), 12), SV(NB(5), ix(1, xb), 12));
     gg[4] = YI(7, 13, ym, 0);
+    // deviation from the conduction profile along x (the heated axis)
+    C Tcn = C(0.0);
+    if (Tr<ST>::kDevT) {
+        Tcn = C(tc_value(G, i));
+        const C sT = C(0.125 * G.dt * tc_gradient(G));
+        gg[1] -= sT;
+        gg[3] += sT;
+    }
 
     // walls (2B:731-801): centre values of row j
     auto CN = [&](int ni, int q) -> C { return SV(NB(ni), ix(L::nc(ni), 0), q); };
@@ -534,11 +548,11 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     const C two_wT = C(2.0) * C(0.125);
     if (i == 0) {
         f[1] = CN(2, 3); f[5] = CY(4, 7); f[8] = CY(3, 6);
-        gg[1] = -CN(5, 12) + two_wT * C(G.Thot);
+        gg[1] = -CN(5, 12) + two_wT * (Tr<ST>::kDevT ? C(G.Thot) - Tcn : C(G.Thot));
     }
     if (i == G.nx - 1) {
         f[3] = CN(1, 1); f[6] = CY(5, 8); f[7] = CY(2, 5);
-        gg[3] = -CN(4, 10) + two_wT * C(G.Tcold);
+        gg[3] = -CN(4, 10) + two_wT * (Tr<ST>::kDevT ? C(G.Tcold) - Tcn : C(G.Tcold));
     }
     if (j == ny - 1) {
         f[4] = CY(0, 2); f[7] = CY(2, 5); f[8] = CY(3, 6);
@@ -559,22 +573,18 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     const C u = (f[1]-f[3]+f[5]-f[6]-f[7]+f[8])*rinv;
     const C v = (f[2]-f[4]+f[5]+f[6]-f[7]-f[8]+C(0.5)*dt*Fy0)*rinv;
 #endif
-    const C T = gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
+    const C T = Tr<ST>::kDevT ? Tcn + (gg[0]+gg[1]+gg[2]+gg[3]+gg[4]) : gg[0]+gg[1]+gg[2]+gg[3]+gg[4];
     if (write_macro) {
         const int64_t mid = (int64_t)j * G.nx + i;
         B.rho[mid] = double(rho); B.u[mid] = double(u); B.v[mid] = double(v); B.T[mid] = double(T);
     }
     C fp[9], gp[5], Fy;
-    collide2d<C, Tr<ST>::kShift>(f, gg, rho, u, v, T, G, fp, gp, Fy);
+    collide2d<C, Tr<ST>::kShift, Tr<ST>::kDevT>(f, gg, rho, u, v, T, G, fp, gp, Fy);
     Fout[id] = Fy;
 #pragma unroll
     for (int q = 0; q < 9; ++q) dst[q * P + id] = tostore<S, C>(fp[q]);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
-        C val = gp[q];
-        if (Tr<ST>::kShiftG) val -= C(wT2(q)) * C(G.T0);
-        dst[(9 + q) * P + id] = tostore<S, C>(val);
-    }
+    for (int q = 0; q < 5; ++q) dst[(9 + q) * P + id] = tostore<S, C>(gp[q]);
 }
 
 // The 2D march over a list of segments (a cavity, a TX-wide column strip at

@@ -177,21 +177,17 @@ cudaError_t reduce_sums(const Geo &g, const Bufs &b, cudaStream_t s)
 // layout conversions between the Fortran f(0:Q-1, nx, ny[, nz]) order and the
 // structure-of-arrays planes
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double shift_of(const Geo &G, int q)
+// Reduced-precision storage keeps deviations: f - w (rho0 = 1) and g - wT*Tc
+// with Tc the conduction profile at the node (tc_value).  Node n is packed,
+// x fastest; the heated axis is x in 2D and y in 3D.
+__device__ __forceinline__ double shift_of(const Geo &G, int q, int64_t n)
 {
-    // lattice weight of plane q (f: w * rho0, g: w * T0); shifted storage only
     if (G.dim == 2) {
         if (q < 9) return q == 0 ? 4.0 / 9.0 : (q < 5 ? 1.0 / 9.0 : 1.0 / 36.0);
-        return (q == 9 ? 0.5 : 0.125) * G.T0;
+        return (q == 9 ? 0.5 : 0.125) * tc_value(G, int(n % G.nx));
     }
     if (q < 19) return q == 0 ? 1.0 / 3.0 : (q < 7 ? 1.0 / 18.0 : 1.0 / 36.0);
-    return (q == 19 ? 0.5 : 1.0 / 12.0) * G.T0;
-}
-
-// FP32 storage shifts the flow populations only
-__device__ __forceinline__ double shift_f32(const Geo &G, int q)
-{
-    return q < (G.dim == 2 ? 9 : 19) ? shift_of(G, q) : 0.0;
+    return (q == 19 ? 0.5 : 1.0 / 12.0) * tc_value(G, int((n / G.nx) % G.ny));
 }
 
 __device__ __forceinline__ int64_t pidx(const Geo &G, int64_t n)
@@ -212,8 +208,8 @@ __global__ void k_aos_to_planes(const Geo G, int q0, int nq, const double *__res
     const int64_t dst = (int64_t)q * G.plane + pidx(G, n);
     const double val = aos[e];
     if (ST == kF64) ((double *)pop)[dst] = val;
-    else if (ST == kF32) ((float *)pop)[dst] = float(val - shift_f32(G, q));
-    else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q)) * kF16Scale);
+    else if (ST == kF32) ((float *)pop)[dst] = float(val - shift_of(G, q, n));
+    else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q, n)) * kF16Scale);
 }
 
 template <int ST>
@@ -226,8 +222,8 @@ __global__ void k_planes_to_aos(const Geo G, int q0, int nq, const void *pop, do
     const int64_t src = (int64_t)q * G.plane + pidx(G, n);
     double val;
     if (ST == kF64) val = ((const double *)pop)[src];
-    else if (ST == kF32) val = double(((const float *)pop)[src]) + shift_f32(G, q);
-    else val = double(__half2float(((const __half *)pop)[src]) * kF16InvScale) + shift_of(G, q);
+    else if (ST == kF32) val = double(((const float *)pop)[src]) + shift_of(G, q, n);
+    else val = double(__half2float(((const __half *)pop)[src]) * kF16InvScale) + shift_of(G, q, n);
     aos[e] = val;
 }
 
@@ -266,8 +262,8 @@ __global__ void k_macro_from_pops(const Geo G, const void *pop, const Bufs B)
     auto ld = [&](int q) -> double {
         const int64_t a = (int64_t)q * G.plane + id;
         if (ST == kF64) return ((const double *)pop)[a];
-        if (ST == kF32) return double(((const float *)pop)[a]) + shift_f32(G, q);
-        return double(__half2float(((const __half *)pop)[a]) * kF16InvScale) + shift_of(G, q);
+        if (ST == kF32) return double(((const float *)pop)[a]) + shift_of(G, q, n);
+        return double(__half2float(((const __half *)pop)[a]) * kF16InvScale) + shift_of(G, q, n);
     };
     const int ex2[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
     const int ey2[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};

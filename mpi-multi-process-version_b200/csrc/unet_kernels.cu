@@ -549,12 +549,13 @@ bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 // Same implicit GEMM as k_conv3x3 (M = pixels, N = Cout, K = 9 Cin), with the
 // accumulator tile (128 pixels x BN channels, FP32) held in tensor memory:
 //   * 4 warps gather the im2col tile and the weight tile of each K chunk (one
-//     tap, 32 input channels) with cp.async into a 4-stage ring, in the
-//     no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
-//     matrix; K-adjacent core matrices 128 B apart, 8-row groups 512 B apart);
+//     tap, 32 input channels) with cp.async into a 4-stage ring, two chunks
+//     ahead, in the no-swizzle K-major core-matrix layout (8 rows x 16 bytes
+//     per core matrix; K-adjacent core matrices 128 B apart, 8-row groups
+//     512 B apart);
 //   * after a generic-to-async proxy fence and a CTA barrier, one thread issues
 //     two tcgen05.mma (K = 16 each) and commits them to the stage's mbarrier,
-//     which frees the stage for the copy of chunk kc + 3;
+//     which frees the stage for the copy of chunk kc + 4;
 //   * the epilogue reads the accumulators back with tcgen05.ld (warp w owns
 //     TMEM lanes 32w..32w+31, i.e. pixels 32w..32w+31 of the tile).
 // Every mbarrier wait is bounded; on timeout the CTA counts the event in
@@ -697,19 +698,22 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
     constexpr uint32_t idesc = umma_idesc<BN>();
     bool fail = false;
     int issued = 0;  // K chunks whose MMAs were issued (uniform over the CTA)
-    for (int kc = 0; kc < TSTAGES - 1; ++kc) {
+    // copies run two chunks ahead of the MMAs: the stage refilled at chunk kc
+    // held chunk kc-2, whose MMAs were issued an iteration earlier and have
+    // normally completed, so the wait below rarely stalls
+    constexpr int AHEAD = TSTAGES - 2;
+    for (int kc = 0; kc < AHEAD; ++kc) {
         if (kc < nk) load(kc);
         cp_commit();
     }
     for (int kc = 0; kc < nk; ++kc) {
-        // refill the stage chunk kc-1 used once its MMAs are done
-        const int nxt = kc + TSTAGES - 1;
+        const int nxt = kc + AHEAD;
         if (nxt < nk) {
-            if (kc >= 1 && !nn_mbar_wait(&bars[(kc - 1) % TSTAGES], uint32_t(((kc - 1) / TSTAGES) & 1))) fail = true;
+            if (kc >= 2 && !nn_mbar_wait(&bars[(kc - 2) % TSTAGES], uint32_t(((kc - 2) / TSTAGES) & 1))) fail = true;
             if (!fail) load(nxt);
         }
         cp_commit();
-        cp_wait<TSTAGES - 1>();
+        cp_wait<AHEAD>();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         if (__syncthreads_or(fail)) {

@@ -188,7 +188,7 @@ def test_step_before_init_is_a_state_error(pkg):
 
 
 def test_init_equilibrium_rest_state(pkg, ora):
-    # BASELINE's rest initial state (rho = 1, u = 0, T = 0) through the
+    # the rest initial state (rho = 1, u = 0, T = 0) through the
     # equilibrium entry point, against the oracle's set_macro
     cav = pkg.Cavity(2, 40, 40, grid="tanh", stretch=1.5, Ra=1e4, mode="exact")
     o = ora.Oracle(2, 40, 40, x=cav.mesh.x, y=cav.mesh.y, dt=cav.mesh.dt, length_LB=cav.mesh.length_LB, Ra=1e4)

@@ -405,3 +405,19 @@ def test_network_gradients_on_tcgen05_path(pkg):
         for k in range(2):
             err = np.linalg.norm(gd[name][k] - gr[name][k]) / max(np.linalg.norm(gr[name][k]), 1e-30)
             assert err <= 2e-2, (name, k, err)
+
+
+def test_centro_symmetrize_is_a_projection(pkg):
+    # the projection keeps symmetric fields, removes antisymmetric ones, and is idempotent
+    W = pkg.warmstart
+    rng = np.random.default_rng(4)
+    u, v, T = rng.normal(size=(3, 12, 9))
+    su, sv, sT = W.centro_symmetrize(u, v, T, 1.0, 0.0)
+    assert np.allclose(su, -su[::-1, ::-1]) and np.allclose(sv, -sv[::-1, ::-1])
+    assert np.allclose(sT, 1.0 - sT[::-1, ::-1])
+    again = W.centro_symmetrize(su, sv, sT, 1.0, 0.0)
+    assert all(np.allclose(a, b) for a, b in zip(again, (su, sv, sT)))
+    # the mesh the projection relies on: node i mirrors node n+1-i about the centre
+    m = pkg.mesh_box(24, 24, 0, 1.0, 1.0, 1.0, "tanh", 1.7)
+    lo, hi = m.x[1] - 0.5 * m.dt, m.x[24] + 0.5 * m.dt
+    assert np.allclose(m.x[1:25] - lo, hi - m.x[24:0:-1], atol=1e-9)

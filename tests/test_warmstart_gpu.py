@@ -42,13 +42,16 @@ def test_warm_start_needs_fewer_iterations_than_cold(pkg, model):
     W = pkg.warmstart
     cases = _cases(pkg)
     assert len(cases) == 3
-    cold = W.solve(cases, init="cold", storage="f64", eps=EPS, max_steps=1200000)
-    warm = W.solve(cases, init="warm", model=model, storage="f64", eps=EPS, max_steps=1200000)
+    # iterations to the reference's criterion
+    cold = W.solve(cases, init="cold", storage="f64", eps=W.F32_EPS, max_steps=1200000)
+    warm = W.solve(cases, init="warm", model=model, storage="f64", eps=W.F32_EPS, max_steps=1200000)
     assert (cold["status"] == 1).all() and (warm["status"] == 1).all()
     assert not warm["fallback"].any()
-    # the trained network's gain over the conduction start, summed over the set
-    assert warm["steps"].sum() <= 0.9 * cold["steps"].sum(), (warm["steps"], cold["steps"])
-    # both runs end at the same FP64 fixed point
+    assert warm["steps"].sum() <= 0.85 * cold["steps"].sum(), (warm["steps"], cold["steps"])
+    # both end at the same FP64 fixed point (checked at the tighter criterion)
+    cold = W.solve(cases, init="cold", storage="f64", eps=EPS, max_steps=1500000)
+    warm = W.solve(cases, init="warm", model=model, storage="f64", eps=EPS, max_steps=1500000)
+    assert (cold["status"] == 1).all() and (warm["status"] == 1).all()
     err = np.abs(warm["nu_hot"] - cold["nu_hot"]) / cold["nu_hot"]
     assert err.max() <= 1e-4, err
 

@@ -46,8 +46,10 @@ extern "C" {
 
 /* population storage precision */
 #define LBM_STORE_F64   0  /* FP64 storage, FP64 arithmetic: the drop-in */
-#define LBM_STORE_F32   1  /* FP32 storage, FP32 arithmetic */
-#define LBM_STORE_F16S  2  /* FP16 storage of f - w*rho0 and g - w*T0, FP32 arithmetic */
+#define LBM_STORE_F32   1  /* FP32 storage and arithmetic on deviations: f - w*rho0 and
+                              g - wT*Tc (Tc: the conduction profile between the walls) */
+#define LBM_STORE_F16S  2  /* the same deviations stored as binary16 (scaled by 2^12),
+                              FP32 arithmetic; inaccurate for steady states */
 
 /* arithmetic mode (FP64 storage only) */
 #define LBM_MODE_FAST   0  /* multiply-add contraction, reciprocal constants */

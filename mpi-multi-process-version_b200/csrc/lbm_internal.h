@@ -77,8 +77,8 @@ struct MarchShape {
 
 enum Store { kF64 = 0, kF32 = 1, kF16S = 2 };
 
-// Shifted FP16 storage keeps (f - w*rho0) * 2^12 and (g - w*T0) * 2^12 as
-// binary16.  The power-of-two scale is exact; it lifts the small deviations
+// Shifted FP16 storage keeps (f - w*rho0) * 2^12 and (g - wT*Tc) * 2^12 as
+// binary16 (Tc: the conduction profile, tc_value).  The power-of-two scale is exact; it lifts the small deviations
 // from the shift (1e-8 .. 1e-3) out of the binary16 subnormal range (below
 // 6.1e-5), where the absolute step is 6e-8, while |f - w| < 16 still fits.
 constexpr float kF16Scale = 4096.0f;

@@ -421,3 +421,42 @@ def test_centro_symmetrize_is_a_projection(pkg):
     m = pkg.mesh_box(24, 24, 0, 1.0, 1.0, 1.0, "tanh", 1.7)
     lo, hi = m.x[1] - 0.5 * m.dt, m.x[24] + 0.5 * m.dt
     assert np.allclose(m.x[1:25] - lo, hi - m.x[24:0:-1], atol=1e-9)
+
+
+def test_surrogate_entry_points_reject_bad_arguments_without_a_gpu(pkg):
+    # argument checks come before any device work, so they hold on a machine
+    # without a GPU; fake (never dereferenced) but aligned addresses stand in
+    # for device buffers
+    lib = pkg.surrogate.nn()
+    P = pkg.lib()
+    x, w, o = 1 << 20, 2 << 20, 3 << 20
+    ERR_PARAM = -1
+    # Cin not a multiple of 32
+    assert lib.lbm_nn_conv3x3(x, 16, 0, w, None, 1, 8, 8, 16, 32, o, 32, 0, 0, None, 0, 0, 1, None) == ERR_PARAM
+    # input channel window outside the stride
+    assert lib.lbm_nn_conv3x3(x, 32, 8, w, None, 1, 8, 8, 32, 32, o, 32, 0, 0, None, 0, 0, 1, None) == ERR_PARAM
+    # misaligned input
+    assert lib.lbm_nn_conv3x3(x + 2, 32, 0, w, None, 1, 8, 8, 32, 32, o, 32, 0, 0, None, 0, 0, 1, None) == ERR_PARAM
+    # accumulate with a bias
+    assert lib.lbm_nn_conv3x3(x, 32, 0, w, o, 1, 8, 8, 32, 32, o, 32, 0, 1, None, 0, 0, 0, None) == ERR_PARAM
+    # no output at all
+    assert lib.lbm_nn_conv3x3(x, 32, 0, w, None, 1, 8, 8, 32, 32, None, 0, 0, 0, None, 0, 0, 1, None) == ERR_PARAM
+    # weight gradient: Cout not a multiple of 8, workspace too small
+    assert lib.lbm_nn_conv3x3_wgrad(x, w, 32, 0, 1, 8, 8, 32, 12, o, 1 << 20, o, None) == ERR_PARAM
+    need = lib.lbm_nn_wgrad_workspace(1, 8, 8, 32, 32)
+    assert need > 0
+    assert lib.lbm_nn_conv3x3_wgrad(x, w, 32, 0, 1, 8, 8, 32, 32, o, need - 1, o, None) == ERR_PARAM
+    # pooling needs even sizes; the head at most 8 outputs; Adam needs positive bias corrections
+    assert lib.lbm_nn_pool2(x, 32, 0, 1, 7, 8, 32, o, 32, 0, None) == ERR_PARAM
+    assert lib.lbm_nn_head(x, 32, 0, w, None, 64, 32, 9, o, None) == ERR_PARAM
+    assert lib.lbm_nn_adam(x, None, w, o, o, 10, 1e-3, 0.9, 0.999, 1e-8, 0.0, 1.0, 0.0, None) == ERR_PARAM
+    assert lib.lbm_nn_set_tensor_path(3) == ERR_PARAM
+    assert "path" in P.lbm_last_error().decode()
+    assert lib.lbm_nn_get_tensor_path() in (0, 1)
+
+
+def test_masked_batch_run_rejects_a_null_batch(pkg):
+    import ctypes
+    conv = (ctypes.c_int32 * 1)()
+    done = (ctypes.c_int64 * 1)()
+    assert pkg.lib().lbm_batch_run_masked(None, None, 10, 2, 1e-6, conv, done) == -1

@@ -1,0 +1,145 @@
+"""Host logic of the warm-start driver on CPU: warmstart.solve's cold-start
+fallback and its mixed-precision hand-over, driven through a stand-in for the
+batch API (no GPU), and the evaluation summary."""
+import numpy as np
+import pytest
+
+
+class _FakeMember:
+    def __init__(self, log, i):
+        self.log, self.i, self.nnode = log, i, 100 + i
+        self.state = None
+
+    def initial(self):
+        self.log.append(("initial", self.i))
+        self.state = "cold"
+
+    def init_warm(self, rho, u, v, w, T):
+        self.log.append(("warm", self.i))
+        self.state = "warm"
+
+    def populations(self):
+        return ("f", self.i), ("g", self.i)
+
+    def set_populations(self, f, g):
+        self.log.append(("set", self.i, f[1], g[1]))
+        self.state = "loaded"
+
+
+class _FakeBatch:
+    """Scripted lbm_batch_run_masked outcomes: statuses[k] for the k-th run."""
+    instances = []
+
+    def __init__(self, dim, specs, storage="f64", device=0):
+        self.storage, self.n = storage, len(specs)
+        self.log = []
+        self.members = [_FakeMember(self.log, i) for i in range(self.n)]
+        self.runs = []
+        self.closed = False
+        _FakeBatch.instances.append(self)
+
+    def initial(self):
+        for m in self.members:
+            m.initial()
+
+    def set_option(self, name, value):
+        self.log.append(("option", name, value))
+
+    def synchronize(self):
+        pass
+
+    def run_masked(self, mask, max_steps, check_every, eps):
+        k = len(self.runs)
+        self.runs.append((None if mask is None else [bool(x) for x in mask], eps))
+        script = self.script[k]
+        status = np.array(script["status"], dtype=np.int32)
+        steps = np.array(script["steps"], dtype=np.int64)
+        if mask is not None:
+            status = np.where(mask, status, 0)
+            steps = np.where(mask, steps, 0)
+        return status, steps
+
+    def nusselt(self):
+        return np.arange(self.n, dtype=float) + 1.0, np.zeros(self.n)
+
+    def close(self):
+        self.closed = True
+
+
+@pytest.fixture
+def fake(pkg, monkeypatch):
+    _FakeBatch.instances.clear()
+    monkeypatch.setattr(pkg.warmstart.L, "Batch", _FakeBatch)
+    return _FakeBatch
+
+
+def _cases(n):
+    return [{"nx": 8, "ny": 8, "Ra": 1e4, "Pr": 0.71} for _ in range(n)]
+
+
+def _preds(n):
+    z = np.zeros((8, 8))
+    return [{"rho": z + 1, "u": z, "v": z, "T": z} for _ in range(n)]
+
+
+def test_diverged_members_restart_cold_and_their_steps_add_up(pkg, fake):
+    W = pkg.warmstart
+    _FakeBatch.script = [{"status": [1, -1, 1], "steps": [4000, 6000, 8000]},
+                         {"status": [0, 1, 0], "steps": [0, 10000, 0]}]
+    r = W.solve(_cases(3), init="warm", predictions=_preds(3), storage="f64", eps=1e-6, growth=50)
+    b = _FakeBatch.instances[0]
+    assert ("option", "growth", 50) in b.log
+    # only the diverged member was re-initialised and re-run
+    assert [e for e in b.log if e[0] == "initial"] == [("initial", 1)]
+    assert b.runs[1][0] == [False, True, False]
+    assert r["status"].tolist() == [1, 1, 1]
+    assert r["steps"].tolist() == [4000, 16000, 8000]
+    assert r["fallback"].tolist() == [False, True, False]
+    assert b.closed
+
+
+def test_mixed_precision_hands_the_populations_to_fp64(pkg, fake):
+    W = pkg.warmstart
+    _FakeBatch.script = [{"status": [1, 0], "steps": [20000, 30000]}]
+    orig_init = _FakeBatch.__init__
+
+    def init(self, *a, **k):
+        orig_init(self, *a, **k)
+        if self.storage == "f64":
+            self.script = [{"status": [1, 1], "steps": [6000, 4000]}]
+
+    _FakeBatch.__init__ = init
+    try:
+        r = W.solve(_cases(2), init="cold", storage="mixed", eps=1e-6, switch_eps=1e-5)
+    finally:
+        _FakeBatch.__init__ = orig_init
+    b32, b64 = _FakeBatch.instances
+    assert (b32.storage, b64.storage) == ("f32", "f64")
+    assert b32.runs[0][1] == 1e-5 and b64.runs[0][1] == 1e-6
+    # every member's FP32 populations reached the FP64 batch, after an init
+    sets = [e for e in b64.log if e[0] == "set"]
+    assert [(e[1], e[2], e[3]) for e in sets] == [(0, 0, 0), (1, 1, 1)]
+    assert b32.closed and b64.closed
+    assert r["steps"].tolist() == [26000, 34000]
+    assert r["steps_low_precision"].tolist() == [20000, 30000]
+    assert r["status"].tolist() == [1, 1]
+
+
+def test_summary_counts_and_ratios(pkg):
+    W = pkg.warmstart
+    ref = np.array([1.0, 2.0, 4.0])
+    rows = {
+        "f64_ref": {"nu": ref},
+        "f64_cold": {"status": np.array([1, 1, 0]), "steps": np.array([10, 20, 30]), "seconds": 6.0,
+                     "nu": ref * (1 + np.array([1e-5, 2e-5, 1e-3])), "sequential_seconds": 12.0},
+        "mixed_warm": {"status": np.array([1, 1, 1]), "steps": np.array([5, 10, 15]), "seconds": 2.0,
+                       "predict_seconds": 1.0, "nu": ref * (1 + np.array([5e-5, 2e-4, 0.0])),
+                       "fallback": np.array([False, True, False])},
+    }
+    s = W.summarize(rows)
+    m = s["mixed_warm"]
+    assert m["converged"] == 3 and m["nu_within_1e-4"] == 2 and m["fallbacks"] == 1
+    assert m["step_ratio_vs_f64_cold"] == pytest.approx(2.0)
+    assert m["speedup_vs_f64_cold_sequential"] == pytest.approx(4.0)
+    assert m["speedup_vs_f64_cold_batched"] == pytest.approx(2.0)
+    assert s["f64_cold"]["nu_within_1e-4"] == 2

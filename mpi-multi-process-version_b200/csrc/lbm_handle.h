@@ -43,7 +43,7 @@ struct lbm_handle {
     int nblocks = 0;             // resolved persistent grid
     int l2promo = 0;             // LBM_OPT_L2PROMO
     int use_graphs = 1;          // LBM_OPT_GRAPHS
-    int resident_opt = 1;        // LBM_OPT_RESIDENT as set
+    int resident_opt = 0;        // LBM_OPT_RESIDENT as set (opt-in)
     int resident = 0;            // resolved: blocks of the resident multi-step launch (0: off)
     unsigned *d_bar = nullptr;   // grid barrier of the resident launch (two counters)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 2-step graphs from cur = 0 / 1

@@ -398,6 +398,8 @@ def test_resident_multistep_launch_is_bit_identical(pkg, shape, mode):
 
 def test_resident_path_matches_oracle_in_exact_mode(pkg, ora):
     cav, o = pair(pkg, ora, 2, 48, 48, grid="tanh", stretch=1.5, Ra=1e4, mode="exact")
+    assert cav.get_option(pkg.lbm.OPT_RESIDENT) == 0  # opt-in
+    cav.set_option(pkg.lbm.OPT_RESIDENT, 1)
     assert cav.get_option(pkg.lbm.OPT_RESIDENT) == 1
     cav.step(200)
     o.step(200)

@@ -242,7 +242,7 @@ def run_reference(args, world, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": config_of(args, wl, inner=1),
+        "config": config_of(args, wl), "iterations_per_step": 1,
         "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
                          "sample": f"{args.steps} full-domain iterations per run, one per step; the Fortran "
                                    f"reference is not compilable here (no Fortran compiler / MPI), its C "
@@ -252,22 +252,25 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def config_of(args, wl, inner):
+def config_of(args, wl):
+    """The workload, identical in both arms (the metric is per lattice update,
+    so how many iterations one bench step runs is not part of it)."""
     dim, nx, ny, nz, grid, stretch, Ra, Pr = wl
     return {"workload": args.workload, "lattice": "D2Q9+D2Q5" if dim == 2 else "D3Q19+D3Q7",
             "nodes": [nx, ny, nz] if dim == 3 else [nx, ny], "grid": f"{grid} stretch {stretch}",
             "Ra": Ra, "Pr": Pr, "Ma": 0.1, "storage": args.storage, "mode": args.mode,
-            "iterations_per_step": inner, "init": "rest (rho=1, u=0, T=0)",
+            "init": "rest (rho=1, u=0, T=0)",
             "l2": "state larger than L2 (2 x ping-pong buffers), no flush",
             "parallelism": f"{args.gpus} independent cavities, one per GPU"}
 
 
-def add_kernel_config(cfg, cav, pkg):
-    cfg["kernel"] = cav.kernel
+def kernel_config(cav, pkg):
+    """How this arm runs the workload (not part of the workload itself)."""
+    kc = {"kernel": cav.kernel}
     if cav.kernel == "march":
-        cfg["march_blocks"] = cav.get_option(pkg.lbm.OPT_NBLOCKS)
-        cfg["l2_promotion"] = ["none", "64B", "128B", "256B"][cav.get_option(pkg.lbm.OPT_L2PROMO)]
-    return cfg
+        kc["march_blocks"] = cav.get_option(pkg.lbm.OPT_NBLOCKS)
+        kc["l2_promotion"] = ["none", "64B", "128B", "256B"][cav.get_option(pkg.lbm.OPT_L2PROMO)]
+    return kc
 
 
 def _reduce(x: float, world: int, op: str) -> float:
@@ -635,7 +638,8 @@ def main():
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "f16s": "f16 storage / f32"}[args.storage],
-            "data": "synthetic", "config": add_kernel_config(config_of(args, wl, args.inner), cav, pkg),
+            "data": "synthetic", "config": config_of(args, wl), "iterations_per_step": args.inner,
+            "kernel_config": kernel_config(cav, pkg),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_lup": bpl,

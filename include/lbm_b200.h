@@ -8,7 +8,8 @@
  * are called from the `do while` loop of `program main`
  * (2dim_mono.f90:307-330, 3dim_mono.f90:373-396).  Each entry point below
  * replaces one or more of those subroutines; the comment on each names them.
- * A Fortran caller binds these with `iso_c_binding`.
+ * A Fortran caller binds these with `iso_c_binding` (`bind(C, name=...)`
+ * interfaces over the same argument lists).
  *
  * Conventions
  *   - every function returns an int status: LBM_OK (0) or a negative

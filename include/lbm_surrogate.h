@@ -100,10 +100,10 @@ int lbm_nn_mse(const float *y, const float *t, const float *cw, int64_t P, int32
 int lbm_nn_adam(float *p, void *pb, const float *g, float *m, float *v, int64_t n, float lr, float b1,
                 float b2, float eps, float c1, float c2, float wd, void *stream);
 
-/* Which tensor-core path lbm_nn_conv3x3 uses: 0 mma.sync (m16n8k16), 1
- * tcgen05 with the accumulator in tensor memory (the default); 2 is the tcgen05 path with
- * the two shared-memory descriptor strides swapped, kept only to check the
- * descriptor layout against path 0.  Process-wide. */
+/* Which tensor-core path lbm_nn_conv3x3 uses: 0 mma.sync (m16n8k16, the
+ * default: faster on the network's layer sizes), 1 tcgen05 with the
+ * accumulator in tensor memory.  Both give the same results to bf16 rounding.
+ * Process-wide. */
 int lbm_nn_set_tensor_path(int32_t path);
 int lbm_nn_get_tensor_path(void);
 

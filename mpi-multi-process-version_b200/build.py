@@ -37,7 +37,7 @@ UNITS = [
     ("kernels_exact.o", "lbm_kernels.cu", ["-DLBM_NS=exact", "-DLBM_EXACT=1", "--fmad=false"]),
     ("reduce.o", "lbm_reduce.cu", ["--fmad=false"]),
     ("capi.o", "lbm_capi.cu", []),
-    ("noalloc.o", "lbm_noalloc.cu", []),
+    ("noalloc.o", "lbm_noalloc.cu", ["--fmad=false"]),
     ("batch.o", "lbm_batch.cu", []),
     ("unet.o", "unet_kernels.cu", []),
 ]

@@ -629,7 +629,7 @@ struct TcLayout {
 };
 
 template <int BN>
-__global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int desc_swap)
+__global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a)
 {
     using Lt = TcLayout<BN>;
     extern __shared__ unsigned char tc_raw[];
@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
     };
 
     // K-direction core matrices 128 B apart, 8-row groups 512 B apart
-    const uint32_t lbo = desc_swap ? 512u : 128u, sbo = desc_swap ? 128u : 512u;
+    const uint32_t lbo = 128u, sbo = 512u;
     constexpr uint32_t idesc = umma_idesc<BN>();
     bool fail = false;
     int issued = 0;  // K chunks whose MMAs were issued (uniform over the CTA)
@@ -798,8 +798,7 @@ __global__ void __launch_bounds__(TTHREADS) k_conv3x3_tc(const ConvArgs a, int d
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
 }
 
-int g_use_tc = 1;          // 1: 3x3 convolutions on tcgen05 (the default), 0: mma.sync (lbm_nn_set_tensor_path)
-int g_desc_swap = 0;       // layout probe only: swap the two descriptor strides
+int g_use_tc = 0;          // 0: mma.sync (the default, faster on these layer sizes), 1: tcgen05 (lbm_nn_set_tensor_path)
 
 }  // namespace
 
@@ -831,18 +830,18 @@ extern "C" int lbm_nn_conv3x3(const void *x, int64_t xs, int32_t xo, const void 
         dim3 grid(unsigned((M + TBM - 1) / TBM), unsigned((Cout + bn - 1) / bn));
         if (bn == 32) {
             cudaFuncSetAttribute(k_conv3x3_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<32>::SMEM);
-            k_conv3x3_tc<32><<<grid, TTHREADS, TcLayout<32>::SMEM, s>>>(a, g_desc_swap);
+            k_conv3x3_tc<32><<<grid, TTHREADS, TcLayout<32>::SMEM, s>>>(a);
         } else if (bn == 64) {
             cudaFuncSetAttribute(k_conv3x3_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<64>::SMEM);
-            k_conv3x3_tc<64><<<grid, TTHREADS, TcLayout<64>::SMEM, s>>>(a, g_desc_swap);
+            k_conv3x3_tc<64><<<grid, TTHREADS, TcLayout<64>::SMEM, s>>>(a);
         } else if (bn == 128) {
             cudaFuncSetAttribute(k_conv3x3_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<128>::SMEM);
-            k_conv3x3_tc<128><<<grid, TTHREADS, TcLayout<128>::SMEM, s>>>(a, g_desc_swap);
+            k_conv3x3_tc<128><<<grid, TTHREADS, TcLayout<128>::SMEM, s>>>(a);
         } else {
             // 256 TMEM columns per CTA; its 97 KB of shared memory keep at most
             // two CTAs on an SM, within the SM's 512 columns
             cudaFuncSetAttribute(k_conv3x3_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<256>::SMEM);
-            k_conv3x3_tc<256><<<grid, TTHREADS, TcLayout<256>::SMEM, s>>>(a, g_desc_swap);
+            k_conv3x3_tc<256><<<grid, TTHREADS, TcLayout<256>::SMEM, s>>>(a);
         }
         return launched("lbm_nn_conv3x3 (tcgen05)");
     }
@@ -1034,14 +1033,12 @@ extern "C" int lbm_nn_to_bf16(const float *x, void *y, int64_t n, void *stream)
 
 extern "C" int lbm_nn_set_tensor_path(int32_t path)
 {
-    NN_REQUIRE(path == 0 || path == 1 || path == 2, "lbm_nn_set_tensor_path: path must be 0 (mma.sync), 1 (tcgen05)"
-                                                    " or 2 (tcgen05, strides swapped: layout probe)");
-    g_use_tc = path != 0;
-    g_desc_swap = path == 2;
+    NN_REQUIRE(path == 0 || path == 1, "lbm_nn_set_tensor_path: path must be 0 (mma.sync) or 1 (tcgen05)");
+    g_use_tc = path == 1;
     return LBM_OK;
 }
 
-extern "C" int lbm_nn_get_tensor_path(void) { return g_use_tc ? (g_desc_swap ? 2 : 1) : 0; }
+extern "C" int lbm_nn_get_tensor_path(void) { return g_use_tc ? 1 : 0; }
 
 extern "C" int lbm_nn_timeouts(int32_t *count, int32_t reset)
 {

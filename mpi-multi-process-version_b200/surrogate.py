@@ -63,7 +63,7 @@ NN_EXPORTS = list(_SIGS)
 
 
 def set_tensor_path(path):
-    """0: mma.sync convolutions; 1: tcgen05 (TMEM accumulators); 2: layout probe."""
+    """0: mma.sync convolutions (the default); 1: tcgen05 (TMEM accumulators)."""
     _chk(nn().lbm_nn_set_tensor_path(int(path)), "lbm_nn_set_tensor_path")
 
 

@@ -92,9 +92,13 @@ def assemble(name, states):
     return out
 
 
+# where the reference programs are mounted (read-only) in the build container
+REFERENCE_DIR = os.environ.get("LBM_REFERENCE_DIR", "/root/reference")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=REFERENCE_DIR)
     ap.add_argument("--only", default=None)
     ap.add_argument("--dump-python", default=None, help="write the translated programs here")
     args = ap.parse_args()

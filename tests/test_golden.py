@@ -10,6 +10,8 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# the reference programs (read-only, present only where the fixtures are made)
+REFERENCE_DIR = os.environ.get("LBM_REFERENCE_DIR", "/root/reference")
 FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "ref_*.npz")))
 
 
@@ -67,18 +69,19 @@ def test_mono_and_block_decompositions_agree():
             assert np.array_equal(a[k], b[k]), (dim, k)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference sources not mounted")
+@pytest.mark.skipif(not os.path.isdir(REFERENCE_DIR), reason="reference sources not mounted")
 def test_fixture_regenerates_from_reference(tmp_path):
     # regenerate the smallest fixture from the reference source and compare
     import subprocess
     import sys
     src = os.path.join(GOLDEN, "make_golden.py")
     code = ("import sys, numpy as np; sys.path.insert(0, %r); import f90py, make_golden as m; "
-            "src = open('/root/reference/natural-convection_2dim_mono.f90').read(); "
+            "src = open(%r).read(); "
             "states, _ = f90py.run(src, 2, {'nx': 24, 'itc_max': 40}, 20); "
             "out = m.assemble('2dim_mono', states); "
             "ref = np.load(%r); "
             "assert all(np.array_equal(out[k], ref[k]) for k in ('f', 'g', 'u', 'v', 'T', 'rho'))"
-            % (GOLDEN, os.path.join(GOLDEN, "ref_2dim_mono.npz")))
+            % (GOLDEN, os.path.join(REFERENCE_DIR, "natural-convection_2dim_mono.f90"),
+               os.path.join(GOLDEN, "ref_2dim_mono.npz")))
     subprocess.check_call([sys.executable, "-c", code])
     assert os.path.exists(src)

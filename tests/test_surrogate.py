@@ -123,7 +123,7 @@ def test_conv3x3_forward_and_data_gradient(pkg, Cin, Cout, xs, xo, path):
     try:
         _conv_forward_and_data_gradient(torch, dev, lib, Cin, Cout, xs, xo)
     finally:
-        pkg.surrogate.set_tensor_path(1)
+        pkg.surrogate.set_tensor_path(0)
     assert pkg.surrogate.timeouts(reset=True) == 0
 
 
@@ -303,7 +303,7 @@ def test_network_forward_and_gradients_match_oracle(pkg):
         net.backward(B)
         torch.cuda.synchronize()
     finally:
-        S.set_tensor_path(1)
+        S.set_tensor_path(0)
     yr, cache = U.forward({k: (np.asarray(w, np.float64), np.asarray(b, np.float64)) for k, (w, b) in params.items()},
                           x, bf16=True)
     assert np.linalg.norm(_np(y) - yr.reshape(-1, 3)) <= 1e-2 * np.linalg.norm(yr)
@@ -367,7 +367,7 @@ def test_tcgen05_convolution_matches_oracle(pkg, Cin, Cout, H, W):
             torch.cuda.synchronize()
             outs[path] = (_np(z), _np(a), _np(acc))
     finally:
-        S.set_tensor_path(1)
+        S.set_tensor_path(0)
     assert S.timeouts(reset=True) == 0
     zr = U.conv3x3(x, w, bias)
     z1, a1, acc1 = outs[1]
@@ -394,7 +394,7 @@ def test_network_gradients_on_tcgen05_path(pkg):
         net.backward(2)
         torch.cuda.synchronize()
     finally:
-        S.set_tensor_path(1)
+        S.set_tensor_path(0)
     assert S.timeouts(reset=True) == 0
     yr, cache = U.forward({k: (np.asarray(w, np.float64), np.asarray(b, np.float64)) for k, (w, b) in params.items()},
                           x)
@@ -451,6 +451,7 @@ def test_surrogate_entry_points_reject_bad_arguments_without_a_gpu(pkg):
     assert lib.lbm_nn_head(x, 32, 0, w, None, 64, 32, 9, o, None) == ERR_PARAM
     assert lib.lbm_nn_adam(x, None, w, o, o, 10, 1e-3, 0.9, 0.999, 1e-8, 0.0, 1.0, 0.0, None) == ERR_PARAM
     assert lib.lbm_nn_set_tensor_path(3) == ERR_PARAM
+    assert lib.lbm_nn_set_tensor_path(2) == ERR_PARAM
     assert "path" in P.lbm_last_error().decode()
     assert lib.lbm_nn_get_tensor_path() in (0, 1)
 

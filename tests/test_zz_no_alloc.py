@@ -23,15 +23,22 @@ def test_check_noalloc_agrees_with_lbm_check(pkg, dim):
     n = cav.nnode
     # the previous-check fields start at zero, as lbm_check's do after initial()
     prev = {k: torch.zeros(n, dtype=torch.float64, device="cuda:0") for k in ("u", "v", "w", "T")}
-    for _ in range(2):
+    for it in range(2):
         cav.step(25)
         m = cav.macro()
         cur = {k: _dev(m[k], torch) for k in m}
         torch.cuda.synchronize()
         w = cur["w"].data_ptr() if dim == 3 else None
         wp = prev["w"].data_ptr() if dim == 3 else None
+        free0 = torch.cuda.mem_get_info(0)[0]
         eu, et = pkg.check_noalloc(cur["u"].data_ptr(), cur["v"].data_ptr(), w, cur["T"].data_ptr(),
                                    prev["u"].data_ptr(), prev["v"].data_ptr(), wp, prev["T"].data_ptr(), n)
+        torch.cuda.synchronize()
+        if it > 0:
+            # after the first call on the device, whose set-up only looks up the
+            # static scratch array's address, a call leaves the device's free
+            # memory exactly as it found it
+            assert torch.cuda.mem_get_info(0)[0] == free0
         ru, rt = cav.check()
         # same sums, different block partition: equal to rounding
         assert eu == pytest.approx(ru, rel=1e-12, abs=0.0)

@@ -270,6 +270,9 @@ def kernel_config(cav, pkg):
     if cav.kernel == "march":
         kc["march_blocks"] = cav.get_option(pkg.lbm.OPT_NBLOCKS)
         kc["l2_promotion"] = ["none", "64B", "128B", "256B"][cav.get_option(pkg.lbm.OPT_L2PROMO)]
+        if cav.dim == 3:
+            kc["tile_rows"] = cav.get_option(pkg.lbm.OPT_TILEY)
+            kc["plan"] = ["z-lockstep, balanced tails", "contiguous shares"][cav.get_option(pkg.lbm.OPT_PLAN)]
     return kc
 
 
@@ -515,6 +518,8 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "march"])
     ap.add_argument("--nblocks", type=int, default=0, help="persistent blocks of the march kernel (0 = auto)")
     ap.add_argument("--l2promo", type=int, default=-1, help="TMA L2 promotion 0..3 (-1 = library default)")
+    ap.add_argument("--tiley", type=int, default=0, help="3D march tile rows 4 or 8 (0 = library default)")
+    ap.add_argument("--plan", type=int, default=-1, help="3D march work plan 0 or 1 (-1 = library default)")
     ap.add_argument("--batch-shard", action="store_true",
                     help="batch256 on N GPUs: split one sweep by LPT (strong scaling) instead of one sweep per rank")
     args = ap.parse_args()
@@ -541,6 +546,10 @@ def main():
                      mode=args.mode, device=local, kernel=args.kernel, nblocks=args.nblocks)
     if args.l2promo >= 0:
         cav.set_option(pkg.lbm.OPT_L2PROMO, args.l2promo)
+    if args.tiley and dim == 3:
+        cav.set_option(pkg.lbm.OPT_TILEY, args.tiley)
+    if args.plan >= 0 and dim == 3:
+        cav.set_option(pkg.lbm.OPT_PLAN, args.plan)
     shape = cav.shape
     # pinned host fields for the end-to-end leg
     pin = {k: torch.zeros(shape, dtype=torch.float64, pin_memory=True) for k in ("rho", "u", "v", "w", "T")}

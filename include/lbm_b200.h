@@ -68,6 +68,18 @@ extern "C" {
                                barrier between iterations.  Measured at 128^2 on B200: 3.87 us per
                                iteration in FP32 (4.10 with graph-replayed launches) but 4.85 us
                                in FP64, hence opt-in.  Batch members always step per iteration. */
+#define LBM_OPT_TILEY    6  /* 3D march kernel tile rows: 0 automatic, 4 (two blocks per SM) or 8 */
+#define LBM_OPT_PLAN     7  /* 3D march work plan: 0 (default) every tile column in equal z-chunks
+                               run side by side (neighbours share halo rows through L2), the blocks
+                               left over taking the chunks' last slices in lockstep rounds;
+                               1 contiguous equal shares of the (tile, slice) items */
+#define LBM_OPT_WAIT_LIMIT 8 /* limit, in GPU clock cycles, of the march kernels' waits for their TMA
+                               copies within a step, for every handle on the handle's device;
+                               0 restores the default (4e9, about 2 s).  A wait that runs out sets
+                               the device error flag: the next synchronising call returns
+                               LBM_ERR_TIMEOUT and the populations are not valid until the next
+                               init call.  For tests of that error path.  lbm_get_option reports
+                               the value last set through this handle (0: default). */
 
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */
@@ -162,7 +174,10 @@ int lbm_step(lbm_handle *h, int32_t nsteps);
  * check_every iterations (counted from the last init, as itc is), both
  * residuals of lbm_check are at most eps, or max_steps iterations were done.
  * Reports the iterations done and the last residuals; returns
- * LBM_ERR_NONFINITE if a residual sum stops being finite. */
+ * LBM_ERR_NONFINITE if a residual sum stops being finite.  The stop test runs
+ * on the device after each check (the same sums and residuals as lbm_check):
+ * once it fires, the steps queued after it do nothing, and the host
+ * synchronises once every four checks instead of at every check. */
 int lbm_run(lbm_handle *h, int64_t max_steps, int32_t check_every, double eps,
             int64_t *steps_done, double *errU, double *errT);
 
@@ -232,9 +247,11 @@ int64_t lbm_kernel_launches(void);
 /* ------------------------------------------------------------------------ */
 typedef struct lbm_batch lbm_batch;
 
-#define LBM_BATCH_OPT_TILE        1  /* tile width of the 2D batch kernel: 32, 64, 128 */
+#define LBM_BATCH_OPT_TILE        1  /* tile width of the 2D batch kernel: 32, 64, 128 (3D: 32 x 8) */
 #define LBM_BATCH_OPT_NBLOCKS     2  /* persistent blocks (0 = one full wave) */
-#define LBM_BATCH_OPT_PERSISTENT  3  /* 1: one persistent kernel per step, 0: one launch per cavity */
+#define LBM_BATCH_OPT_PERSISTENT  3  /* 1: one persistent kernel per step (2D and 3D; a 3D batch with a
+                                        member whose ny % 8 == 1 steps per member), 0: one launch per
+                                        cavity */
 #define LBM_BATCH_OPT_GRAPHS      4  /* 1: replay steps from CUDA graphs */
 #define LBM_BATCH_OPT_GROWTH      5  /* lbm_batch_run stops a member whose residual is not finite or
                                         exceeds this factor x its smallest one in the run and reports
@@ -261,7 +278,10 @@ int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold);
 /* The reference's loop for every member (2M:307-330): step check_every
  * iterations, check, and retire members whose errorU and errorT are both at
  * most eps; stop when all are retired or after max_steps.  converged[i] and
- * steps_done[i] (optional) report each member's outcome. */
+ * steps_done[i] (optional) report each member's outcome.  The stop test runs
+ * on the device after each check: a stopped member's kernels become no-ops at
+ * once, and the host reads all members' state (one copy, one
+ * synchronisation) once every four checks to shrink the work list. */
 int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps,
                   int32_t *converged, int64_t *steps_done);
 /* lbm_batch_run over the members with mask[i] != 0 only (the others are not
@@ -298,6 +318,17 @@ int lbm_check_noalloc(const double *u, const double *v, const double *w,
                       const double *T, double *u_prev, double *v_prev,
                       double *w_prev, double *T_prev, int64_t n,
                       double *errU, double *errT, void *stream);
+
+/* The 3D march kernel's work plan (host code, no device needed), for tools
+ * and tests that check it: ntiles tile columns of nz slices over `nblocks`
+ * persistent blocks, kind as LBM_OPT_PLAN.  On entry *seg_count is the
+ * capacity of segs (in segments); on return the number of segments.  segs
+ * receives (tile, first slice, end slice) per segment, off (blocks_used + 1
+ * entries) each block's first segment.  segs or off NULL: size query only.
+ * No reference counterpart (the reference runs one MPI rank per subdomain). */
+int lbm_march_plan3d(int32_t ntiles, int32_t nz, int32_t nblocks, int32_t kind,
+                     int32_t *seg_count, int32_t *segs, int32_t *off,
+                     int32_t *blocks_used);
 
 #ifdef __cplusplus
 }

@@ -10,12 +10,17 @@
 //     in device memory;
 //   * steps between checks are replayed from 2-step CUDA graphs;
 //   * lbm_batch_run applies the reference's stop test per cavity (errorU and
-//     errorT at most eps at a check, 2M:307) and drops converged cavities
+//     errorT at most eps at a check, 2M:307) and drops stopped cavities
 //     from the work list;
 //   * lbm_batch_tune times the tile widths and grid sizes on the batch itself
 //     and keeps the fastest;
-//   * 3D batches (and 2D batches with the persistent kernel switched off)
-//     step every cavity with its own kernel launch on the batch's stream.
+//   * 3D batches: one persistent TMA march kernel per step too
+//     (k_march3d_batch), over segments (tile, first slice, end slice,
+//     cavity) that split the (tile column, slice) items into equal shares;
+//   * with the persistent kernel switched off (or a 3D member the march
+//     kernel does not cover), every cavity steps with its own launch;
+//   * lbm_batch_run and lbm_batch_run_masked test the stop criterion on the
+//     device and read the members' run state once every few checks.
 // Every member is an ordinary lbm_handle (lbm_batch_cavity) sharing the
 // batch's stream, so initialisation, checks and getters are the single-
 // cavity entry points.
@@ -47,6 +52,7 @@ struct lbm_batch {
     int tile_opt = 0, tile = 64;   // tile width of the 2D batch kernel (32, 64, 128)
     int nblocks_opt = 0, nblocks = 0;
     int persistent = 1;            // 0: one launch per cavity
+    bool march_ok = true;          // every member can run in the persistent kernel (3D: tile rows fit)
     int use_graphs = 1;
     double growth = 0.0;           // residual growth factor that stops a member in lbm_batch_run (0: off)
     Geo *d_geo = nullptr;
@@ -59,12 +65,22 @@ struct lbm_batch {
     BatchDev dev{};
     bool dirty = true;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t run_graph[2] = {nullptr, nullptr};  // check periods of lbm_batch_run from cur = 0 / 1
+    int run_graph_period = 0;
     int64_t active_nodes = 0;
+    RunCtl *d_ctl = nullptr;       // run state of every member (member i's bufs.ctl = d_ctl + i)
+    int *d_idx = nullptr;          // members on the work list, for the batched check
+    int nidx = 0;
 };
 
 static void drop_graphs(lbm_batch *b)
 {
     for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    for (auto &g : b->run_graph)
         if (g) {
             cudaGraphExecDestroy(g);
             g = nullptr;
@@ -78,7 +94,7 @@ extern "C" int lbm_batch_destroy(lbm_batch *b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
     for (lbm_handle *h : b->cav) lbm_destroy(h);
-    void *ptrs[] = {b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff, b->d_err};
+    void *ptrs[] = {b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff, b->d_err, b->d_ctl, b->d_idx};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -125,7 +141,23 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
         b->cav.push_back(h);
     }
     b->active.assign(n, 1);
-    if (b->dim == 2) {
+    {
+        // one run-state array for all members, so a run reads every member's state in one copy
+        cudaError_t e = cudaMalloc(&b->d_ctl, sizeof(RunCtl) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_idx, sizeof(int) * n);
+        std::vector<RunCtl> c(n);
+        for (auto &x : c) x.active = 1;
+        if (e == cudaSuccess) e = cudaMemcpy(b->d_ctl, c.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(set_error(LBM_ERR_NOMEM, "batch run state: %s", cudaGetErrorString(e)));
+        for (int i = 0; i < n; ++i) {
+            lbm_handle *h = b->cav[i];
+            cudaFree(h->bufs.ctl);
+            h->bytes -= (int64_t)sizeof(RunCtl);
+            h->bufs.ctl = b->d_ctl + i;
+            h->owns_ctl = false;
+        }
+    }
+    {
         cudaError_t e = cudaMalloc(&b->d_geo, sizeof(Geo) * n);
         if (e == cudaSuccess) e = cudaMalloc(&b->d_bufs, sizeof(Bufs) * n);
         if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, sizeof(TmapSet) * 2 * n);
@@ -142,23 +174,30 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
         if (e == cudaSuccess) e = cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e)));
     }
+    // the 3D batch kernel has 32 x 8 tiles: a last tile row of a single y-row
+    // (its one-sided stencil would reach two rows below the box) is not covered
+    if (b->dim == 3)
+        for (int i = 0; i < n; ++i)
+            if (b->cav[i]->geo.ny % 8 == 1 || b->cav[i]->tiley != 8) b->march_ok = false;
     *out = b;
     return LBM_OK;
 }
 
-// descriptors for the tile width, and the work list of the active cavities
+// descriptors for the tile width, and the work list of the active cavities.
+// A column is one march: 2D a TX-wide strip of rows, 3D a 32 x 8 tile of slices.
 static int build_tables(lbm_batch *b)
 {
     drop_graphs(b);
-    const int TX = b->tile;
+    const bool d3 = b->dim == 3;
+    const int TX = d3 ? 32 : b->tile;
     std::vector<TmapSet> maps(2 * (size_t)b->n);
     for (int i = 0; i < b->n; ++i)
-        if (!encode_maps_tx(b->cav[i], TX, &maps[2 * (size_t)i]))
+        if (!encode_maps_tx(b->cav[i], d3 ? 0 : TX, &maps[2 * (size_t)i]))
             return set_error(LBM_ERR_UNSUPPORTED, "batch: TMA descriptors for cavity %d could not be encoded", i);
     BCU(cudaMemcpyAsync(b->d_maps, maps.data(), sizeof(TmapSet) * maps.size(), cudaMemcpyHostToDevice, b->stream));
 
     struct Col {
-        int cav, i0, ny;
+        int cav, pos, ny;  // pos: 2D the strip's x-offset, 3D the tile index; ny: items (rows or slices)
     };
     std::vector<Col> cols;
     int64_t total = 0;
@@ -166,12 +205,20 @@ static int build_tables(lbm_batch *b)
     for (int i = 0; i < b->n; ++i) {
         if (!b->active[i]) continue;
         const Geo &g = b->cav[i]->geo;
-        for (int i0 = 0; i0 < g.nx; i0 += TX) cols.push_back({i, i0, g.ny});
-        total += (int64_t)((g.nx + TX - 1) / TX) * g.ny;
+        if (d3) {
+            const int nt = ((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+            for (int t = 0; t < nt; ++t) cols.push_back({i, t, g.nz});
+            total += (int64_t)nt * g.nz;
+        } else {
+            for (int i0 = 0; i0 < g.nx; i0 += TX) cols.push_back({i, i0, g.ny});
+            total += (int64_t)((g.nx + TX - 1) / TX) * g.ny;
+        }
         b->active_nodes += g.nnode;
     }
-    const int bps = b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, TX)
-                                              : fast::march_batch_blocks_per_sm(b->storage, TX);
+    const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(b->storage)
+                                                     : fast::march_batch3d_blocks_per_sm(b->storage))
+                       : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, TX)
+                                                    : fast::march_batch_blocks_per_sm(b->storage, TX));
     if (bps <= 0) return set_error(LBM_ERR_UNSUPPORTED, "batch kernel with tile %d cannot be resident", TX);
     int sms = 0;
     BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
@@ -191,7 +238,10 @@ static int build_tables(lbm_batch *b)
         while (u < hi) {
             while (c < cols.size() && colbase + cols[c].ny <= u) colbase += cols[c++].ny;
             const int64_t end = std::min<int64_t>(hi, colbase + cols[c].ny);
-            segs.push_back(make_int4(cols[c].cav, cols[c].i0, (int)(u - colbase), (int)(end - colbase)));
+            if (d3)
+                segs.push_back(make_int4(cols[c].pos, (int)(u - colbase), (int)(end - colbase), cols[c].cav));
+            else
+                segs.push_back(make_int4(cols[c].cav, cols[c].pos, (int)(u - colbase), (int)(end - colbase)));
             u = end;
         }
     }
@@ -211,12 +261,24 @@ static int build_tables(lbm_batch *b)
     BCU(cudaMemcpyAsync(b->d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
     b->dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff};
+    {
+        std::vector<int> idx;
+        for (int i = 0; i < b->n; ++i)
+            if (b->active[i]) idx.push_back(i);
+        b->nidx = (int)idx.size();
+        if (!idx.empty())
+            BCU(cudaMemcpy(b->d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice));
+    }
     b->dirty = false;
     return LBM_OK;
 }
 
 static cudaError_t launch_step(lbm_batch *b, int cur, int wm)
 {
+    if (b->dim == 3)
+        return b->mode == LBM_MODE_EXACT
+                   ? exact::march_batch3d(b->storage, b->dev, b->nblocks, cur, wm, b->d_err, b->stream)
+                   : fast::march_batch3d(b->storage, b->dev, b->nblocks, cur, wm, b->d_err, b->stream);
     return b->mode == LBM_MODE_EXACT
                ? exact::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream)
                : fast::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream);
@@ -254,7 +316,7 @@ extern "C" int lbm_batch_step(lbm_batch *b, int32_t nsteps)
     for (int i = 0; i < b->n; ++i)
         if (b->active[i] && b->cav[i]->phase == 0)
             return set_error(LBM_ERR_STATE, "batch: cavity %d stepped before an init call", i);
-    if (b->dim == 3 || !b->persistent) {
+    if (!b->persistent || !b->march_ok) {
         for (int i = 0; i < b->n; ++i)
             if (b->active[i]) {
                 int st = lbm_step(b->cav[i], nsteps);
@@ -369,53 +431,159 @@ extern "C" int lbm_batch_nusselt(lbm_batch *b, double *nu_hot, double *nu_cold)
     return LBM_OK;
 }
 
+// One check period of a persistent batch as a graph: `period` steps of every
+// member on the work list, the last writing the macroscopic fields, then the
+// batched check with the stop test on the device.
+static int batch_period_graph(lbm_batch *b, int cur, int period, cudaGraphExec_t *out)
+{
+    if (b->run_graph_period != period) {
+        for (auto &g : b->run_graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        b->run_graph_period = period;
+    }
+    if (!b->run_graph[cur]) {
+        cudaGraph_t g = nullptr;
+        BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < period && e == cudaSuccess; ++i) e = launch_step(b, (cur + i) & 1, i == period - 1);
+        if (e == cudaSuccess) e = run_check_batch(b->dev, b->d_idx, b->nidx, period, b->stream);
+        const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+        g_launches -= period + 2;  // counted when replayed
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return set_error(LBM_ERR_CUDA, "batch check-period graph capture: %s",
+                             cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&b->run_graph[cur], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return set_error(LBM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = b->run_graph[cur];
+    return LBM_OK;
+}
+
+// check periods a batch run queues between two reads of the members' run state
+static constexpr int kBatchPeriodsPerRead = 4;
+
 extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
                                     double eps, int32_t *converged, int64_t *steps_done)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
     if (max_steps < 0 || check_every < 1) return set_error(LBM_ERR_PARAM, "need max_steps >= 0, check_every >= 1");
-    std::vector<double> eu(b->n), et(b->n), best(b->n, INFINITY);
-    std::vector<int> checks(b->n, 0);
+    BCU(cudaSetDevice(b->device));
+    const int n = b->n;
     int remaining = 0;
-    for (int i = 0; i < b->n; ++i) {
+    for (int i = 0; i < n; ++i) {
         const bool on = !mask || mask[i] != 0;
         if (converged) converged[i] = 0;
         if (steps_done) steps_done[i] = 0;
         b->active[i] = on ? 1 : 0;
         remaining += on ? 1 : 0;
     }
+    for (int i = 0; i < n; ++i)
+        if (b->active[i] && b->cav[i]->phase == 0)
+            return set_error(LBM_ERR_STATE, "batch: cavity %d run before an init call", i);
+    for (int i = 0; i < n; ++i)
+        if (b->active[i]) {
+            int st = first_collision(b->cav[i]);
+            if (st) return st;
+        }
+    // the stop test of every member runs on the device (run_decide): the
+    // reference's criterion (errorU, errorT <= eps, 2M:307) and, with
+    // LBM_BATCH_OPT_GROWTH, a residual that stops being finite or grows past
+    // growth x its smallest value in this run stops the member (status -1)
+    std::vector<RunCtl> ctl(n);
+    for (int i = 0; i < n; ++i) {
+        ctl[i] = RunCtl{};
+        ctl[i].active = b->active[i];  // members off the mask stay out of the batched check
+        ctl[i].errU = ctl[i].errT = 100.0;
+        ctl[i].best = INFINITY;
+        ctl[i].eps = eps;
+        ctl[i].growth = b->growth;
+        ctl[i].stop_bad = 1;
+    }
+    BCU(cudaMemcpyAsync(b->d_ctl, ctl.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    std::vector<int64_t> itc0(n);
+    std::vector<int> cur0(n);
+    for (int i = 0; i < n; ++i) {
+        itc0[i] = b->cav[i]->itc;
+        cur0[i] = b->cav[i]->cur;
+    }
     b->dirty = true;
+    const bool persistent = b->persistent && b->march_ok;
     int64_t steps = 0;
+    int periods = 0;
     int st = LBM_OK;
     while (steps < max_steps && remaining > 0) {
         const int k = (int)std::min<int64_t>(check_every, max_steps - steps);
-        if ((st = lbm_batch_step(b, k))) break;
+        if (persistent) {
+            if (b->dirty && (st = build_tables(b))) break;
+            // the common parity of the members on the work list
+            int cur = -1;
+            for (int i = 0; i < n; ++i)
+                if (b->active[i]) {
+                    if (cur < 0) cur = b->cav[i]->cur;
+                    if (b->cav[i]->cur != cur) {
+                        st = set_error(LBM_ERR_STATE, "batch: cavity %d is out of step with the others", i);
+                        break;
+                    }
+                }
+            if (st) break;
+            if (b->use_graphs && k >= 2) {
+                cudaGraphExec_t g;
+                if ((st = batch_period_graph(b, cur, k, &g))) break;
+                cudaError_t e = cudaGraphLaunch(g, b->stream);
+                if (e != cudaSuccess) {
+                    st = set_error(LBM_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
+                    break;
+                }
+                g_launches += k + 2;
+            } else {
+                for (int i = 0; i < k && !st; ++i) {
+                    cudaError_t e = launch_step(b, (cur + i) & 1, i == k - 1);
+                    if (e != cudaSuccess) st = set_error(LBM_ERR_CUDA, "batch step: %s", cudaGetErrorString(e));
+                }
+                if (st) break;
+                cudaError_t e = run_check_batch(b->dev, b->d_idx, b->nidx, k, b->stream);
+                if (e != cudaSuccess) {
+                    st = set_error(LBM_ERR_CUDA, "batch check: %s", cudaGetErrorString(e));
+                    break;
+                }
+            }
+            for (int i = 0; i < n; ++i)
+                if (b->active[i]) {
+                    b->cav[i]->cur = (cur + k) & 1;
+                    b->cav[i]->itc += k;
+                }
+        } else {
+            // one launch per member (the persistent kernel switched off)
+            for (int i = 0; i < n && !st; ++i)
+                if (b->active[i]) {
+                    lbm_handle *h = b->cav[i];
+                    if ((st = lbm_step(h, k))) break;
+                    cudaError_t e = run_check(h->geo, h->bufs, k, b->stream);
+                    if (e != cudaSuccess) st = set_error(LBM_ERR_CUDA, "batch check: %s", cudaGetErrorString(e));
+                }
+            if (st) break;
+        }
         steps += k;
+        if (++periods % kBatchPeriodsPerRead != 0 && steps < max_steps) continue;
+        // read every member's run state: one copy, one synchronisation
+        BCU(cudaMemcpyAsync(ctl.data(), b->d_ctl, sizeof(RunCtl) * n, cudaMemcpyDeviceToHost, b->stream));
         if ((st = lbm_batch_synchronize(b))) break;
         bool changed = false;
-        for (int i = 0; i < b->n; ++i) {
+        for (int i = 0; i < n; ++i) {
             if (!b->active[i]) continue;
-            st = lbm_check(b->cav[i], &eu[i], &et[i]);
-            if (steps_done) steps_done[i] = steps;
-            const double r = std::max(eu[i], et[i]);
-            // a member whose residual stops being finite, or grows past growth x
-            // its smallest value in this run, is stopped and reported as -1
-            const bool bad = st == LBM_ERR_NONFINITE || !std::isfinite(r) ||
-                             (b->growth > 0 && checks[i] >= 2 && r > b->growth * best[i]);
-            if (st && st != LBM_ERR_NONFINITE) break;
-            if (st == LBM_ERR_NONFINITE && b->growth <= 0) break;
-            st = LBM_OK;
-            ++checks[i];
-            best[i] = std::min(best[i], r);
-            if (bad) {
+            if (ctl[i].status == -2) {
+                st = set_error(LBM_ERR_NONFINITE, "check: non-finite residual sum (cavity %d)", i);
+                break;
+            }
+            if (!ctl[i].active) {
                 b->active[i] = 0;
-                if (converged) converged[i] = -1;
-                --remaining;
-                changed = true;
-            } else if (!(eu[i] > eps || et[i] > eps)) {
-                // the reference keeps iterating while errorU > eps or errorT > eps (2M:307)
-                b->active[i] = 0;
-                if (converged) converged[i] = 1;
                 --remaining;
                 changed = true;
             }
@@ -423,7 +591,26 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
         if (st) break;
         if (changed) b->dirty = true;
     }
-    b->active.assign(b->n, 1);
+    // the final state: iterations each member ran, its parity and counter
+    cudaError_t e = cudaMemcpyAsync(ctl.data(), b->d_ctl, sizeof(RunCtl) * n, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess && !st) st = set_error(LBM_ERR_CUDA, "batch run state: %s", cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+        const bool on = !mask || mask[i] != 0;
+        if (!on) continue;
+        lbm_handle *h = b->cav[i];
+        const int64_t ran = ctl[i].active ? steps : ctl[i].steps;
+        h->itc = itc0[i] + ran;
+        h->cur = (int)((cur0[i] + ran) & 1);
+        if (steps_done) steps_done[i] = ran;
+        if (converged) converged[i] = ctl[i].active ? 0 : (ctl[i].status == 1 ? 1 : (ctl[i].status == -1 ? -1 : 0));
+        if (!st && ctl[i].status == -2) st = set_error(LBM_ERR_NONFINITE, "check: non-finite residual sum (cavity %d)", i);
+    }
+    for (auto &c : ctl) c.active = 1;
+    e = cudaMemcpyAsync(b->d_ctl, ctl.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess && !st) st = set_error(LBM_ERR_CUDA, "batch run state: %s", cudaGetErrorString(e));
+    b->active.assign(n, 1);
     b->dirty = true;
     return st;
 }
@@ -437,21 +624,27 @@ extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_ever
 extern "C" int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
-    if (b->dim != 2) return set_error(LBM_ERR_UNSUPPORTED, "lbm_batch_tune: 2D batches only");
+    if (!b->persistent || !b->march_ok)
+        return set_error(LBM_ERR_UNSUPPORTED, "lbm_batch_tune: the batch does not use the persistent kernel");
     if (steps < 2) steps = 2;
     BCU(cudaSetDevice(b->device));
     int sms = 0;
     BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    const int tiles[3] = {32, 64, 128};
+    const int tiles2[3] = {32, 64, 128}, tiles3[1] = {32};  // 3D: the tile is fixed at 32 x 8
+    const int *tiles = b->dim == 3 ? tiles3 : tiles2;
+    const int ntile = b->dim == 3 ? 1 : 3;
     double best = -1.0;
     int best_tile = b->tile, best_nb = 0;
     cudaEvent_t e0, e1;
     BCU(cudaEventCreate(&e0));
     BCU(cudaEventCreate(&e1));
     const int keep_nb = b->nblocks_opt;
-    for (int t : tiles) {
-        const int bps = b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, t)
-                                                  : fast::march_batch_blocks_per_sm(b->storage, t);
+    for (int ti = 0; ti < ntile; ++ti) {
+        const int t = tiles[ti];
+        const int bps = b->dim == 3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(b->storage)
+                                                                 : fast::march_batch3d_blocks_per_sm(b->storage))
+                                    : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, t)
+                                                                 : fast::march_batch_blocks_per_sm(b->storage, t));
         if (bps <= 0) continue;
         const int cands[2] = {bps, bps > 1 ? bps / 2 : 0};
         for (int c : cands) {

@@ -275,7 +275,7 @@ static void free_all(lbm_handle *h)
                     h->bufs.v, h->bufs.w, h->bufs.T, h->bufs.up, h->bufs.vp, h->bufs.wp, h->bufs.Tp,
                     h->bufs.partials, h->bufs.scal, h->d_wgt[0], h->d_wgt[1], h->d_wgt[2], h->d_coord[0],
                     h->d_coord[1], h->d_coord[2], h->d_cellw[0], h->d_cellw[1], h->d_cellw[2], h->staging,
-                    h->aos, h->bufs.err, h->d_bar};
+                    h->aos, h->bufs.err, h->d_bar, h->d_msegs, h->d_msegoff, h->owns_ctl ? h->bufs.ctl : nullptr};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->stream && h->owns_stream) cudaStreamDestroy(h->stream);
@@ -320,7 +320,7 @@ bool lbm::encode_maps_tx(const lbm_handle *h, int tx, TmapSet out[2])
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     const Geo &g = h->geo;
-    const MarchShape ms = march_shape(g.dim, h->p.storage, tx);
+    const MarchShape ms = march_shape(g.dim, h->p.storage, tx, h->tiley);
     const CUtensorMapDataType dtype = h->p.storage == LBM_STORE_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
                                       : h->p.storage == LBM_STORE_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                                       : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
@@ -385,9 +385,134 @@ static bool encode_maps(lbm_handle *h) { return lbm::encode_maps_tx(h, 0, h->tma
 static bool march_supported(const lbm_handle *h)
 {
     if (!h->march_ok) return false;
-    const MarchShape ms = march_shape(h->geo.dim, h->p.storage);
+    const MarchShape ms = march_shape(h->geo.dim, h->p.storage, 0, h->tiley);
     if (h->geo.dim == 3 && h->geo.ny % ms.TY == 1) return false;
     return true;
+}
+
+// tile rows of the 3D march kernel unless LBM_OPT_TILEY says otherwise
+static constexpr int kDefaultTileY = 8;
+
+// ---------------------------------------------------------------------------
+// 3D march work plan
+// ---------------------------------------------------------------------------
+// Neighbouring tiles share halo rows and columns: when two neighbours are at
+// the same slice at about the same time, the second reader finds those rows
+// in L2.  A grid of (tile columns x equal z-chunks) blocks keeps every tile in
+// lockstep with its neighbours but seldom fills the SMs: the 64 tile columns
+// of a 128^3 cube on 148 SMs give 2 chunks, 128 blocks, and 20 idle SMs.  Here
+// the left-over blocks take each chunk's last r slices ("tails"), round-robin
+// over the tails in (chunk, tile) order, so each round is a patch of
+// consecutive tiles that also run side by side.  r balances a main chunk (its
+// length less r, plus one pipeline start) against the busiest tail block
+// (one start and r slices per round).
+int lbm::plan_march3d(int ntiles, int nz, int nblocks, int kind, std::vector<int4> &segs, std::vector<int> &off)
+{
+    segs.clear();
+    off.clear();
+    const int64_t total = (int64_t)ntiles * nz;
+    int64_t G = nblocks < 1 ? 1 : nblocks;
+    if (G > total) G = total;
+    auto push = [&](int t, int z0, int z1) { segs.push_back(make_int4(t, z0, z1, 0)); };
+    const int c = (int)(G / ntiles);
+    if (kind == 1 || c < 1) {
+        for (int64_t b = 0; b < G; ++b) {
+            off.push_back((int)segs.size());
+            int64_t u = total * b / G;
+            const int64_t hi = total * (b + 1) / G;
+            while (u < hi) {
+                const int t = (int)(u / nz), z0 = (int)(u % nz);
+                const int z1 = (int)std::min<int64_t>(nz, z0 + (hi - u));
+                push(t, z0, z1);
+                u += z1 - z0;
+            }
+        }
+        off.push_back((int)segs.size());
+        return (int)G;
+    }
+    const int E = (int)(G - (int64_t)c * ntiles);
+    auto zb = [&](int k) { return (int)((int64_t)k * nz / c); };
+    const int minL = nz / c;  // chunk lengths are minL or minL + 1
+    int r = 0;
+    if (E > 0 && minL >= 4) {
+        const double start = 1.5;  // a segment's pipeline start, in slice times
+        const int rounds = (c * ntiles + E - 1) / E;
+        double best = (double)(minL + 1) + start;  // r = 0: the left-over blocks stay idle
+        for (int rr = 1; rr < minL / 2; ++rr) {
+            const double t = std::max((double)(minL + 1 - rr) + start, rounds * (rr + start));
+            if (t < best - 1e-9) {
+                best = t;
+                r = rr;
+            }
+        }
+    }
+    for (int k = 0; k < c; ++k)
+        for (int t = 0; t < ntiles; ++t) {
+            off.push_back((int)segs.size());
+            push(t, zb(k), zb(k + 1) - r);
+        }
+    if (r > 0) {
+        const int ntail = c * ntiles;
+        for (int e = 0; e < E; ++e) {
+            off.push_back((int)segs.size());
+            for (int i = e; i < ntail; i += E) push(i % ntiles, zb(i / ntiles + 1) - r, zb(i / ntiles + 1));
+        }
+    }
+    off.push_back((int)segs.size());
+    return (int)off.size() - 1;
+}
+
+// plan the 3D march for grid G and upload it; sets h->nblocks
+static int upload_plan3d(lbm_handle *h, int G)
+{
+    CU(cudaStreamSynchronize(h->stream));  // no launch in flight reads the old plan
+    const MarchShape ms = march_shape(3, h->p.storage, 0, h->tiley);
+    const int ntiles = ((h->geo.nx + ms.TX - 1) / ms.TX) * ((h->geo.ny + ms.TY - 1) / ms.TY);
+    std::vector<int4> segs;
+    std::vector<int> off;
+    const int nb = lbm::plan_march3d(ntiles, h->geo.nz, G, h->plan_opt, segs, off);
+    if (segs.size() > h->msegs_cap) {
+        if (h->d_msegs) cudaFree(h->d_msegs);
+        h->d_msegs = nullptr;
+        h->msegs_cap = 0;
+        int st = dalloc(h, &h->d_msegs, sizeof(int4) * segs.size());
+        if (st) return st;
+        h->msegs_cap = segs.size();
+    }
+    if (off.size() > h->msegoff_cap) {
+        if (h->d_msegoff) cudaFree(h->d_msegoff);
+        h->d_msegoff = nullptr;
+        h->msegoff_cap = 0;
+        int st = dalloc(h, &h->d_msegoff, sizeof(int) * off.size());
+        if (st) return st;
+        h->msegoff_cap = off.size();
+    }
+    CU(cudaMemcpy(h->d_msegs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(h->d_msegoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice));
+    h->nblocks = nb;
+    return LBM_OK;
+}
+
+extern "C" int lbm_march_plan3d(int32_t ntiles, int32_t nz, int32_t nblocks, int32_t kind, int32_t *seg_count,
+                                int32_t *segs, int32_t *off, int32_t *blocks_used)
+{
+    if (ntiles < 1 || nz < 3 || nblocks < 1 || (kind != 0 && kind != 1) || !seg_count)
+        return fail(LBM_ERR_PARAM, "lbm_march_plan3d: bad arguments");
+    std::vector<int4> sg;
+    std::vector<int> of;
+    const int nb = lbm::plan_march3d(ntiles, nz, nblocks, kind, sg, of);
+    const int cap = *seg_count;
+    *seg_count = (int32_t)sg.size();
+    if (blocks_used) *blocks_used = nb;
+    if (!segs || !off) return LBM_OK;  // size query
+    if ((int)sg.size() > cap) return fail(LBM_ERR_PARAM, "lbm_march_plan3d: %d segments do not fit", (int)sg.size());
+    for (size_t i = 0; i < sg.size(); ++i) {
+        segs[3 * i] = sg[i].x;
+        segs[3 * i + 1] = sg[i].y;
+        segs[3 * i + 2] = sg[i].z;
+    }
+    for (size_t i = 0; i < of.size(); ++i) off[i] = of[i];
+    return LBM_OK;
 }
 
 static int resolve_path(lbm_handle *h)
@@ -398,8 +523,8 @@ static int resolve_path(lbm_handle *h)
         return fail(LBM_ERR_UNSUPPORTED, "march kernel not available for this shape / device");
     h->use_march = h->kernel_opt == 2 || (h->kernel_opt == 0 && ok && h->geo.nnode >= (1 << 15));
     if (h->use_march) {
-        const int bps = h->p.mode == LBM_MODE_EXACT ? exact::march_blocks_per_sm(h->geo, h->p.storage)
-                                                   : fast::march_blocks_per_sm(h->geo, h->p.storage);
+        const int bps = h->p.mode == LBM_MODE_EXACT ? exact::march_blocks_per_sm(h->geo, h->p.storage, h->tiley)
+                                                   : fast::march_blocks_per_sm(h->geo, h->p.storage, h->tiley);
         if (bps <= 0) {
             if (h->kernel_opt == 2) return fail(LBM_ERR_UNSUPPORTED, "march kernel cannot be resident");
             h->use_march = 0;
@@ -408,7 +533,11 @@ static int resolve_path(lbm_handle *h)
         int sms = 0;
         CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
         const int slots = bps * sms;
-        if (h->nblocks_opt > 0) {
+        if (h->geo.dim == 3) {
+            // one full wave, planned
+            int st = upload_plan3d(h, h->nblocks_opt > 0 ? h->nblocks_opt : slots);
+            if (st) return st;
+        } else if (h->nblocks_opt > 0) {
             h->nblocks = h->nblocks_opt;
         } else {
             // z-lockstep grid: every tile column split into the same number of
@@ -528,6 +657,13 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
         (st = dalloc(h, &b.partials, 592 * 4 * 8)) || (st = dalloc(h, &b.scal, 16 * 8)))
         return bail(st);
     if ((st = dalloc(h, &b.err, 16))) return bail(st);
+    if ((st = dalloc(h, &b.ctl, sizeof(RunCtl)))) return bail(st);
+    {
+        RunCtl c{};
+        c.active = 1;
+        if (cudaMemcpy(b.ctl, &c, sizeof c, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(fail(LBM_ERR_CUDA, "run state upload failed"));
+    }
     if ((st = dalloc(h, &h->d_bar, 2 * sizeof(unsigned)))) return bail(st);
     if (cudaMemset(h->d_bar, 0, 2 * sizeof(unsigned)) != cudaSuccess)
         return bail(fail(LBM_ERR_CUDA, "memset failed"));
@@ -676,9 +812,9 @@ static cudaError_t launch_one(lbm_handle *h, int cur, int wm)
     const int nxt = 1 - cur;
     if (h->use_march)
         return ex ? exact::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
-                                 h->nblocks, h->stream)
+                                 h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->stream)
                   : fast::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
-                                h->nblocks, h->stream);
+                                h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->stream);
     return ex ? exact::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream)
               : fast::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream);
 }
@@ -686,6 +822,11 @@ static cudaError_t launch_one(lbm_handle *h, int cur, int wm)
 void lbm::drop_graphs(lbm_handle *h)
 {
     for (auto &g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+    for (auto &g : h->run_graph)
         if (g) {
             cudaGraphExecDestroy(g);
             g = nullptr;
@@ -754,34 +895,141 @@ extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
     return LBM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// runs to the reference's stop criterion with the test on the device
+// ---------------------------------------------------------------------------
+// The reference's loop (2M:307-330) iterates while errorU > eps or errorT > eps,
+// calling check() every check_every iterations.  Here each check period (its
+// steps, the check sums and the stop test) is queued without waiting for the
+// previous one: the test runs on the device (run_check) and, once it fires,
+// clears RunCtl::active, which turns the step and check kernels queued after it
+// into no-ops.  The host reads the run state once every kRunPeriodsPerRead
+// periods, so a run syncs once per that many checks instead of once per check.
+static constexpr int kRunPeriodsPerRead = 4;
+
+static int sync_and_check(lbm_handle *h);
+
+int lbm::run_begin(lbm_handle *h, double eps, double growth, int stop_bad)
+{
+    RunCtl c{};
+    c.active = 1;
+    c.errU = c.errT = 100.0;
+    c.best = INFINITY;
+    c.eps = eps;
+    c.growth = growth;
+    c.stop_bad = stop_bad;
+    CU(cudaMemcpyAsync(h->bufs.ctl, &c, sizeof c, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+int lbm::run_read(lbm_handle *h, RunCtl *out)
+{
+    CU(cudaMemcpyAsync(out, h->bufs.ctl, sizeof *out, cudaMemcpyDeviceToHost, h->stream));
+    return sync_and_check(h);
+}
+
+int lbm::run_end(lbm_handle *h)
+{
+    static const int one = 1;
+    CU(cudaMemcpyAsync(&h->bufs.ctl->active, &one, sizeof one, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return LBM_OK;
+}
+
+// one check period of `period` iterations from buffer `cur` as a graph
+// (steps, the last writing the macroscopic fields, then the device check)
+static int period_graph(lbm_handle *h, int cur, int period, cudaGraphExec_t *out)
+{
+    if (h->run_graph_period != period) {
+        for (auto &g : h->run_graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        h->run_graph_period = period;
+    }
+    if (!h->run_graph[cur]) {
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < period && e == cudaSuccess; ++i) e = launch_one(h, (cur + i) & 1, i == period - 1);
+        if (e == cudaSuccess) e = run_check(h->geo, h->bufs, period, h->stream);
+        const cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        lbm::g_launches -= period + 2;  // counted when replayed
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(LBM_ERR_CUDA, "check-period graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&h->run_graph[cur], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(LBM_ERR_CUDA, "check-period graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *out = h->run_graph[cur];
+    return LBM_OK;
+}
+
 extern "C" int lbm_run(lbm_handle *h, int64_t max_steps, int32_t check_every, double eps, int64_t *steps_done,
                        double *errU, double *errT)
 {
     CHECK_H(h);
     if (max_steps < 0 || check_every < 1) return fail(LBM_ERR_PARAM, "need max_steps >= 0 and check_every >= 1");
     if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_run before an init call");
-    // the reference's loop (2M:307-330): iterate while errorU > eps or
-    // errorT > eps, checking every check_every iterations
-    double eu = 100.0, et = 100.0;
-    int64_t done = 0;
-    while ((eu > eps || et > eps) && done < max_steps) {
-        const int64_t k = std::min<int64_t>(check_every - (h->itc % check_every), max_steps - done);
-        int st = lbm_step(h, (int32_t)k);
-        if (st) return st;
-        done += k;
-        if (h->itc % check_every == 0) {
-            st = lbm_check(h, &eu, &et);
-            if (steps_done) *steps_done = done;
-            if (errU) *errU = eu;
-            if (errT) *errT = et;
-            if (st) return st;
+    int st = lbm::first_collision(h);
+    if (st) return st;
+    if ((st = lbm::run_begin(h, eps, 0.0, 0))) return st;
+    const int64_t itc0 = h->itc;
+    const int cur0 = h->cur;
+    int64_t launched = 0;
+    int periods = 0;
+    RunCtl c{};
+    c.active = 1;
+    c.errU = c.errT = 100.0;
+    while (launched < max_steps) {
+        const int64_t to_check = check_every - (h->itc % check_every);
+        const int64_t k = std::min<int64_t>(to_check, max_steps - launched);
+        if (k == to_check && k == check_every && h->use_graphs && !h->resident && k >= 2) {
+            cudaGraphExec_t g;
+            if ((st = period_graph(h, h->cur, (int)k, &g))) break;
+            cudaError_t e = cudaGraphLaunch(g, h->stream);
+            if (e != cudaSuccess) {
+                st = fail(LBM_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
+                break;
+            }
+            lbm::g_launches += k + 2;
+            h->cur = (int)((h->cur + k) & 1);
+            h->itc += k;
+        } else {
+            if ((st = lbm_step(h, (int32_t)k))) break;
+            if (k == to_check) {
+                cudaError_t e = run_check(h->geo, h->bufs, (int)k, h->stream);
+                if (e != cudaSuccess) {
+                    st = fail(LBM_ERR_CUDA, "run check: %s", cudaGetErrorString(e));
+                    break;
+                }
+            }
+        }
+        launched += k;
+        if (k == to_check && ++periods % kRunPeriodsPerRead == 0) {
+            if ((st = lbm::run_read(h, &c))) break;
+            if (!c.active) break;
         }
     }
-    if (steps_done) *steps_done = done;
-    if (errU) *errU = eu;
-    if (errT) *errT = et;
-    return lbm::sync_handle(h);
+    int st2 = lbm::run_read(h, &c);
+    if (!st) st = st2;
+    // iterations that ran: up to the stopping check, or all that were queued
+    const int64_t ran = c.active ? launched : c.steps;
+    h->itc = itc0 + ran;
+    h->cur = (int)((cur0 + ran) & 1);
+    st2 = lbm::run_end(h);
+    if (!st) st = st2;
+    if (steps_done) *steps_done = ran;
+    if (errU) *errU = c.errU;
+    if (errT) *errT = c.errT;
+    if (!st && c.status == -2) st = fail(LBM_ERR_NONFINITE, "check: non-finite residual sum");
+    return st;
 }
+
 extern "C" int lbm_itc(const lbm_handle *h, int64_t *itc)
 {
     if (!h || !itc) return fail(LBM_ERR_PARAM, "NULL argument");
@@ -982,6 +1230,25 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         h->l2promo = (int)value;
         h->march_ok = encode_maps(h);
         return resolve_path(h);
+    case LBM_OPT_TILEY:
+        if (value != 0 && value != 4 && value != 8) return fail(LBM_ERR_PARAM, "tile rows must be 0, 4 or 8");
+        CU(cudaStreamSynchronize(h->stream));
+        h->tiley_opt = (int)value;
+        h->tiley = value ? (int)value : kDefaultTileY;
+        h->march_ok = encode_maps(h);
+        return resolve_path(h);
+    case LBM_OPT_PLAN:
+        if (value != 0 && value != 1) return fail(LBM_ERR_PARAM, "plan must be 0 or 1");
+        CU(cudaStreamSynchronize(h->stream));
+        h->plan_opt = (int)value;
+        return resolve_path(h);
+    case LBM_OPT_WAIT_LIMIT:
+        if (value < 0) return fail(LBM_ERR_PARAM, "wait limit must be >= 0");
+        CU(cudaStreamSynchronize(h->stream));
+        CU(fast::set_wait_limit(value));
+        CU(exact::set_wait_limit(value));
+        h->wait_limit = value;
+        return LBM_OK;
     default:
         return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
@@ -996,6 +1263,9 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     case LBM_OPT_L2PROMO: *value = h->l2promo; return LBM_OK;
     case LBM_OPT_GRAPHS: *value = h->use_graphs; return LBM_OK;
     case LBM_OPT_RESIDENT: *value = h->resident > 0; return LBM_OK;
+    case LBM_OPT_TILEY: *value = h->geo.dim == 3 ? h->tiley : 0; return LBM_OK;
+    case LBM_OPT_PLAN: *value = h->plan_opt; return LBM_OK;
+    case LBM_OPT_WAIT_LIMIT: *value = h->wait_limit; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

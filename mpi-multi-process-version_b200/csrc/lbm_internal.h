@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace lbm {
 
 // Geometry and physics constants a kernel needs, passed by value.
@@ -42,6 +44,26 @@ __host__ __device__ inline double tc_value(const Geo &G, int m)
 }
 
 
+// Device-side state of a run to a stop criterion (lbm_run, lbm_batch_run):
+// the check kernels write it after every check, and while `active` is 0 the
+// step and check kernels of the cavity do nothing, so graph replays queued
+// past the stop cost only their launch.  Outside runs active = 1.
+struct RunCtl {
+    int active;        // 1: keep stepping
+    int status;        // 0 running, 1 criterion met, -1 residual stopped being finite or grew (growth),
+                       // -2 non-finite residual sums (the check's own error)
+    int checks;        // checks done in this run
+    int pad0_;
+    long long steps;   // iterations up to the last check of this run
+    double errU, errT; // residuals of the last check
+    double best;       // smallest max(errU, errT) of this run
+    double eps;        // stop when errU <= eps and errT <= eps
+    double growth;     // > 0: stop (status -1) when max(errU, errT) > growth x best after 2 checks
+    int stop_bad;      // batch rule: a residual that is not finite, or grew (growth), stops the
+                       // member with status -1; non-finite sums give -1 with growth > 0, else -2
+    int pad1_;
+};
+
 // Device buffers of one cavity.
 struct Bufs {
     void *pop[2];          // ping-pong population buffers, (Q+QT) planes each
@@ -51,6 +73,7 @@ struct Bufs {
     double *partials;      // reduction partials
     double *scal;          // reduction results
     int *err;              // device error flag (bounded waits that gave up)
+    RunCtl *ctl;           // run state; the step kernels return at once while ctl->active is 0
 };
 
 // TMA descriptors of one population buffer (one per box class) and of the
@@ -60,12 +83,12 @@ struct alignas(64) TmapSet {
     CUtensorMap fmap;
 };
 
-// Per-cavity tables of a batch of 2D cavities (device memory)
+// Per-cavity tables of a batch of cavities (device memory)
 struct BatchDev {
     const Geo *geo;          // [ncav]
     const TmapSet *maps;     // [ncav][2]: descriptors of pop[0], pop[1] (+ their force arrays)
     const Bufs *bufs;        // [ncav]
-    const int4 *segs;        // all segments: (cavity, i0, ja, jb)
+    const int4 *segs;        // all segments: 2D (cavity, i0, ja, jb); 3D (tile, z0, z1, cavity)
     const int *seg_off;      // [nblocks + 1]
 };
 
@@ -108,16 +131,23 @@ constexpr float kF16InvScale = 1.0f / 4096.0f;
     /* stream + walls + macro only: pre-collision populations into pop_out, macro fields */  \
     cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in,    \
                             void *pop_out, const Bufs &b, cudaStream_t s);                    \
-    /* fused step through the TMA-fed persistent march kernel */                              \
+    /* fused step through the TMA-fed persistent march kernel; 3D: tile rows ty (4 or 8)  */ \
+    /* and the blocks' segment lists segs[segoff[b] .. segoff[b+1]) (device memory)        */ \
     cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in,          \
                       void *pop_out, void *F_out, const Bufs &b, int write_macro, int nblocks,\
-                      cudaStream_t s);                                                        \
+                      int ty, const int4 *segs, const int *segoff, cudaStream_t s);           \
     /* resident blocks per SM of the march kernel (0 if it cannot launch) */                  \
-    int march_blocks_per_sm(const Geo &g, int store);                                         \
+    int march_blocks_per_sm(const Geo &g, int store, int ty);                                 \
     /* one step of every cavity of a 2D batch (tile width TX = 32, 64 or 128) */              \
     cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur,       \
                             int write_macro, int *err, cudaStream_t s);                       \
     int march_batch_blocks_per_sm(int store, int TX);                                         \
+    /* one step of every cavity of a 3D batch (segments: tile, z0, z1, cavity; 32x8 tiles) */ \
+    cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur,             \
+                              int write_macro, int *err, cudaStream_t s);                     \
+    int march_batch3d_blocks_per_sm(int store);                                               \
+    /* limit of the march kernels' per-step waits on this device, in clock cycles */          \
+    cudaError_t set_wait_limit(long long cycles);                                             \
     }
 
 LBM_DECLARE_LAUNCHERS(fast)
@@ -127,6 +157,12 @@ LBM_DECLARE_LAUNCHERS(exact)
 cudaError_t reduce_check(const Geo &g, const Bufs &b, cudaStream_t s);      // scal[0..3]
 cudaError_t reduce_nusselt(const Geo &g, const Bufs &b, cudaStream_t s);    // scal[4..6]
 cudaError_t reduce_sums(const Geo &g, const Bufs &b, cudaStream_t s);       // scal[7..8]
+// check() of a run: the same sums as reduce_check, then the stop test on the
+// device (b.ctl); does nothing while b.ctl->active is 0.  period: iterations
+// since the previous check
+cudaError_t run_check(const Geo &g, const Bufs &b, int period, cudaStream_t s);
+// the same for the batch members idx[0..n-1] (tables of D), in one pair of launches
+cudaError_t run_check_batch(const BatchDev &D, const int *idx, int n, int period, cudaStream_t s);
 // AoS (Fortran f(0:Q-1,nodes)) <-> SoA planes, for FP64/FP32/FP16S storage
 cudaError_t aos_to_planes(const Geo &g, int store, int q0, int nq, const double *aos,
                           void *pop, cudaStream_t s);
@@ -142,7 +178,16 @@ extern int64_t g_launches;  // kernels launched by this library
 int set_error(int code, const char *fmt, ...);
 
 // tile shape of the march kernels (identical in both arithmetic modes); tx
-// selects the tile width of the 2D kernels (0: the single-cavity default)
-MarchShape march_shape(int dim, int store, int tx = 0);
+// selects the tile width of the 2D kernels (0: the single-cavity default),
+// ty the tile rows of the 3D kernel (4 or 8; 0: 8)
+MarchShape march_shape(int dim, int store, int tx = 0, int ty = 0);
+
+// Work plan of the 3D march kernel: for `nblocks` persistent blocks over
+// `ntiles` tile columns of nz slices, the segments (tile, z0, z1, 0) of each
+// block, block b owning segs[off[b] .. off[b+1]).  kind 0: balanced z-lockstep
+// (every tile column in equal chunks run side by side, the blocks left over
+// take the chunks' last slices in lockstep rounds); 1: contiguous equal
+// shares of the (tile-major, slice-minor) items.  Returns the blocks used.
+int plan_march3d(int ntiles, int nz, int nblocks, int kind, std::vector<int4> &segs, std::vector<int> &off);
 
 }  // namespace lbm

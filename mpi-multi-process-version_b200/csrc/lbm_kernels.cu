@@ -336,6 +336,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
          int write_macro)
 {
+    if (!B.ctl->active) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     if (i >= G.nx || j >= G.ny) return;
@@ -386,6 +387,7 @@ k_steps2d_resident(const Geo G, typename Tr<ST>::S *p0, typename Tr<ST>::S *p1, 
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
+    if (!B.ctl->active) return;
     const int64_t nn = (int64_t)G.nx * G.ny;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int s = 0; s < nsteps; ++s) {
@@ -773,6 +775,7 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
+    if (!B.ctl->active) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
     const int k = blockIdx.z;
@@ -1197,71 +1200,105 @@ cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out, 
 #undef CALL
 }
 
-template <int ST>
-static cudaError_t prepare_march(const Geo &g)
+template <int ST, int TY>
+static cudaError_t prepare_march3d()
 {
-    static bool done3 = false, done2 = false;
-    if (g.dim == 3 && !done3) {
-        cudaError_t e = cudaFuncSetAttribute(k_march3d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             L3<ST>::smem());
+    static bool done = false;
+    if (!done) {
+        cudaError_t e = cudaFuncSetAttribute(k_march3d<ST, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L3<ST, TY>::smem());
         if (e != cudaSuccess) return e;
-        done3 = true;
-    }
-    if (g.dim == 2 && !done2) {
-        cudaError_t e = cudaFuncSetAttribute(k_march2d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             L2<ST>::smem());
-        if (e != cudaSuccess) return e;
-        done2 = true;
+        done = true;
     }
     return cudaSuccess;
 }
 
 template <int ST>
-static int mbps(const Geo &g)
+static cudaError_t prepare_march2d()
 {
-    if (prepare_march<ST>(g) != cudaSuccess) return 0;
-    int n = 0;
-    cudaError_t e = g.dim == 3
-                        ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d<ST>, L3<ST>::NT, L3<ST>::smem())
-                        : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2<ST>::NT, L2<ST>::smem());
-    return e == cudaSuccess ? n : 0;
+    static bool done = false;
+    if (!done) {
+        cudaError_t e = cudaFuncSetAttribute(k_march2d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L2<ST>::smem());
+        if (e != cudaSuccess) return e;
+        done = true;
+    }
+    return cudaSuccess;
 }
 
-int march_blocks_per_sm(const Geo &g, int store)
+template <int ST, int TY>
+static int mbps3(void)
 {
-#define CALL(ST) mbps<ST>(g)
+    if (prepare_march3d<ST, TY>() != cudaSuccess) return 0;
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d<ST, TY>, L3<ST, TY>::NT,
+                                                         L3<ST, TY>::smem()) == cudaSuccess
+               ? n
+               : 0;
+}
+
+template <int ST>
+static int mbps(const Geo &g, int ty)
+{
+    if (g.dim == 3) return ty == 4 ? mbps3<ST, 4>() : mbps3<ST, 8>();
+    if (prepare_march2d<ST>() != cudaSuccess) return 0;
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2<ST>::NT, L2<ST>::smem()) ==
+                   cudaSuccess
+               ? n
+               : 0;
+}
+
+int march_blocks_per_sm(const Geo &g, int store, int ty)
+{
+#define CALL(ST) mbps<ST>(g, ty)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }
 
-template <int ST>
-static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
-                                const Bufs &b, int wm, int nblocks, cudaStream_t s)
+template <int ST, int TY>
+static cudaError_t launch_march3d(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
+                                  const Bufs &b, int wm, const int4 *segs, const int *segoff, int nblocks,
+                                  cudaStream_t s)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    cudaError_t e = prepare_march<ST>(g);
+    cudaError_t e = prepare_march3d<ST, TY>();
     if (e != cudaSuccess) return e;
-    if (g.dim == 3) {
-        using L = L3<ST>;
-        const int64_t ntiles = (int64_t)((g.nx + L::TX - 1) / L::TX) * ((g.ny + L::TY - 1) / L::TY);
-        const int64_t total = ntiles * g.nz;
-        const int nb = int(nblocks < total ? nblocks : total);
-        k_march3d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
-    } else {
-        using L = L2<ST>;
-        const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
-        const int nb = int(nblocks < total ? nblocks : total);
-        k_march2d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
-    }
-    ++g_launches;
+    k_march3d<ST, TY><<<nblocks, L3<ST, TY>::NT, L3<ST, TY>::smem(), s>>>(m, g, (const C *)Fin, (S *)pout,
+                                                                        (C *)Fout, b, wm, segs, segoff, b.err);
     return cudaGetLastError();
 }
 
-cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in, void *pop_out, void *F_out,
-                  const Bufs &b, int write_macro, int nblocks, cudaStream_t s)
+template <int ST>
+static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
+                                const Bufs &b, int wm, int nblocks, int ty, const int4 *segs, const int *segoff,
+                                cudaStream_t s)
 {
-#define CALL(ST) launch_march<ST>(g, src, F_in, pop_out, F_out, b, write_macro, nblocks, s)
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    cudaError_t e;
+    if (g.dim == 3) {
+        e = ty == 4 ? launch_march3d<ST, 4>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, s)
+                    : launch_march3d<ST, 8>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, s);
+    } else {
+        using L = L2<ST>;
+        e = prepare_march2d<ST>();
+        if (e != cudaSuccess) return e;
+        const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
+        const int nb = int(nblocks < total ? nblocks : total);
+        k_march2d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
+        e = cudaGetLastError();
+    }
+    ++g_launches;
+    return e;
+}
+
+cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in, void *pop_out, void *F_out,
+                  const Bufs &b, int write_macro, int nblocks, int ty, const int4 *segs, const int *segoff,
+                  cudaStream_t s)
+{
+#define CALL(ST) launch_march<ST>(g, src, F_in, pop_out, F_out, b, write_macro, nblocks, ty, segs, segoff, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }
@@ -1337,26 +1374,89 @@ int march_batch_blocks_per_sm(int store, int TX)
 #undef CALL
 }
 
+template <int ST>
+static cudaError_t prepare_batch3d()
+{
+    static bool done = false;
+    if (!done) {
+        cudaError_t e = cudaFuncSetAttribute(k_march3d_batch<ST, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L3<ST, 8>::smem());
+        if (e != cudaSuccess) return e;
+        done = true;
+    }
+    return cudaSuccess;
+}
+
+template <int ST>
+static cudaError_t launch_batch3d(const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+{
+    cudaError_t e = prepare_batch3d<ST>();
+    if (e != cudaSuccess) return e;
+    k_march3d_batch<ST, 8><<<nblocks, L3<ST, 8>::NT, L3<ST, 8>::smem(), s>>>(D, cur, wm, err);
+    ++g_launches;
+    return cudaGetLastError();
+}
+
+template <int ST>
+static int batch3d_bps()
+{
+    if (prepare_batch3d<ST>() != cudaSuccess) return 0;
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d_batch<ST, 8>, L3<ST, 8>::NT,
+                                                         L3<ST, 8>::smem()) == cudaSuccess
+               ? n
+               : 0;
+}
+
+cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur, int write_macro, int *err,
+                          cudaStream_t s)
+{
+#define CALL(ST) launch_batch3d<ST>(D, nblocks, cur, write_macro, err, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+int march_batch3d_blocks_per_sm(int store)
+{
+#define CALL(ST) batch3d_bps<ST>()
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+cudaError_t set_wait_limit(long long cycles)
+{
+    if (cycles <= 0) cycles = kWaitCycles;
+    return cudaMemcpyToSymbol(g_wait_limit, &cycles, sizeof cycles);
+}
+
 }  // namespace LBM_NS
 
 #if !LBM_EXACT
 // tile shapes of the march kernels, for the host's tensor-map encoding
-MarchShape march_shape(int dim, int store, int tx)
+MarchShape march_shape(int dim, int store, int tx, int ty)
 {
     MarchShape m{};
     auto fill = [&](auto layout, int dims) {
         using L = decltype(layout);
         m.TX = L::TX;
-        m.TY = dims == 3 ? fast::L3<kF64>::TY : 1;
+        m.TY = dims == 3 ? (ty == 4 ? 4 : 8) : 1;
         m.HX = L::HX;
         m.threads = L::NT;
         m.smem = L::smem();
     };
     if (dim == 3) {
-        switch (store) {
-        case kF64: fill(fast::L3<kF64>{}, 3); break;
-        case kF32: fill(fast::L3<kF32>{}, 3); break;
-        default: fill(fast::L3<kF16S>{}, 3); break;
+        if (ty == 4) {
+            switch (store) {
+            case kF64: fill(fast::L3<kF64, 4>{}, 3); break;
+            case kF32: fill(fast::L3<kF32, 4>{}, 3); break;
+            default: fill(fast::L3<kF16S, 4>{}, 3); break;
+            }
+        } else {
+            switch (store) {
+            case kF64: fill(fast::L3<kF64, 8>{}, 3); break;
+            case kF32: fill(fast::L3<kF32, 8>{}, 3); break;
+            default: fill(fast::L3<kF16S, 8>{}, 3); break;
+            }
         }
         for (int c = 0; c < 4; ++c) {
             m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);

@@ -6,9 +6,12 @@
 //
 // Scheme (3D; 2D is the same one dimension down):
 //   * the domain is cut into cross-section tiles of TX x TY nodes (x, y); a
-//     work item is a tile at one z-slice, and each persistent CTA takes a
-//     contiguous, equal share of the (tile-major, z-minor) work items, so it
-//     marches along z through at most a few tile columns;
+//     work item is a tile at one z-slice.  In 3D each persistent CTA runs a
+//     host-made list of segments (tile, first slice, end slice) and marches
+//     along z through each; the host plans the lists so that neighbouring
+//     tiles are at the same slice at the same time (their shared halo rows
+//     then come from L2) while every SM has an equal share; in 2D each CTA
+//     takes a contiguous, equal share of the (strip-major, row-minor) items;
 //   * for every slice the CTA fetches one TMA box per population plane into
 //     shared memory: a box covers the tile plus the in-plane halo the plane's
 //     interpolation stencil needs (x +-HX columns, y +-1 rows);
@@ -21,12 +24,16 @@
 //     computes its node from shared memory and stores the new post-collision
 //     populations straight to global memory; a __syncthreads ends each step
 //     and frees the slots the next copies reuse;
-//   * every wait is bounded (kWaitCycles): on timeout the kernel records an
-//     error code in *err, stops issuing, lets outstanding copies drain (also
-//     bounded) and returns; the host reports LBM_ERR_TIMEOUT.
+//   * every wait is bounded: a step's waits by g_wait_limit (kWaitCycles
+//     unless LBM_OPT_WAIT_LIMIT sets it), the final drain by kWaitCycles.  On
+//     timeout the kernel records an error code in *err, stops issuing, lets
+//     outstanding copies drain and returns; the host reports LBM_ERR_TIMEOUT.
 // No copy uses cluster multicast; every copy reads this GPU's own buffers.
 
 static constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+// limit of a step's waits, in clock cycles (set_wait_limit)
+__device__ long long g_wait_limit = kWaitCycles;
 
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -53,13 +60,13 @@ __device__ __forceinline__ uint32_t mbar_test(uint64_t *b, uint32_t parity)
     return ok;
 }
 
-// bounded wait for the phase of parity `parity`; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity)
+// bounded wait for the phase of parity `parity`; false after `limit` cycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, long long limit = kWaitCycles)
 {
     if (mbar_test(b, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_test(b, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -119,12 +126,12 @@ __device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k ==
 // 3D layout
 // ---------------------------------------------------------------------------
 // box classes: 0 tile only, 1 +-HX columns, 2 +-1 rows, 3 both
-template <int ST>
+template <int ST, int TY_ = 8>
 struct L3 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
-    static constexpr int TX = 32, TY = 8, NT = TX * TY;
+    static constexpr int TX = 32, TY = TY_, NT = TX * TY;
     static constexpr int HX = 16 / ES;
     __host__ __device__ static constexpr int bx(int c) { return TX + ((c & 1) ? 2 * HX : 0); }
     __host__ __device__ static constexpr int by(int c) { return TY + ((c & 2) ? 2 : 0); }
@@ -181,17 +188,20 @@ struct L3 {
 };
 
 // ---------------------------------------------------------------------------
-// 3D march kernel
+// 3D march
 // ---------------------------------------------------------------------------
-template <int ST>
-__global__ void __launch_bounds__(256, 1)
-k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
-          typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
-          int write_macro, int64_t total, int *err)
+// TY: tile rows (8: 256 threads, one CTA per SM in FP64; 4: 128 threads, two
+// CTAs per SM).  A block runs segments segs[sbeg .. send), each (tile, first
+// slice, end slice, cavity); tiles are numbered x-fastest within a cavity.
+// `cavity(c, G, maps, dst, Fout, B)` yields cavity c's geometry, the TMA
+// descriptors of the buffer read this step, the outputs and the buffers.
+template <int ST, int TY_, class CavFn>
+__device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int sbeg, int send, CavFn cavity,
+                                            int write_macro, int *err)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    using L = L3<ST>;
+    using L = L3<ST, TY_>;
     constexpr int TX = L::TX, TY = L::TY, HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
@@ -201,8 +211,6 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    const int nz = G.nz;
-    const int ntx = (G.nx + TX - 1) / TX;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&zbar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
@@ -213,6 +221,8 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 
     uint32_t znext = 0, nnext = 0;  // per-slot parity of the next copy
     int i0 = 0, j0 = 0;
+    const Geo *Gp = nullptr;       // the current segment's cavity
+    const TmapSet *Mp = nullptr;
 
     auto issue_z = [&](int s) {
         const int slot = s & 3;
@@ -223,7 +233,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 #pragma unroll
             for (int zi = 0; zi < 12; ++zi) {
                 const int c = L::zc(zi);
-                tma_load4(base + L::zoff(zi), &maps.m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
+                tma_load4(base + L::zoff(zi), &Mp->m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
                           s, L::zq(zi));
             }
         }
@@ -238,28 +248,35 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 #pragma unroll
             for (int ni = 0; ni < 14; ++ni) {
                 const int c = L::nc(ni);
-                tma_load4(base + L::noff(ni), &maps.m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
+                tma_load4(base + L::noff(ni), &Mp->m[c], bar, i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0),
                           s, L::nq(ni));
             }
-            tma_load3(base + L::fo(), &maps.fmap, bar, i0, j0, s);
-            bulk_load(base + L::wo(), G.wgt[2] + (int64_t)s * 6, 48, bar);
+            tma_load3(base + L::fo(), &Mp->fmap, bar, i0, j0, s);
+            bulk_load(base + L::wo(), Gp->wgt[2] + (int64_t)s * 6, 48, bar);
         }
         nnext ^= 1u << slot;
     };
-    auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u); };
-    auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
+    const long long wlim = g_wait_limit;
+    auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u, wlim); };
+    auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
-    const int64_t G_ = gridDim.x;
-    const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
-    const int64_t P = G.plane;
     bool aborted = false;
 
-    for (int64_t u = ubeg; u < uend && !aborted;) {
-        const int64_t t = u / nz;
-        const int ka = int(u % nz);
-        const int kb = int(ka + ((uend - u) < (nz - ka) ? (uend - u) : (nz - ka)));
-        i0 = int(t % ntx) * TX;
-        j0 = int(t / ntx) * TY;
+    for (int si = sbeg; si < send && !aborted; ++si) {
+        const int4 sg = segs[si];
+        S *dst;
+        C *Fout;
+        const Bufs *Bp;
+        cavity(sg.w, Gp, Mp, dst, Fout, Bp);
+        if (!Bp->ctl->active) continue;  // a batch member whose run has stopped
+        const Geo &G = *Gp;
+        const Bufs &B = *Bp;
+        const int nz = G.nz;
+        const int ntx = (G.nx + TX - 1) / TX;
+        const int64_t P = G.plane;
+        const int t = sg.x, ka = sg.y, kb = sg.z;
+        i0 = (t % ntx) * TX;
+        j0 = (t / ntx) * TY;
         // the segment's z-slices: the first step's needs, then one slice per step
         const int pre_lo = need_lo(ka, nz), pre_hi = need_hi(ka, nz);
         const int seg_hi = need_hi(kb - 1, nz) > pre_hi ? need_hi(kb - 1, nz) : pre_hi;
@@ -419,13 +436,51 @@ k_march3d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
                 break;
             }
         }
-        u += kb - ka;
     }
     if (aborted && tid == 0) {
         // let copies still in flight land before the CTA's shared memory is released
         for (int s = 0; s < 4; ++s) mbar_wait(&zbar[s], ((znext >> s) & 1u) ^ 1u);
         for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
     }
+}
+
+template <int ST, int TY_>
+__global__ void __launch_bounds__(32 * TY_, TY_ == 8 ? 1 : 2)
+k_march3d(const __grid_constant__ TmapSet maps, const __grid_constant__ Geo G,
+          const typename Tr<ST>::C *__restrict__ Fin, typename Tr<ST>::S *__restrict__ dst,
+          typename Tr<ST>::C *__restrict__ Fout, const __grid_constant__ Bufs B, int write_macro,
+          const int4 *__restrict__ segs, const int *__restrict__ seg_off, int *err)
+{
+    (void)Fin;
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    if (!B.ctl->active) return;
+    auto cavity = [&](int, const Geo *&Gp, const TmapSet *&Mp, S *&d, C *&Fo, const Bufs *&Bp) {
+        Gp = &G;
+        Mp = &maps;
+        d = dst;
+        Fo = Fout;
+        Bp = &B;
+    };
+    march3d_run<ST, TY_>(segs, seg_off[blockIdx.x], seg_off[blockIdx.x + 1], cavity, write_macro, err);
+}
+
+// many 3D cavities: segments (tile, z0, z1, cavity) of the batch's work list;
+// `cur` is the ping-pong buffer holding the populations read this step
+template <int ST, int TY_>
+__global__ void __launch_bounds__(32 * TY_, TY_ == 8 ? 1 : 2)
+k_march3d_batch(const BatchDev D, int cur, int write_macro, int *err)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    auto cavity = [&](int c, const Geo *&Gp, const TmapSet *&Mp, S *&d, C *&Fo, const Bufs *&Bp) {
+        Gp = &D.geo[c];
+        Mp = &D.maps[(int64_t)c * 2 + cur];
+        Bp = &D.bufs[c];
+        d = (S *)D.bufs[c].pop[1 - cur];
+        Fo = (C *)D.bufs[c].F[1 - cur];
+    };
+    march3d_run<ST, TY_>(D.segs, D.seg_off[blockIdx.x], D.seg_off[blockIdx.x + 1], cavity, write_macro, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -616,6 +671,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
 
     uint32_t ynext = 0, nnext = 0;
     bool aborted = false;
+    const long long wlim = g_wait_limit;
     for (int k = 0; k < nseg && !aborted; ++k) {
         int cav, i0, ja, jb;
         seg(k, cav, i0, ja, jb);
@@ -625,6 +681,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         C *Fout;
         const Bufs *Bp;
         cavity(cav, Gp, maps, dst, Fout, Bp);
+        if (!Bp->ctl->active) continue;  // a batch member whose run has stopped
         const Geo &G = *Gp;
         const int ny = G.ny;
 
@@ -658,8 +715,10 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             }
             nnext ^= 1u << slot;
         };
-        auto wait_y = [&](int s) -> bool { return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u); };
-        auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u); };
+        auto wait_y = [&](int s) -> bool {
+            return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u, wlim);
+        };
+        auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
         const int pre_lo = need_lo(ja, ny), pre_hi = need_hi(ja, ny);
         const int seg_hi = need_hi(jb - 1, ny) > pre_hi ? need_hi(jb - 1, ny) : pre_hi;
@@ -714,6 +773,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     constexpr int TX = L2<ST, 128>::TX;
+    if (!B.ctl->active) return;
     const int ny = G.ny;
     const int64_t G_ = gridDim.x;
     const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;

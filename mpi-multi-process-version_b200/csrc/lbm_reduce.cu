@@ -56,12 +56,12 @@ __global__ void k_final(const double *__restrict__ partials, int nb, double *__r
 }
 
 // check(): 2M:755-805 / 3M:1027-1082.  sums of |du|^2, |u|^2, dT^2, T^2, then
-// the previous fields take the current ones.
-__global__ void __launch_bounds__(kRedThreads) k_check(const Geo G, const Bufs B)
+// the previous fields take the current ones.  Block `blk` of kRedBlocks.
+__device__ __forceinline__ void check_block(const Geo &G, const Bufs &B, int blk)
 {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < G.nnode; n += stride) {
+    const int64_t stride = (int64_t)kRedBlocks * blockDim.x;
+    for (int64_t n = (int64_t)blk * blockDim.x + threadIdx.x; n < G.nnode; n += stride) {
         const double u = B.u[n], v = B.v[n], T = B.T[n];
         const double du = u - B.up[n], dv = v - B.vp[n], dT = T - B.Tp[n];
         if (G.dim == 2) {
@@ -80,13 +80,122 @@ __global__ void __launch_bounds__(kRedThreads) k_check(const Geo G, const Bufs B
         B.vp[n] = v;
         B.Tp[n] = T;
     }
-    block_reduce_store<4>(acc, B.partials + (int64_t)blockIdx.x * 4);
+    block_reduce_store<4>(acc, B.partials + (int64_t)blk * 4);
 }
+
+__global__ void __launch_bounds__(kRedThreads) k_check(const Geo G, const Bufs B) { check_block(G, B, blockIdx.x); }
 
 cudaError_t reduce_check(const Geo &g, const Bufs &b, cudaStream_t s)
 {
     k_check<<<kRedBlocks, kRedThreads, 0, s>>>(g, b);
     k_final<4><<<1, kRedThreads, 0, s>>>(b.partials, kRedBlocks, b.scal + 0);
+    g_launches += 2;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// the stop test of a run on the device (lbm_run, lbm_batch_run)
+// ---------------------------------------------------------------------------
+// The sums are those of k_check / k_final (same blocks, same order), so the
+// residuals are bit-identical to lbm_check's; errorU = sqrt(sum du^2) /
+// sqrt(sum u^2), errorT likewise (2M:784, 798), and the loop continues while
+// errorU > eps or errorT > eps (2M:307).
+__device__ void run_decide(RunCtl *c, const double *sum, int period)
+{
+    const double eu = sqrt(sum[0]) / sqrt(sum[1]), et = sqrt(sum[2]) / sqrt(sum[3]);
+    c->errU = eu;
+    c->errT = et;
+    c->steps += period;
+    const bool sums_finite = isfinite(sum[0]) && isfinite(sum[1]) && isfinite(sum[2]) && isfinite(sum[3]);
+    if (!c->stop_bad) {
+        // single cavity (lbm_run): non-finite sums end the run as an error
+        if (!sums_finite) {
+            c->status = -2;
+            c->active = 0;
+        } else if (!(eu > c->eps || et > c->eps)) {
+            c->status = 1;
+            c->active = 0;
+        }
+        ++c->checks;
+        return;
+    }
+    // batch member: a residual that stops being finite, or grows past growth x
+    // its smallest value in this run, stops the member (status -1)
+    const double r = eu < et ? et : eu;
+    const bool bad = !sums_finite || !isfinite(r) || (c->growth > 0.0 && c->checks >= 2 && r > c->growth * c->best);
+    if (!sums_finite && !(c->growth > 0.0)) {
+        c->status = -2;
+        c->active = 0;
+        return;
+    }
+    ++c->checks;
+    c->best = r < c->best ? r : c->best;
+    if (bad) {
+        c->status = -1;
+        c->active = 0;
+    } else if (!(eu > c->eps || et > c->eps)) {
+        c->status = 1;
+        c->active = 0;
+    }
+}
+
+// the final sum of k_final<4>, then the decision, by one block
+__device__ __forceinline__ void run_final_block(const Bufs &B, int period)
+{
+    __shared__ double sum[4];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < kRedBlocks; b += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[c] += B.partials[(int64_t)b * 4 + c];
+    block_reduce_store<4>(acc, sum);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 4; ++c) B.scal[c] = sum[c];
+        run_decide(B.ctl, sum, period);
+    }
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_run_check(const Geo G, const Bufs B)
+{
+    if (!B.ctl->active) return;
+    check_block(G, B, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_run_final(const Bufs B, int period)
+{
+    if (!B.ctl->active) return;
+    run_final_block(B, period);
+}
+
+cudaError_t run_check(const Geo &g, const Bufs &b, int period, cudaStream_t s)
+{
+    k_run_check<<<kRedBlocks, kRedThreads, 0, s>>>(g, b);
+    k_run_final<<<1, kRedThreads, 0, s>>>(b, period);
+    g_launches += 2;
+    return cudaGetLastError();
+}
+
+// batch: blockIdx.y (check) / blockIdx.x (final) picks the member idx[...]
+__global__ void __launch_bounds__(kRedThreads) k_run_check_batch(const BatchDev D, const int *idx)
+{
+    const int m = idx[blockIdx.y];
+    const Bufs &B = D.bufs[m];
+    if (!B.ctl->active) return;
+    check_block(D.geo[m], B, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(kRedThreads) k_run_final_batch(const BatchDev D, const int *idx, int period)
+{
+    const Bufs &B = D.bufs[idx[blockIdx.x]];
+    if (!B.ctl->active) return;
+    run_final_block(B, period);
+}
+
+cudaError_t run_check_batch(const BatchDev &D, const int *idx, int n, int period, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_run_check_batch<<<dim3(kRedBlocks, n), kRedThreads, 0, s>>>(D, idx);
+    k_run_final_batch<<<n, kRedThreads, 0, s>>>(D, idx, period);
     g_launches += 2;
     return cudaGetLastError();
 }

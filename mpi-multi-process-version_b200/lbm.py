@@ -32,13 +32,14 @@ EXPORTS = [
     "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_init_warm", "lbm_step", "lbm_run", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
-    "lbm_set_option", "lbm_get_option", "lbm_check_noalloc",
+    "lbm_set_option", "lbm_get_option", "lbm_check_noalloc", "lbm_march_plan3d",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_size", "lbm_batch_cavity", "lbm_batch_init_reference",
     "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_run_masked", "lbm_batch_tune",
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
+OPT_TILEY, OPT_PLAN, OPT_WAIT_LIMIT = 6, 7, 8
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 

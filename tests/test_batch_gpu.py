@@ -145,3 +145,102 @@ def test_batch_3d_members_match_standalone(pkg):
             assert np.array_equal(got[k], ref[k]), k
         c.close()
     b.close()
+
+
+
+def test_sweep_members_against_oracle(pkg, ora):
+    # members of the benchmark's seeded 256-cavity sweep (smallest to largest,
+    # aspect up to 4) advanced together by the persistent batch kernel in fast
+    # mode, each against the oracle: populations <= 1e-12 relative, Nu <= 1e-10
+    specs = pkg.sweep_specs(256, seed=0)
+    order = sorted(range(len(specs)), key=lambda i: specs[i]["nx"] * specs[i]["ny"])
+    pick = sorted({order[0], order[1], order[len(order) // 4], order[len(order) // 2], order[3 * len(order) // 4],
+                   max(range(len(specs)), key=lambda i: specs[i]["aspect"]), order[-2], order[-1]})
+    sel = [specs[i] for i in pick]
+    assert max(sp["aspect"] for sp in sel) > 3.5 and max(sp["nx"] for sp in sel) == 512
+    steps = 300
+    b = pkg.Batch(2, sel, mode="fast")
+    assert b.get_option("persistent") == 1
+    b.initial()
+    b.step(steps)
+    for m, sp in zip(b.members, sel):
+        c = sp["coords"]
+        o = ora.Oracle(2, sp["nx"], sp["ny"], 1, x=c.x, y=c.y, dt=c.dt, length_LB=c.length_LB, Ra=sp["Ra"],
+                       Pr=sp["Pr"])
+        o.step(steps)
+        f, g = m.populations()
+        for got, ref in ((f, o.pops("f")), (g, o.pops("g"))):
+            assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+        for a, r in zip(m.nusselt(), o.nusselt()):
+            assert abs(a - r) <= 1e-10 * abs(r)
+    b.close()
+
+
+@pytest.mark.parametrize("dim,growth", [(2, 0), (2, 100), (3, 0)])
+def test_batch_run_matches_host_loop(pkg, dim, growth):
+    # the device-side stop test of lbm_batch_run against each member run alone
+    # with the reference's loop on the host: the same iterations, the same
+    # stop, the same fields (exact mode, bit for bit)
+    if dim == 2:
+        specs = [dict(nx=32, ny=32, Ra=1e3, Pr=0.71, grid="tanh", stretch=1.5),
+                 dict(nx=48, ny=40, Ra=1e4, Pr=2.0, grid="tanh", stretch=1.2),
+                 dict(nx=40, ny=64, Ra=3e4, Pr=0.71, grid="tanh", stretch=1.7),
+                 dict(nx=64, ny=64, Ra=1e5, Pr=7.0, grid="tanh", stretch=1.0)]
+        for sp in specs:
+            sp["coords"] = pkg.mesh_box(sp["nx"], sp["ny"], 0, 1.0, sp["ny"] / sp["nx"], 1.0, sp["grid"],
+                                        sp["stretch"])
+    else:
+        specs = [dict(nx=16, ny=16, nz=12, Ra=1e4, Pr=0.71, grid="tanh", stretch=1.5),
+                 dict(nx=20, ny=12, nz=10, Ra=1e3, Pr=2.0, grid="tanh", stretch=1.2)]
+    ce, eps, max_steps = 150, 3e-2, 4500
+    b = pkg.Batch(dim, specs, mode="exact")
+    b.set_option("growth", growth)
+    b.initial()
+    status, steps = b.run_masked(None, max_steps, ce, eps)
+    assert (status == 1).any()
+    for m, sp, st, n in zip(b.members, specs, status, steps):
+        c = pkg.Cavity(dim, sp["nx"], sp["ny"], sp.get("nz", 1), Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"],
+                       stretch=sp["stretch"], mode="exact", coords=m.mesh)
+        c.initial()
+        done, ref = 0, (100.0, 100.0)
+        while done < max_steps:
+            c.step(ce)
+            done += ce
+            ref = c.check()
+            if not (ref[0] > eps or ref[1] > eps):
+                break
+        conv = not (ref[0] > eps or ref[1] > eps)
+        assert n == done and st == (1 if conv else 0)
+        assert m.itc == done
+        got, want = m.macro(), c.macro()
+        for k in want:
+            assert np.array_equal(got[k], want[k]), k
+        c.close()
+    b.close()
+
+
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_batch_3d_persistent_matches_standalone(pkg, persistent):
+    # 3D members of different sizes in one persistent kernel (or one launch
+    # each) evolve bit for bit as each cavity alone
+    specs = [dict(nx=40, ny=24, nz=18, Ra=1e5, Pr=0.71, grid="tanh", stretch=1.5),
+             dict(nx=33, ny=16, nz=12, Ra=1e4, Pr=2.0, grid="erf", stretch=3.2),
+             dict(nx=64, ny=32, nz=20, Ra=3e5, Pr=0.71, grid="tanh", stretch=1.2)]
+    b = pkg.Batch(3, specs, mode="exact")
+    b.set_option("persistent", persistent)
+    b.initial()
+    b.step(9)
+    b.step(4)
+    for m, sp in zip(b.members, specs):
+        c = pkg.Cavity(3, sp["nx"], sp["ny"], sp["nz"], Ra=sp["Ra"], Pr=sp["Pr"], grid=sp["grid"],
+                       stretch=sp["stretch"], mode="exact", coords=m.mesh, kernel="direct")
+        c.initial()
+        c.step(13)
+        ref, got = c.macro(), m.macro()
+        for k in ref:
+            assert np.array_equal(got[k], ref[k]), k
+        c.close()
+    if persistent:
+        r = b.tune(steps=4)
+        assert r["tile"] == 32 and r["nblocks"] > 0
+    b.close()

@@ -13,8 +13,12 @@ for) and every shared-memory element index the stencils touch, and checks:
   * the persistent CTAs cover every (tile, slice) work item exactly once.
 """
 import itertools
+import os
+import sys
 
 import pytest
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 
 def off_a(i, n):
@@ -33,21 +37,54 @@ def need_hi(k, n):
     return 2 if k == 0 else (k if k == n - 1 else k + 1)
 
 
-def replay(n, total, grid, nodes_of_unit, check_node):
-    """Replay the march schedule along an axis of n slices for `grid` CTAs.
-    The in-plane indices of a node do not depend on the step, so each tile's
-    nodes are checked once, at every step kind (first, inner, last slice)."""
-    covered = [0] * total
-    checked = set()
+def contiguous_plan(n, total, grid):
+    """Per CTA, its segments (tile, first slice, end slice): an equal
+    contiguous share of the (tile-major, slice-minor) items, split at tile
+    boundaries (the 2D march kernel's own split)."""
+    plan = []
     for b in range(grid):
-        ubeg, uend = total * b // grid, total * (b + 1) // grid
-        slot = {}  # ring slot -> slice currently held
-        nslot = {}
-        inflight = set()
-        u = ubeg
+        u, uend = total * b // grid, total * (b + 1) // grid
+        segs = []
         while u < uend:
             t, ka = divmod(u, n)
             kb = ka + min(uend - u, n - ka)
+            segs.append((t, ka, kb))
+            u += kb - ka
+        plan.append(segs)
+    return plan
+
+
+def library_plan(ntiles, nz, grid, kind):
+    """The 3D march kernel's work plan as the library makes it (host code,
+    no GPU needed)."""
+    import ctypes
+    from __graft_entry__ import load_package
+    lib = load_package().lib()
+    i32 = ctypes.c_int32
+    fn = lib.lbm_march_plan3d
+    fn.argtypes = [i32, i32, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32),
+                   ctypes.POINTER(i32)]
+    cnt, used = i32(0), i32(0)
+    assert fn(ntiles, nz, grid, kind, ctypes.byref(cnt), None, None, ctypes.byref(used)) == 0
+    segs = (i32 * (3 * cnt.value))()
+    off = (i32 * (used.value + 1))()
+    assert fn(ntiles, nz, grid, kind, ctypes.byref(cnt), segs, off, ctypes.byref(used)) == 0
+    return [[tuple(segs[3 * i:3 * i + 3]) for i in range(off[b], off[b + 1])] for b in range(used.value)]
+
+
+def replay(n, total, plan, nodes_of_unit, check_node):
+    """Replay the march schedule along an axis of n slices for the CTAs of
+    `plan` (per CTA, its segments).  The in-plane indices of a node do not
+    depend on the step, so each tile's nodes are checked once, at every step
+    kind (first, inner, last slice)."""
+    covered = [0] * total
+    checked = set()
+    for segs in plan:
+        slot = {}  # ring slot -> slice currently held
+        nslot = {}
+        inflight = set()
+        for t, ka, kb in segs:
+            assert 0 <= ka < kb <= n
             pre_lo, pre_hi = need_lo(ka, n), need_hi(ka, n)
             seg_hi = max(need_hi(kb - 1, n), pre_hi)
 
@@ -84,15 +121,14 @@ def replay(n, total, grid, nodes_of_unit, check_node):
                         check_node(node, k)
                 covered[t * n + k] += 1
             assert not inflight, ("copies left in flight", inflight)
-            u += kb - ka
     assert all(c == 1 for c in covered)
 
 
-# 3D: tiles of 32 x 8 (x, y), boxes with +-HX columns and +-1 rows
-TX3, TY3 = 32, 8
+# 3D: tiles of 32 x TY3 (x, y), TY3 = 8 or 4, boxes with +-HX columns and +-1 rows
+TX3 = 32
 
 
-def check_3d(nx, ny, nz, grid, es):
+def check_3d(nx, ny, nz, grid, es, TY3=8, kind=0):
     HX = 16 // es
     bx = lambda c: TX3 + (2 * HX if c & 1 else 0)  # noqa: E731
     by = lambda c: TY3 + (2 if c & 2 else 0)  # noqa: E731
@@ -131,7 +167,7 @@ def check_3d(nx, ny, nz, grid, es):
         for s in (k + off_a(k, nz), k, k + off_b(k, nz)):
             assert need_lo(k, nz) <= s <= need_hi(k, nz)
 
-    replay(nz, ntiles * nz, grid, nodes, check_node)
+    replay(nz, ntiles * nz, library_plan(ntiles, nz, grid, kind), nodes, check_node)
 
 
 def check_2d(nx, ny, grid, es, TX=128):
@@ -160,19 +196,38 @@ def check_2d(nx, ny, grid, es, TX=128):
         for s in (j + off_a(j, ny), j, j + off_b(j, ny)):
             assert need_lo(j, ny) <= s <= need_hi(j, ny)
 
-    replay(ny, ntx * ny, grid, nodes, check_node)
+    replay(ny, ntx * ny, contiguous_plan(ny, ntx * ny, grid), nodes, check_node)
 
 
-@pytest.mark.parametrize("shape", [(128, 128, 128), (20, 16, 16), (33, 18, 7), (64, 24, 3), (40, 10, 5), (16, 16, 16)])
-@pytest.mark.parametrize("es", [8, 4, 2])
-def test_march3d_schedule_and_indices(shape, es):
+@pytest.mark.parametrize("shape", [(128, 128, 128), (20, 16, 16), (33, 18, 7), (64, 24, 3), (40, 10, 5), (16, 16, 16),
+                                   (96, 64, 40)])
+@pytest.mark.parametrize("es", [8, 2])
+@pytest.mark.parametrize("ty", [8, 4])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_march3d_schedule_and_indices(shape, es, ty, kind):
     nx, ny, nz = shape
-    assert ny % TY3 != 1  # the host routes such shapes to the direct-load kernel
-    ntiles = -(-nx // TX3) * -(-ny // TY3)
+    if ny % ty == 1:
+        pytest.skip("the host routes such shapes to the direct-load kernel")
+    ntiles = -(-nx // TX3) * -(-ny // ty)
     total = ntiles * nz
-    for grid in sorted({1, 2, 3, 7, 148, min(296, total), total}):
+    for grid in sorted({1, 3, 7, 128, 148, 256, 296, total}):
         if grid <= total:
-            check_3d(nx, ny, nz, grid, es)
+            check_3d(nx, ny, nz, grid, es, ty, kind)
+
+
+@pytest.mark.parametrize("ntiles,nz,grid", [(64, 128, 148), (128, 128, 296), (64, 128, 128), (16, 100, 148),
+                                            (64, 256, 148)])
+def test_march3d_plan_balances_the_sms(ntiles, nz, grid):
+    # the balanced plan keeps every SM busy: the busiest block's work (slices
+    # plus 1.5 slice times per segment start) is within 10 % of the even
+    # share, and a grid that is a multiple of the tile count is pure lockstep
+    plan = library_plan(ntiles, nz, grid, 0)
+    assert len(plan) <= grid
+    cost = [sum(kb - ka + 1.5 for _, ka, kb in segs) for segs in plan]
+    ideal = ntiles * nz / grid + 1.5
+    assert max(cost) <= 1.10 * ideal, (max(cost), ideal)
+    if grid % ntiles == 0:
+        assert len(plan) == grid and all(len(s) == 1 for s in plan)
 
 
 @pytest.mark.parametrize("shape", [(2048, 64), (128, 128), (130, 9), (48, 48), (300, 3), (40, 24)])

@@ -307,6 +307,50 @@ def test_run_matches_manual_loop(pkg):
     b.close()
 
 
+@pytest.mark.parametrize("dim,shape,ce,eps,max_steps,pre", [
+    (2, (40, 40, 1), 200, 2e-2, 20000, 0),
+    (2, (40, 40, 1), 137, 2e-2, 20000, 55),    # odd period; the first period is partial
+    (2, (48, 40, 1), 200, 1e-12, 1500, 0),     # never met: max_steps is not a multiple of the period
+    (2, (96, 80, 1), 300, 3e-2, 30000, 0),     # the TMA march kernel
+    (3, (20, 16, 12), 100, 5e-2, 6000, 10),
+], ids=["2d", "2d-odd-offset", "2d-cap", "2d-march", "3d"])
+def test_device_stop_test_matches_host_loop(pkg, dim, shape, ce, eps, max_steps, pre):
+    # lbm_run tests the criterion on the device and reads its state once every
+    # few checks; iterations, residuals, counter and state equal the
+    # reference's loop driven from the host (2M:307-330: step, check every
+    # check_every iterations, stop when errorU and errorT are at most eps)
+    kern = "march" if shape[0] >= 96 else "auto"
+    a = pkg.Cavity(dim, *shape, Ra=1e4, grid="tanh", stretch=1.5, mode="exact", kernel=kern)
+    b = pkg.Cavity(dim, *shape, Ra=1e4, grid="tanh", stretch=1.5, mode="exact", kernel=kern)
+    for c in (a, b):
+        c.initial()
+        if pre:
+            c.step(pre)
+            c.check()
+    steps, eu, et = a.run(max_steps=max_steps, check_every=ce, eps=eps)
+    done, ref = 0, (100.0, 100.0)
+    while (ref[0] > eps or ref[1] > eps) and done < max_steps:
+        k = min(ce - b.itc % ce, max_steps - done)
+        b.step(k)
+        done += k
+        if b.itc % ce == 0:
+            ref = b.check()
+    assert steps == done and (eu, et) == ref
+    assert a.itc == b.itc == pre + done
+    ma, mb = a.macro(), b.macro()
+    for k in ma:
+        assert np.array_equal(ma[k], mb[k]), k
+    fa, ga = a.populations()
+    fb, gb = b.populations()
+    assert np.array_equal(fa, fb) and np.array_equal(ga, gb)
+    # stepping after the run continues from the same state
+    a.step(3)
+    b.step(3)
+    assert np.array_equal(a.macro()["u"], b.macro()["u"])
+    a.close()
+    b.close()
+
+
 def _smooth_fields(shape, dim, seed):
     # smooth random fields: products of low-order sines in the node index
     rng = np.random.default_rng(seed)
@@ -405,4 +449,91 @@ def test_resident_path_matches_oracle_in_exact_mode(pkg, ora):
     o.step(200)
     f, g = cav.populations()
     assert np.array_equal(f, o.pops("f")) and np.array_equal(g, o.pops("g"))
+    cav.close()
+
+
+
+# ---------------------------------------------------------------------------
+# the drop-in tolerance at the benchmark configurations, through the kernels
+# and grids the benchmark times
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", [
+    # 2D differentially heated square cavity, 128^2, tanh 1.5, Ra 1e4 (both step kernels)
+    dict(dim=2, n=(128, 128, 1), Ra=1e4, kernel="direct", steps=1000),
+    dict(dim=2, n=(128, 128, 1), Ra=1e4, kernel="march", steps=1000),
+    # 3D cubic cavity, 128^3, tanh 1.5, Ra 1e5: the TMA march kernel on its default
+    # persistent grid and work plan, as the benchmark runs it
+    dict(dim=3, n=(128, 128, 128), Ra=1e5, kernel="auto", steps=1000),
+], ids=["C1-direct", "C1-march", "C2-march"])
+def test_benchmark_config_within_drop_in_tolerance(pkg, ora, case):
+    # populations <= 1e-12 relative after 1000 steps, Nu_avg <= 1e-10 (the
+    # reference's loop body natural-convection_3dim_mono.f90:373-396 repeated)
+    cav, o = pair(pkg, ora, case["dim"], *case["n"], grid="tanh", stretch=1.5, Ra=case["Ra"], mode="fast",
+                  kernel=case["kernel"])
+    if case["dim"] == 3:
+        assert cav.kernel == "march"
+        assert cav.get_option(pkg.lbm.OPT_PLAN) == 0
+    cav.step(case["steps"])
+    o.step(case["steps"])
+    f, g = cav.populations()
+    assert rel_err(f, o.pops("f")) <= 1e-12
+    assert rel_err(g, o.pops("g")) <= 1e-12
+    for a, b in zip(cav.nusselt(), o.nusselt()):
+        assert abs(a - b) <= 1e-10 * abs(b)
+    fscale = np.abs(o.pops("f")).max()
+    m = cav.macro()
+    for k in (FIELDS2 if case["dim"] == 2 else FIELDS3):
+        assert np.abs(m[k] - o.field(k)).max() <= 1e-12 * fscale, k
+    cav.close()
+
+
+@pytest.mark.parametrize("ty,plan,nblocks", [(8, 0, 0), (4, 0, 0), (8, 1, 0), (4, 1, 0), (8, 0, 37), (4, 0, 300)])
+def test_march3d_tiles_and_plans_bit_identical(pkg, ora, ty, plan, nblocks):
+    # every tile shape and work plan of the 3D march kernel gives the oracle's
+    # populations bit for bit (exact mode), on a domain with partial tiles
+    cav, o = pair(pkg, ora, 3, 72, 30, 24, grid="tanh", stretch=1.5, Ra=1e5, mode="exact", kernel="march")
+    cav.set_option(pkg.lbm.OPT_TILEY, ty)
+    cav.set_option(pkg.lbm.OPT_PLAN, plan)
+    if nblocks:
+        cav.set_option(pkg.lbm.OPT_NBLOCKS, nblocks)
+    assert cav.get_option(pkg.lbm.OPT_TILEY) == ty and cav.kernel == "march"
+    cav.step(9)
+    o.step(9)
+    f, g = cav.populations()
+    assert np.array_equal(f, o.pops("f")) and np.array_equal(g, o.pops("g"))
+    m = cav.macro()
+    for k in FIELDS3:
+        assert np.array_equal(m[k], o.field(k)), k
+    cav.close()
+
+
+@pytest.mark.parametrize("dim,shape", [(3, (64, 24, 16)), (2, (256, 48, 1))])
+def test_wait_timeout_is_reported_and_recoverable(pkg, dim, shape):
+    # the march kernels bound every wait for their TMA copies; a limit that
+    # runs out makes the step report LBM_ERR_TIMEOUT (the kernel stops issuing,
+    # drains its copies and returns), and the context stays usable: with the
+    # limit restored a re-initialised run is bit-identical to an untouched one
+    def run(c, n):
+        c.initial()
+        c.step(n)
+        return c.populations()
+
+    ref = pkg.Cavity(dim, *shape, grid="tanh", stretch=1.5, mode="exact", kernel="march")
+    f0, g0 = run(ref, 6)
+    ref.close()
+    cav = pkg.Cavity(dim, *shape, grid="tanh", stretch=1.5, mode="exact", kernel="march")
+    cav.initial()
+    cav.set_option(pkg.lbm.OPT_WAIT_LIMIT, 1)
+    try:
+        assert cav.get_option(pkg.lbm.OPT_WAIT_LIMIT) == 1
+        with pytest.raises(pkg.LBMError) as e:
+            cav.step(4)
+            cav.synchronize()
+        assert e.value.status == -5
+        assert "bounded wait" in str(e.value)
+    finally:
+        cav.set_option(pkg.lbm.OPT_WAIT_LIMIT, 0)
+    cav.synchronize()  # the flag was cleared when it was reported
+    f, g = run(cav, 6)
+    assert np.array_equal(f, f0) and np.array_equal(g, g0)
     cav.close()

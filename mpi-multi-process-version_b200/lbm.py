@@ -554,33 +554,40 @@ def fortran_e(v: float, w: int, d: int) -> str:
     return s.rjust(w)
 
 
-def output_ascii(cav: Cavity, path: str):
-    """Tecplot POINT file in the reference's format: output_ASCII
+def write_tecplot(path: str, x, y, z, fields):
+    """Tecplot POINT file in the reference's format, output_ASCII
     (2M:818-843: X Y U V T rho; 3M:1097-1121: X Y Z U V W RHO T), Fortran
-    formats (1x,2(e11.4,' '),10(e13.6,' '))."""
-    m = cav.macro()
-    x, y = cav.mesh.x, cav.mesh.y
-
+    formats (1x,2(e11.4,' '),10(e13.6,' ')) and the ZONE line of format 101.
+    x, y (, z): node coordinates c(0:n+1) with the walls; fields: arrays of
+    shape (ny, nx) or (nz, ny, nx) (keys rho, u, v, [w,] T); z None in 2D."""
     e = fortran_e
+    u = fields["u"]
     with open(path, "w") as fh:
-        if cav.dim == 2:
+        if z is None:
+            ny, nx = u.shape
             fh.write(' TITLE="thermal convective flows"\n')
             fh.write(' VARIABLES="X" "Y" "U" "V" "T" "rho"\n')
-            fh.write(f"ZONE I= {cav.nx:5d}  J= {cav.ny:5d} F=POINT\n")
-            for j in range(cav.ny):
-                for i in range(cav.nx):
-                    vals = [m["u"][j, i], m["v"][j, i], m["T"][j, i], m["rho"][j, i]]
+            fh.write(f"ZONE I= {nx:5d}  J= {ny:5d} F=POINT\n")
+            for j in range(ny):
+                for i in range(nx):
+                    vals = [fields["u"][j, i], fields["v"][j, i], fields["T"][j, i], fields["rho"][j, i]]
                     fh.write(" " + e(x[i + 1], 11, 4) + " " + e(y[j + 1], 11, 4) + " "
                              + " ".join(e(v, 13, 6) for v in vals) + " \n")
         else:
-            z = cav.mesh.z
+            nz, ny, nx = u.shape
             fh.write(' TITLE="side-heated convection "\n')
             fh.write(' VARIABLES="X" "Y" "Z" "U" "V" "W" "RHO" "T" \n')
-            fh.write(f"ZONE I= {cav.nx:5d}  J= {cav.ny:5d} K= {cav.nz:5d} F=POINT\n")
-            for k in range(cav.nz):
-                for j in range(cav.ny):
-                    for i in range(cav.nx):
-                        vals = [z[k + 1], m["u"][k, j, i], m["v"][k, j, i], m["w"][k, j, i],
-                                m["rho"][k, j, i], m["T"][k, j, i]]
+            fh.write(f"ZONE I= {nx:5d}  J= {ny:5d} K= {nz:5d} F=POINT\n")
+            for k in range(nz):
+                for j in range(ny):
+                    for i in range(nx):
+                        vals = [z[k + 1], fields["u"][k, j, i], fields["v"][k, j, i], fields["w"][k, j, i],
+                                fields["rho"][k, j, i], fields["T"][k, j, i]]
                         fh.write(" " + e(x[i + 1], 11, 4) + " " + e(y[j + 1], 11, 4) + " "
                                  + " ".join(e(v, 13, 6) for v in vals) + " \n")
+
+
+def output_ascii(cav: Cavity, path: str):
+    """The cavity's macroscopic fields (gathered from the GPU) as the
+    reference's Tecplot file (write_tecplot)."""
+    write_tecplot(path, cav.mesh.x, cav.mesh.y, cav.mesh.z if cav.dim == 3 else None, cav.macro())

@@ -10,7 +10,10 @@ scalars and arrays with explicit lower bounds, allocatable and automatic
 arrays, `data` statements, `parameter`s, do / do while / if chains, array
 element, section and whole-array assignment, array constructors, the
 intrinsics dble, sqrt, dsqrt, erf, mod, abs, min, max, and the MPI routines
-they call.  Output statements (write, open, close, format) and character
+they call.  Output statements are dropped, except, with `with_output`, the
+formatted writes to numbered units (open / write with a format label or
+list-directed / format statements), which render through f90fmt.py into
+S._io[unit] -- the reference's Tecplot writer output_ASCII; character
 variables are dropped.
 
 Arithmetic follows gfortran -O2 on x86-64: IEEE double, operands evaluated
@@ -271,8 +274,23 @@ def logical_lines(text):
         s = buf + s
         buf = ""
         if s.strip():
-            out.append(s.strip().lower())
+            out.append(_lower_outside_quotes(s.strip()))
     return out
+
+
+def _lower_outside_quotes(s):
+    out, inq = [], None
+    for ch in s:
+        if inq:
+            out.append(ch)
+            if ch == inq:
+                inq = None
+        elif ch in "'\"":
+            inq = ch
+            out.append(ch)
+        else:
+            out.append(ch.lower())
+    return "".join(out)
 
 
 TOKEN = re.compile(r"""
@@ -407,9 +425,16 @@ class Sym:
 
 
 def split_top(s, sep=","):
-    parts, depth, cur = [], 0, ""
+    parts, depth, cur, inq = [], 0, "", None
     for ch in s:
-        if ch in "(":
+        if inq:
+            cur += ch
+            if ch == inq:
+                inq = None
+            continue
+        if ch in "'\"":
+            inq = ch
+        elif ch in "(":
             depth += 1
         elif ch in ")":
             depth -= 1
@@ -433,7 +458,8 @@ class Unit:
 
 
 class Translator:
-    def __init__(self, src, overrides=None, check_every=None):
+    def __init__(self, src, overrides=None, check_every=None, with_output=False):
+        self.with_output = with_output
         self.lines = logical_lines(src)
         if check_every:
             self.lines = [ln.replace("mod(itc,2000)", f"mod(itc,{int(check_every)})") for ln in self.lines]
@@ -701,6 +727,31 @@ class Translator:
             return [f"mpi.recv({r[1]}, {r[2]}, {E(1)}, {E(3)}, {E(4)})"]
         raise NotImplementedError(name)
 
+    # --- formatted output to numbered units (with_output)
+    def io_stmt(self, unit, ln):
+        """Python for an open / write / close on a numbered unit, None for
+        anything else (stdout, internal files, other statements)."""
+        m = re.match(r"^open\s*\((.*)\)$", ln)
+        if m:
+            mm = re.search(r"unit\s*=\s*(\d+)", m.group(1))
+            return f"fio_open(S, {int(mm.group(1))})" if mm else None
+        if re.match(r"^close\s*\(\s*\d+\s*\)$", ln) or re.match(r"^\d+\s+format", ln):
+            return "pass"
+        m = re.match(r"^write\s*\(\s*(\d+)\s*,\s*(\*|\d+)\s*\)\s*(.*)$", ln)
+        if not m:
+            return None
+        u, fmt, items = int(m.group(1)), m.group(2), split_top(m.group(3))
+        vals = []
+        for it in items:
+            if it[0] in "'\"":
+                vals.append(repr(it[1:-1]))
+            else:
+                vals.append(self.ex(unit, parse_expr(it)))
+        if fmt == "*":
+            return f"fio_write_list(S, {u}, [{', '.join(vals)}])"
+        text = unit.fmts[fmt]
+        return f"fio_write_fmt(S, {u}, {text!r}, [{', '.join(vals)}])"
+
     # --- array allocation code
     def bounds(self, unit, dims):
         out = []
@@ -719,6 +770,11 @@ class Translator:
         def emit(s):
             out.append(P + s)
 
+        if self.with_output:
+            io = self.io_stmt(unit, ln)
+            if io is not None:
+                emit(io)
+                return
         if re.match(r"^(write|open|close|print|deallocate)\b", ln) or re.match(r"^\d+\s+format", ln):
             emit("pass")
             return
@@ -743,7 +799,7 @@ class Translator:
                 for s in self.mpi_call(unit, name, args):
                     emit(s)
                 return
-            if name == "output_ascii":
+            if name == "output_ascii" and not self.with_output:
                 emit("pass")
                 return
             call = f"sub_{name}(S, mpi{''.join(', ' + self.ex(unit, parse_expr(a)) for a in args)})"
@@ -910,6 +966,11 @@ class Translator:
         out.append("    S._checks = []")
 
     def unit_code(self, unit, out):
+        unit.fmts = {}
+        for ln in unit.body:
+            m = re.match(r"^(\d+)\s+format\s*(\(.*\))$", ln)
+            if m:
+                unit.fmts[m.group(1)] = m.group(2)
         if unit.kind == "function":
             args = ", ".join(f"v_{a}" for a in unit.args)
             out.append(f"def fn_{unit.name}({args}):")
@@ -945,12 +1006,16 @@ class Translator:
         return "\n".join(out) + "\n"
 
 
-def run(src, nranks, overrides=None, check_every=None):
+def run(src, nranks, overrides=None, check_every=None, with_output=False):
     """Translate and run a reference program on nranks emulated ranks.
-    Returns the per-rank module states after the program ends."""
-    tr = Translator(src, overrides, check_every)
+    Returns the per-rank module states after the program ends (with_output:
+    each state's _io maps a unit number to the text written to it)."""
+    import f90fmt
+    tr = Translator(src, overrides, check_every, with_output)
     code = tr.python()
-    ns = {"math": math, "FArray": FArray, "Stop": Stop, "fmod": fmod, "idiv": idiv, "f32": f32}
+    ns = {"math": math, "FArray": FArray, "Stop": Stop, "fmod": fmod, "idiv": idiv, "f32": f32,
+          "fio_open": f90fmt.fio_open, "fio_write_list": f90fmt.fio_write_list,
+          "fio_write_fmt": f90fmt.fio_write_fmt}
     exec(compile(code, "<reference-translation>", "exec"), ns)  # noqa: S102
     world = World(nranks)
     states = [type("State", (), {})() for _ in range(nranks)]

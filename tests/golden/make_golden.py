@@ -8,7 +8,9 @@ programs).  Only compile-time parameters are patched: the grid size nx (ny, nz
 follow as in the source), itc_max, and the check interval MOD(itc,2000).  The
 fields the program holds at STOP (populations f, g of every rank, the
 macroscopic fields gathered on rank 0, the grid coordinates and the check()
-history) are written to ref_<program>.npz next to this script.
+history) are written to ref_<program>.npz next to this script; the slab
+programs also run their Tecplot writer output_ASCII, whose file is kept as
+ref_<program>_tecplot.dat.gz.
 
 Run here, where the reference is mounted:
 
@@ -20,6 +22,7 @@ reference at run time.
 from __future__ import annotations
 
 import argparse
+import gzip
 import os
 import sys
 import time
@@ -107,7 +110,14 @@ def main():
             continue
         src = open(os.path.join(args.reference, fname)).read()
         t0 = time.time()
-        states, code = f90py.run(src, ranks, over, every)
+        # the slab programs also run their Tecplot writer, output_ASCII
+        # (2dim_mono.f90:818-843, 3dim_mono.f90:1097-1121); rank 0 writes unit 2
+        mono = name.endswith("_mono")
+        states, code = f90py.run(src, ranks, over, every, with_output=mono)
+        if mono:
+            tec = os.path.join(HERE, f"ref_{name}_tecplot.dat.gz")
+            with open(tec, "wb") as fh, gzip.GzipFile(fileobj=fh, mode="wb", mtime=0, filename="") as gz:
+                gz.write("".join(states[0]._io[2]).encode())
         if args.dump_python:
             os.makedirs(args.dump_python, exist_ok=True)
             open(os.path.join(args.dump_python, name + ".py"), "w").write(code)

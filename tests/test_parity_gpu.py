@@ -537,3 +537,25 @@ def test_wait_timeout_is_reported_and_recoverable(pkg, dim, shape):
     f, g = run(cav, 6)
     assert np.array_equal(f, f0) and np.array_equal(g, g0)
     cav.close()
+
+
+@pytest.mark.parametrize("name", ["2dim_mono", "3dim_mono"])
+def test_output_ascii_matches_reference_writer(pkg, name, tmp_path):
+    # the GPU's fields (exact mode) written by output_ascii are byte for byte
+    # the Tecplot file the reference program's own output_ASCII wrote
+    import gzip
+    gold = _os.path.join(_os.path.dirname(_os.path.abspath(__file__)), "golden")
+    d = dict(np.load(_os.path.join(gold, f"ref_{name}.npz")))
+    dim = d["f"].ndim - 1
+    shape = d["f"].shape[:-1]
+    nz, ny, nx = (shape if dim == 3 else (1,) + shape)
+    m = pkg.Mesh(d["x"], d["y"], d.get("z"), 0.0, float(d["length_LB"]), float(d["dt"]))
+    cav = pkg.Cavity(dim, nx, ny, nz, Ra=float(d["Ra"]), Pr=float(d["Pr"]), Ma=float(d["Ma"]), coords=m,
+                     mode="exact")
+    cav.initial()
+    cav.step(int(d["itc"]))
+    path = str(tmp_path / "out.dat")
+    pkg.output_ascii(cav, path)
+    cav.close()
+    with gzip.open(_os.path.join(gold, f"ref_{name}_tecplot.dat.gz"), "rt") as fh:
+        assert open(path).read() == fh.read()

@@ -458,7 +458,7 @@ def run_steady(args, world, rank, local):
     r = W.solve(cases, init="warm", model=model, storage="mixed", max_steps=max_steps, device=local)
     launches = pkg.kernel_launches() - l0
     clocks = sampler.stop() if sampler else None
-    t_mixed = _reduce(r["seconds"] + r["predict_seconds"], world, "max")
+    t_mixed = _reduce(r["seconds"], world, "max")  # prediction and initialisation included
     t_cold = _reduce(t_cold, world, "max")
     got = pkg.sharding.gather_by_index(idx, {"steps_cold": steps_cold, "nu_cold": nu_cold, "steps_mixed": r["steps"],
                                              "nu_mixed": r["nu_hot"], "status": r["status"],

@@ -227,6 +227,13 @@ int lbm_set_populations(lbm_handle *h, const double *f, const double *g);
 int lbm_set_option(lbm_handle *h, int32_t option, int64_t value);
 int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *value);
 
+/* Convert the cavity's state to another population storage (LBM_STORE_*) in
+ * place, on the device: new buffers, the newest populations and carried
+ * force converted, the check history kept (a mixed-precision run switches
+ * from FP32 to FP64 this way).  Exact mode stays FP64; a batch member uses
+ * lbm_batch_set_storage.  No counterpart in the reference (FP64 throughout). */
+int lbm_set_storage(lbm_handle *h, int32_t storage);
+
 /* Wait for all work of the handle; reports LBM_ERR_TIMEOUT if a kernel's
  * bounded wait gave up since the last synchronisation. */
 int lbm_synchronize(lbm_handle *h);
@@ -257,6 +264,11 @@ typedef struct lbm_batch lbm_batch;
                                         exceeds this factor x its smallest one in the run and reports
                                         it as converged = -1 (0, the default: off, a non-finite
                                         residual ends the run with LBM_ERR_NONFINITE) */
+#define LBM_BATCH_OPT_STORAGES    6  /* the storages lbm_batch_tune may choose, as a mask of
+                                        1 << LBM_STORE_*: the caller's accuracy rule (FP32 and FP64 for
+                                        the transient of a run, FP64 alone to finish it); 0 (the
+                                        default): the batch's current storage only */
+#define LBM_BATCH_OPT_STORAGE     7  /* read only: the batch's current storage (LBM_STORE_*) */
 
 /* Create n cavities (same dim, storage, mode and device; any size and
  * parameters).  x[i], y[i], z[i] are the coordinate arrays of cavity i as for
@@ -290,9 +302,18 @@ int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double e
  * warm-start driver restarts those from the conduction state). */
 int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
                          double eps, int32_t *converged, int64_t *steps_done);
-/* Time each tile width and grid size on the batch itself (the timed steps
- * advance the members) and keep the fastest; reports the choice. */
+/* The autotuner: time each storage LBM_BATCH_OPT_STORAGES allows (the
+ * batch's state is converted in place, lbm_batch_set_storage) x each tile
+ * width and grid size on the batch itself (the timed steps advance the
+ * members) and keep the fastest; reports the tile, grid and rate
+ * (lbm_batch_get_option(LBM_BATCH_OPT_STORAGE) the storage).  No counterpart
+ * in the reference. */
 int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups);
+/* Convert every member's state to another population storage in place, on
+ * the device (new buffers; the newest populations and carried force
+ * converted; the check history kept).  Exact mode stays FP64.  No
+ * counterpart in the reference (FP64 throughout). */
+int lbm_batch_set_storage(lbm_batch *b, int32_t storage);
 int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value);
 int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t *value);
 int lbm_batch_synchronize(lbm_batch *b);

@@ -55,6 +55,7 @@ struct lbm_batch {
     bool march_ok = true;          // every member can run in the persistent kernel (3D: tile rows fit)
     int use_graphs = 1;
     double growth = 0.0;           // residual growth factor that stops a member in lbm_batch_run (0: off)
+    int storages = 0;              // LBM_BATCH_OPT_STORAGES: storages lbm_batch_tune may pick (0: the current)
     Geo *d_geo = nullptr;
     TmapSet *d_maps = nullptr;
     Bufs *d_bufs = nullptr;
@@ -621,9 +622,70 @@ extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_ever
     return lbm_batch_run_masked(b, nullptr, max_steps, check_every, eps, converged, steps_done);
 }
 
+extern "C" int lbm_batch_set_storage(lbm_batch *b, int32_t storage)
+{
+    if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    if (storage == b->storage) return LBM_OK;
+    BCU(cudaSetDevice(b->device));
+    BCU(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);
+    for (int i = 0; i < b->n; ++i) {
+        int st = change_storage(b->cav[i], storage);
+        if (st) return st;
+    }
+    b->storage = storage;
+    std::vector<Bufs> bufs(b->n);
+    for (int i = 0; i < b->n; ++i) bufs[i] = b->cav[i]->bufs;
+    BCU(cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * b->n, cudaMemcpyHostToDevice));
+    b->dirty = true;
+    return LBM_OK;
+}
+
+static int tune_storage(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups);
+
+// The autotuner: every storage the caller's accuracy rule allows
+// (LBM_BATCH_OPT_STORAGES; the current one if none is set) x tile width x
+// grid size, timed on the batch itself; the batch keeps the fastest.
 extern "C" int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    const int mask = b->storages ? b->storages : (1 << b->storage);
+    const int user_nb = b->nblocks_opt;  // a grid the caller set stays
+    double best = -1.0;
+    int best_store = b->storage, best_tile = 0, best_nb = 0;
+    // the current storage first, so a single-storage rule converts nothing
+    int order[3] = {b->storage, -1, -1}, no = 1;
+    for (int s = 0; s < 3; ++s)
+        if (s != b->storage && (mask >> s) & 1) order[no++] = s;
+    for (int k = 0; k < no; ++k) {
+        if (!((mask >> order[k]) & 1)) continue;
+        int st = lbm_batch_set_storage(b, order[k]);
+        if (st) return st;
+        int t = 0, nb = 0;
+        double v = 0.0;
+        b->nblocks_opt = user_nb;
+        if ((st = tune_storage(b, steps, &t, &nb, &v))) return st;
+        if (v > best) {
+            best = v;
+            best_store = order[k];
+            best_tile = t;
+            best_nb = nb;
+        }
+    }
+    int st = lbm_batch_set_storage(b, best_store);
+    if (st) return st;
+    if (b->dim == 2) b->tile = b->tile_opt = best_tile;
+    b->nblocks_opt = user_nb > 0 ? user_nb : best_nb;
+    b->dirty = true;
+    if (tile) *tile = best_tile;
+    if (nblocks) *nblocks = best_nb;
+    if (mlups) *mlups = best;
+    return LBM_OK;
+}
+
+// tile width x grid size for the batch's current storage
+static int tune_storage(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
+{
     if (!b->persistent || !b->march_ok)
         return set_error(LBM_ERR_UNSUPPORTED, "lbm_batch_tune: the batch does not use the persistent kernel");
     if (steps < 2) steps = 2;
@@ -704,6 +766,12 @@ extern "C" int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value)
         if (value < 0) return set_error(LBM_ERR_PARAM, "growth factor must be >= 0");
         b->growth = (double)value;
         break;
+    case LBM_BATCH_OPT_STORAGES:
+        if (value < 0 || value > 7) return set_error(LBM_ERR_PARAM, "storage mask must be 0..7");
+        if (b->mode == LBM_MODE_EXACT && (value & ~1))
+            return set_error(LBM_ERR_UNSUPPORTED, "exact mode computes in FP64 storage only");
+        b->storages = (int)value;
+        break;
     default:
         return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
@@ -720,6 +788,8 @@ extern "C" int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t 
     case LBM_BATCH_OPT_PERSISTENT: *value = b->persistent; return LBM_OK;
     case LBM_BATCH_OPT_GRAPHS: *value = b->use_graphs; return LBM_OK;
     case LBM_BATCH_OPT_GROWTH: *value = (int64_t)b->growth; return LBM_OK;
+    case LBM_BATCH_OPT_STORAGES: *value = b->storages; return LBM_OK;
+    case LBM_BATCH_OPT_STORAGE: *value = b->storage; return LBM_OK;
     default: return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
 }

@@ -1191,6 +1191,72 @@ extern "C" int lbm_set_populations(lbm_handle *h, const double *f, const double 
     return LBM_OK;
 }
 
+// Convert the cavity's state to another population storage in place: new
+// buffers, the newest populations and carried force converted on the device,
+// old buffers released, descriptors and kernel choice redone.
+int lbm::change_storage(lbm_handle *h, int storage)
+{
+    if (storage == h->p.storage) return LBM_OK;
+    if (storage != LBM_STORE_F64 && storage != LBM_STORE_F32 && storage != LBM_STORE_F16S)
+        return fail(LBM_ERR_PARAM, "unknown storage %d", storage);
+    if (h->p.mode == LBM_MODE_EXACT && storage != LBM_STORE_F64)
+        return fail(LBM_ERR_UNSUPPORTED, "exact mode computes in FP64 storage only");
+    CU(cudaStreamSynchronize(h->stream));
+    const size_t es = storage == LBM_STORE_F64 ? 8 : (storage == LBM_STORE_F32 ? 4 : 2);
+    const size_t cs = storage == LBM_STORE_F64 ? 8 : 4;
+    const size_t popb = (size_t)(h->Q + h->QT) * (size_t)h->geo.plane * es;
+    const size_t fb = (size_t)h->geo.plane * cs;
+    void *np[2] = {nullptr, nullptr}, *nF[2] = {nullptr, nullptr};
+    int st = LBM_OK;
+    for (int i = 0; i < 2 && !st; ++i) {
+        st = dalloc(h, &np[i], popb);
+        if (!st) st = dalloc(h, &nF[i], fb);
+    }
+    if (!st && (cudaMemset(nF[0], 0, fb) != cudaSuccess || cudaMemset(nF[1], 0, fb) != cudaSuccess))
+        st = fail(LBM_ERR_CUDA, "memset failed");
+    if (!st && h->phase != 0) {
+        const int c = h->cur;
+        cudaError_t e = convert_state(h->geo, h->p.storage, storage, h->Q + h->QT, h->bufs.pop[c], np[c],
+                                      h->bufs.F[c], nF[c], h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) st = fail(LBM_ERR_CUDA, "storage conversion: %s", cudaGetErrorString(e));
+    }
+    if (st) {
+        for (int i = 0; i < 2; ++i) {
+            if (np[i]) cudaFree(np[i]);
+            if (nF[i]) cudaFree(nF[i]);
+        }
+        return st;
+    }
+    const size_t old_popb = (size_t)(h->Q + h->QT) * (size_t)h->geo.plane * h->esize;
+    const size_t old_fb = (size_t)h->geo.plane * h->csize;
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(h->bufs.pop[i]);
+        cudaFree(h->bufs.F[i]);
+        h->bufs.pop[i] = np[i];
+        h->bufs.F[i] = nF[i];
+    }
+    h->bytes -= (int64_t)(2 * (old_popb + old_fb));
+    if (h->staging) {  // sized for the old storage; ensure_staging makes a new one
+        cudaFree(h->staging);
+        h->staging = nullptr;
+        h->bytes -= (int64_t)old_popb;
+    }
+    h->p.storage = storage;
+    h->esize = es;
+    h->csize = cs;
+    lbm::drop_graphs(h);
+    h->march_ok = encode_maps(h);
+    return resolve_path(h);
+}
+
+extern "C" int lbm_set_storage(lbm_handle *h, int32_t storage)
+{
+    CHECK_H(h);
+    if (!h->owns_ctl) return fail(LBM_ERR_STATE, "a batch member changes storage with lbm_batch_set_storage");
+    return lbm::change_storage(h, storage);
+}
+
 extern "C" int lbm_synchronize(lbm_handle *h)
 {
     CHECK_H(h);

@@ -168,6 +168,9 @@ cudaError_t aos_to_planes(const Geo &g, int store, int q0, int nq, const double 
                           void *pop, cudaStream_t s);
 cudaError_t planes_to_aos(const Geo &g, int store, int q0, int nq, const void *pop,
                           double *aos, cudaStream_t s);
+// a state's populations (nq planes) and carried force in another storage
+cudaError_t convert_state(const Geo &g, int src_store, int dst_store, int nq, const void *pop_src, void *pop_dst,
+                          const void *F_src, void *F_dst, cudaStream_t s);
 // macro fields from populations (used by set_populations)
 cudaError_t macro_from_pops(const Geo &g, int store, const void *pop, const Bufs &b,
                             cudaStream_t s);

@@ -358,6 +358,58 @@ cudaError_t planes_to_aos(const Geo &g, int store, int q0, int nq, const void *p
     return cudaGetLastError();
 }
 
+// Populations of one storage converted to another on the device (the value
+// of a node's population is the same up to the target's rounding; deviation
+// forms are undone and redone through shift_of).
+template <int SRC, int DST>
+__global__ void k_convert_planes(const Geo G, int nq, const void *src, void *dst)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= G.nnode * nq) return;
+    const int64_t n = e / nq;
+    const int q = int(e % nq);
+    const int64_t a = (int64_t)q * G.plane + pidx(G, n);
+    double val;
+    if (SRC == kF64) val = ((const double *)src)[a];
+    else if (SRC == kF32) val = double(((const float *)src)[a]) + shift_of(G, q, n);
+    else val = double(__half2float(((const __half *)src)[a]) * kF16InvScale) + shift_of(G, q, n);
+    if (DST == kF64) ((double *)dst)[a] = val;
+    else if (DST == kF32) ((float *)dst)[a] = float(val - shift_of(G, q, n));
+    else ((__half *)dst)[a] = __float2half_rn(float(val - shift_of(G, q, n)) * kF16Scale);
+}
+
+template <int SRC>
+static void convert_from(const Geo &g, int dst_store, int nq, const void *src, void *dst, unsigned nb, cudaStream_t s)
+{
+    if (dst_store == kF64) k_convert_planes<SRC, kF64><<<nb, 256, 0, s>>>(g, nq, src, dst);
+    else if (dst_store == kF32) k_convert_planes<SRC, kF32><<<nb, 256, 0, s>>>(g, nq, src, dst);
+    else k_convert_planes<SRC, kF16S><<<nb, 256, 0, s>>>(g, nq, src, dst);
+}
+
+// the carried force, one compute-type value per cell of a plane
+__global__ void k_convert_force(int64_t n, int src8, int dst8, const void *src, void *dst)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double v = src8 ? ((const double *)src)[e] : double(((const float *)src)[e]);
+    if (dst8) ((double *)dst)[e] = v;
+    else ((float *)dst)[e] = float(v);
+}
+
+cudaError_t convert_state(const Geo &g, int src_store, int dst_store, int nq, const void *pop_src, void *pop_dst,
+                          const void *F_src, void *F_dst, cudaStream_t s)
+{
+    const int64_t n = g.nnode * nq;
+    const unsigned nb = unsigned((n + 255) / 256);
+    if (src_store == kF64) convert_from<kF64>(g, dst_store, nq, pop_src, pop_dst, nb, s);
+    else if (src_store == kF32) convert_from<kF32>(g, dst_store, nq, pop_src, pop_dst, nb, s);
+    else convert_from<kF16S>(g, dst_store, nq, pop_src, pop_dst, nb, s);
+    k_convert_force<<<unsigned((g.plane + 255) / 256), 256, 0, s>>>(g.plane, src_store == kF64, dst_store == kF64,
+                                                                    F_src, F_dst);
+    g_launches += 2;
+    return cudaGetLastError();
+}
+
 // macroscopic fields of loaded populations: rho = sum f, T = sum g, momentum
 // over rho, with half the buoyancy force gbeta*T*rho of this state added to
 // the gravity-axis velocity (v in 2D, w in 3D), as macro_u does (2M:734-735)

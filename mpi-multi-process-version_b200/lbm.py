@@ -32,12 +32,13 @@ EXPORTS = [
     "lbm_create", "lbm_destroy", "lbm_init_reference", "lbm_init_equilibrium", "lbm_init_warm", "lbm_step", "lbm_run", "lbm_itc",
     "lbm_check", "lbm_nusselt", "lbm_sums", "lbm_get_macro", "lbm_set_macro", "lbm_get_populations",
     "lbm_set_populations", "lbm_synchronize", "lbm_stream", "lbm_device_bytes", "lbm_kernel_launches",
-    "lbm_set_option", "lbm_get_option", "lbm_check_noalloc", "lbm_march_plan3d",
+    "lbm_set_option", "lbm_get_option", "lbm_check_noalloc", "lbm_march_plan3d", "lbm_set_storage",
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_size", "lbm_batch_cavity", "lbm_batch_init_reference",
     "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_run_masked", "lbm_batch_tune",
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
+    "lbm_batch_set_storage",
 ]
-BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5}
+BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5, "storages": 6, "storage": 7}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
 OPT_TILEY, OPT_PLAN, OPT_WAIT_LIMIT = 6, 7, 8
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
@@ -121,6 +122,8 @@ def lib():
         L.lbm_batch_get_option.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
         L.lbm_batch_synchronize.argtypes = [ctypes.c_void_p]
         L.lbm_batch_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_batch_set_storage.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.lbm_set_storage.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         _lib = L
     return _lib
 
@@ -350,6 +353,12 @@ class Cavity:
         assert f.size == self.nnode * self.Q and g.size == self.nnode * self.QT
         _chk(lib().lbm_set_populations(self.h, _p(f), _p(g)), "lbm_set_populations")
 
+    def set_storage(self, storage: str):
+        """lbm_set_storage: the state converted to another population storage
+        in place, on the device (e.g. FP32 -> FP64 to finish a run)."""
+        _chk(lib().lbm_set_storage(self.h, STORE[storage]), "lbm_set_storage")
+        self.storage = storage
+
     def synchronize(self):
         _chk(lib().lbm_synchronize(self.h), "lbm_synchronize")
 
@@ -475,11 +484,27 @@ class Batch:
              "lbm_batch_run_masked")
         return np.array(conv[:], dtype=np.int32), np.array(done[:], dtype=np.int64)
 
-    def tune(self, steps=20):
+    def tune(self, steps=20, storages=None):
+        """lbm_batch_tune; storages: the storages the tuner may pick (names),
+        None for the current one.  Returns the choice."""
+        if storages is not None:
+            self.set_option("storages", sum(1 << STORE[s] for s in storages))
         t, nb, v = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
         _chk(lib().lbm_batch_tune(self.h, int(steps), ctypes.byref(t), ctypes.byref(nb), ctypes.byref(v)),
              "lbm_batch_tune")
-        return {"tile": t.value, "nblocks": nb.value, "mlups": v.value}
+        self._sync_storage()
+        return {"tile": t.value, "nblocks": nb.value, "mlups": v.value, "storage": self.storage}
+
+    def set_storage(self, storage):
+        """lbm_batch_set_storage: every member's state in another storage, in place."""
+        _chk(lib().lbm_batch_set_storage(self.h, STORE[storage]), "lbm_batch_set_storage")
+        self._sync_storage()
+
+    def _sync_storage(self):
+        code = self.get_option("storage")
+        self.storage = {v: k for k, v in STORE.items()}[code]
+        for m in self.members:
+            m.storage = self.storage
 
     def set_option(self, name, value):
         _chk(lib().lbm_batch_set_option(self.h, BATCH_OPT[name], int(value)), "lbm_batch_set_option")

@@ -243,66 +243,93 @@ class WarmStart:
 # ---------------------------------------------------------------------------
 # solving to a steady state
 # ---------------------------------------------------------------------------
-def _prepare(cases, init, storage, model, predictions, device, growth):
+def _prepare(cases, storage, device, growth):
     specs = [{k: v for k, v in c.items()} for c in cases]
     b = L.Batch(2, specs, storage=storage, device=device)
-    t_pred = 0.0
+    b.set_option("growth", int(growth))
+    return b
+
+
+def _init(b, cases, init, model, predictions):
+    """Initial state of every member: the conduction state (cold) or the
+    model's prediction through lbm_init_warm.  Returns the prediction time."""
     if init == "cold":
         b.initial()
-    else:
-        t0 = time.perf_counter()
-        preds = predictions if predictions is not None else model.predict_fields(cases)
-        t_pred = time.perf_counter() - t0
-        for mem, f in zip(b.members, preds):
-            mem.init_warm(f["rho"], f["u"], f["v"], None, f["T"])
-    b.set_option("growth", int(growth))
-    b.synchronize()
-    return b, t_pred
+        return 0.0
+    t0 = time.perf_counter()
+    preds = predictions if predictions is not None else model.predict_fields(cases)
+    t_pred = time.perf_counter() - t0
+    for mem, f in zip(b.members, preds):
+        mem.init_warm(f["rho"], f["u"], f["v"], None, f["T"])
+    return t_pred
 
 
-def _run(b, eps, max_steps, check_every):
+def _run(b, eps, max_steps, check_every, mask=None):
     """lbm_batch_run_masked with the cold-start fallback for members stopped
-    for a diverging residual."""
-    status, steps = b.run_masked(None, max_steps, check_every, eps)
-    fallback = status == -1
+    for a diverging residual; max_steps is per member (an array or a number)."""
+    limit = np.broadcast_to(np.asarray(max_steps, dtype=np.int64), (b.n,)).copy()
+    on = np.ones(b.n, bool) if mask is None else np.asarray(mask, bool).copy()
+    status = np.zeros(b.n, np.int32)
+    steps = np.zeros(b.n, np.int64)
+    # all members run together up to the smallest remaining budget; those still
+    # running with budget left go on together, so no member exceeds its own
+    sel = on & (limit > 0)
+    while sel.any():
+        cap = int((limit - steps)[sel].min())
+        st, n = b.run_masked(None if sel.all() else sel, cap, check_every, eps)
+        status = np.where(sel, st, status)
+        steps = np.where(sel, steps + n, steps)
+        sel = sel & (st == 0) & (steps < limit)
+    fallback = on & (status == -1)
     if fallback.any():
         for i in np.nonzero(fallback)[0]:
             b.members[i].initial()
-        st2, steps2 = b.run_masked(fallback, max_steps, check_every, eps)
+        left = np.where(fallback, limit - steps, 0)
+        st2, n2, _ = _run(b, eps, left, check_every, mask=fallback & (left > 0))
         status = np.where(fallback, st2, status)
-        steps = np.where(fallback, steps + steps2, steps)
+        steps = np.where(fallback, steps + n2, steps)
     return status, steps, fallback
 
 
 def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
           growth=100, want_fields=False, device=0, predictions=None, field_fn=None, switch_eps=1e-5):
     """Run every case to the reference's stop criterion (errorU, errorT <= eps
-    at a check every `check_every` iterations) in one batch.
+    at a check every `check_every` iterations) in one batch, with the stop
+    test on the device.
 
     init "cold": the conduction state of initial(); "warm": the model's
     prediction (or `predictions`, a list of node-field dicts) through
     lbm_init_warm.  Members whose residual diverges (not finite, or growth x
     above its smallest value) restart cold and their steps add up.
-    storage "f64" / "f32" / "f16s", or "mixed": FP32 storage until the
-    residuals reach `switch_eps`, then the populations move to an FP64 batch
-    (lbm_get_populations / lbm_set_populations) that runs to `eps`, so the
-    result is the FP64 fixed point.
-    Returns a dict of per-case arrays and the wall time."""
-    first = "f32" if storage == "mixed" else storage
-    b, t_pred = _prepare(cases, init, first, model, predictions, device, growth)
+    storage "f64" / "f32" / "f16s", "mixed": FP32 storage until the residuals
+    reach `switch_eps`, then the batch converts in place to FP64
+    (lbm_batch_set_storage) and runs to `eps`, so the result is the FP64 fixed
+    point; or "auto": like "mixed", with the first phase's storage picked by
+    the autotuner among FP32 and FP64 (lbm_batch_tune; the tuning steps count).
+    max_steps bounds each member's iterations over all phases.
+    Returns a dict of per-case arrays and the wall time: `seconds` from the
+    first initialisation to the result (prediction and lbm_init_warm included),
+    of which `predict_seconds` was the network."""
+    two_phase = storage in ("mixed", "auto")
+    first = "f32" if two_phase else storage
+    b = _prepare(cases, first, device, growth)
+    b.synchronize()
     t0 = time.perf_counter()
-    status, steps, fallback = _run(b, switch_eps if storage == "mixed" else eps, max_steps, check_every)
-    steps_low = steps.copy()
-    if storage == "mixed":
-        b64 = L.Batch(2, [{k: v for k, v in c.items()} for c in cases], storage="f64", device=device)
-        b64.set_option("growth", int(growth))
-        for m32, m64 in zip(b.members, b64.members):
-            f, g = m32.populations()
-            m64.initial()
-            m64.set_populations(f, g)
-        b.close()
-        b = b64
-        status, steps2, fb2 = _run(b, eps, max_steps, check_every)
+    t_pred = _init(b, cases, init, model, predictions)
+    tuned = None
+    tune_steps = 0
+    if storage == "auto":
+        tune_steps = 12 * 6 + 2 * 6  # 2 storages x 3 tiles x 2 grids x (2 + 4) steps, +2 per storage
+        tuned = b.tune(steps=4, storages=("f32", "f64"))
+    b.synchronize()
+    status, steps, fallback = _run(b, switch_eps if two_phase else eps, max_steps - tune_steps, check_every)
+    steps = steps + tune_steps
+    status_low = status.copy() if two_phase else None
+    steps_low = steps.copy() if two_phase else None
+    if two_phase:
+        b.set_storage("f64")
+        left = np.maximum(max_steps - steps, 0)
+        status, steps2, fb2 = _run(b, eps, left, check_every)
         steps = steps + steps2
         fallback = fallback | fb2
     b.synchronize()
@@ -310,7 +337,8 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
     nu_hot, nu_cold = b.nusselt()
     out = {"status": status, "steps": steps, "fallback": fallback, "nu_hot": nu_hot, "nu_cold": nu_cold,
            "seconds": seconds, "predict_seconds": t_pred, "nodes": np.array([m.nnode for m in b.members]),
-           "storage": storage, "init": init, "steps_low_precision": steps_low if storage == "mixed" else None}
+           "storage": storage, "init": init, "steps_low_precision": steps_low, "status_low_precision": status_low,
+           "tuned": tuned}
     if want_fields:
         out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
     if field_fn is not None:
@@ -399,7 +427,7 @@ def evaluate(model, cases, max_steps=1_500_000, log=print):
                       "fallback": r["fallback"], "predict_seconds": r["predict_seconds"],
                       "steps_low_precision": r["steps_low_precision"]}
         if log:
-            log(f"{name}: {r['seconds']:.1f} s (+{r['predict_seconds']:.2f} s prediction), converged "
+            log(f"{name}: {r['seconds']:.1f} s (of which {r['predict_seconds']:.2f} s prediction), converged "
                 f"{int((r['status'] == 1).sum())}/{len(cases)}, fallbacks {int(r['fallback'].sum())}")
     return rows
 
@@ -416,7 +444,7 @@ def summarize(rows):
         r = rows[name]
         ok = np.asarray(r["status"]) == 1
         err = np.abs(np.asarray(r["nu"]) - ref) / np.abs(ref)
-        secs = r["seconds"] + r.get("predict_seconds", 0.0)
+        secs = r["seconds"]  # from the first initialisation to the result, prediction included
         out[name] = {"seconds": secs, "steps": int(np.sum(r["steps"])), "converged": int(ok.sum()),
                      "nu_within_1e-4": int((ok & (err <= 1e-4)).sum()),
                      "max_nu_rel_err_converged": float(err[ok].max()) if ok.any() else None,

@@ -244,3 +244,21 @@ def test_batch_3d_persistent_matches_standalone(pkg, persistent):
         r = b.tune(steps=4)
         assert r["tile"] == 32 and r["nblocks"] > 0
     b.close()
+
+
+def test_batch_tuner_chooses_storage(pkg):
+    # the autotuner's storage axis: with FP32 and FP64 allowed (the rule for a
+    # run's transient) it keeps the faster one, converting the batch in place;
+    # the members then step on, and FP64 alone converts back
+    b = pkg.Batch(2, pkg.sweep_specs(12, seed=5, sides=(64, 96, 128), aspect=(1.0, 2.0)), storage="f64")
+    b.initial()
+    b.step(10)
+    r = b.tune(steps=6, storages=("f32", "f64"))
+    assert r["storage"] in ("f32", "f64") and r["mlups"] > 0
+    assert all(m.storage == r["storage"] for m in b.members)
+    b.step(20)
+    b.set_storage("f64")
+    b.step(10)
+    eu, et = b.check()
+    assert np.isfinite(eu).all() and np.isfinite(et).all()
+    b.close()

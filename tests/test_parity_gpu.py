@@ -559,3 +559,38 @@ def test_output_ascii_matches_reference_writer(pkg, name, tmp_path):
     cav.close()
     with gzip.open(_os.path.join(gold, f"ref_{name}_tecplot.dat.gz"), "rt") as fh:
         assert open(path).read() == fh.read()
+
+
+@pytest.mark.parametrize("dim,shape", [(2, (64, 48, 1)), (3, (40, 24, 18))])
+def test_storage_conversion_in_place(pkg, dim, shape):
+    # FP32 -> FP64 -> FP32 of an FP32 state is exact, so a run converted there
+    # and back continues bit for bit; FP64 -> FP32 rounds each stored
+    # deviation once (<= 2^-24 relative), and the check history is kept
+    kw = dict(Ra=1e5, grid="tanh", stretch=1.5, kernel="march" if dim == 3 else "auto")
+    a = pkg.Cavity(dim, *shape, storage="f32", **kw)
+    b = pkg.Cavity(dim, *shape, storage="f32", **kw)
+    for c in (a, b):
+        c.initial()
+        c.step(20)
+    b.set_storage("f64")
+    assert b.storage == "f64"
+    b.set_storage("f32")
+    a.step(30)
+    b.step(30)
+    fa, ga = a.populations()
+    fb, gb = b.populations()
+    assert np.array_equal(fa, fb) and np.array_equal(ga, gb)
+    c = pkg.Cavity(dim, *shape, storage="f64", **kw)
+    c.initial()
+    c.step(25)
+    c.check()
+    f64 = c.populations()
+    c.set_storage("f32")
+    f32 = c.populations()
+    for x, y in zip(f32, f64):
+        assert np.abs(x - y).max() <= 1e-7
+    c.step(5)  # steps on in FP32 storage
+    eu, et = c.check()
+    assert np.isfinite(eu) and np.isfinite(et) and eu < 1.0
+    for cav in (a, b, c):
+        cav.close()

@@ -45,6 +45,10 @@ class _FakeBatch:
     def set_option(self, name, value):
         self.log.append(("option", name, value))
 
+    def set_storage(self, storage):
+        self.log.append(("storage", storage))
+        self.storage = storage
+
     def synchronize(self):
         pass
 
@@ -98,31 +102,24 @@ def test_diverged_members_restart_cold_and_their_steps_add_up(pkg, fake):
     assert b.closed
 
 
-def test_mixed_precision_hands_the_populations_to_fp64(pkg, fake):
+def test_mixed_precision_converts_the_batch_to_fp64(pkg, fake):
+    # FP32 to switch_eps, then the same batch converted in place to FP64 runs
+    # to eps on each member's remaining iteration budget: member 1 spent its
+    # whole budget in FP32 and does not run again
     W = pkg.warmstart
-    _FakeBatch.script = [{"status": [1, 0], "steps": [20000, 30000]}]
-    orig_init = _FakeBatch.__init__
-
-    def init(self, *a, **k):
-        orig_init(self, *a, **k)
-        if self.storage == "f64":
-            self.script = [{"status": [1, 1], "steps": [6000, 4000]}]
-
-    _FakeBatch.__init__ = init
-    try:
-        r = W.solve(_cases(2), init="cold", storage="mixed", eps=1e-6, switch_eps=1e-5)
-    finally:
-        _FakeBatch.__init__ = orig_init
-    b32, b64 = _FakeBatch.instances
-    assert (b32.storage, b64.storage) == ("f32", "f64")
-    assert b32.runs[0][1] == 1e-5 and b64.runs[0][1] == 1e-6
-    # every member's FP32 populations reached the FP64 batch, after an init
-    sets = [e for e in b64.log if e[0] == "set"]
-    assert [(e[1], e[2], e[3]) for e in sets] == [(0, 0, 0), (1, 1, 1)]
-    assert b32.closed and b64.closed
-    assert r["steps"].tolist() == [26000, 34000]
-    assert r["steps_low_precision"].tolist() == [20000, 30000]
-    assert r["status"].tolist() == [1, 1]
+    _FakeBatch.script = [{"status": [1, 0], "steps": [20000, 40000]},
+                         {"status": [1, 0], "steps": [6000, 0]}]
+    r = W.solve(_cases(2), init="cold", storage="mixed", eps=1e-6, switch_eps=1e-5, max_steps=40000)
+    assert len(_FakeBatch.instances) == 1
+    b = _FakeBatch.instances[0]
+    assert b.log.index(("storage", "f64")) > 0 and b.storage == "f64"
+    assert [run[1] for run in b.runs] == [1e-5, 1e-6]
+    assert b.runs[0][0] is None and b.runs[1][0] == [True, False]
+    assert b.closed
+    assert r["steps"].tolist() == [26000, 40000]
+    assert r["steps_low_precision"].tolist() == [20000, 40000]
+    assert r["status_low_precision"].tolist() == [1, 0]
+    assert r["status"].tolist() == [1, 0]
 
 
 def test_summary_counts_and_ratios(pkg):
@@ -132,7 +129,7 @@ def test_summary_counts_and_ratios(pkg):
         "f64_ref": {"nu": ref},
         "f64_cold": {"status": np.array([1, 1, 0]), "steps": np.array([10, 20, 30]), "seconds": 6.0,
                      "nu": ref * (1 + np.array([1e-5, 2e-5, 1e-3])), "sequential_seconds": 12.0},
-        "mixed_warm": {"status": np.array([1, 1, 1]), "steps": np.array([5, 10, 15]), "seconds": 2.0,
+        "mixed_warm": {"status": np.array([1, 1, 1]), "steps": np.array([5, 10, 15]), "seconds": 3.0,
                        "predict_seconds": 1.0, "nu": ref * (1 + np.array([5e-5, 2e-4, 0.0])),
                        "fallback": np.array([False, True, False])},
     }

@@ -46,8 +46,8 @@ WORKLOADS = {
     "cavity2d_2048": (2, 2048, 2048, 1, "tanh", 1.5, 1e6, 0.71),
     "cavity2d_128": (2, 128, 128, 1, "tanh", 1.5, 1e4, 0.71),
 }
-BYTES_PER_VALUE = {"f64": 8, "f32": 4, "f16s": 2}
-AUX_BYTES = {"f64": 8, "f32": 4, "f16s": 4}
+BYTES_PER_VALUE = {"f64": 8, "f32": 4}
+AUX_BYTES = {"f64": 8, "f32": 4}
 
 
 def bytes_per_lup(dim: int, storage: str) -> int:
@@ -510,7 +510,7 @@ def main():
     ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS) + ["batch256", "steady"])
     ap.add_argument("--cases", type=int, default=16, help="steady: held-out cavities")
     ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")
-    ap.add_argument("--storage", default="f64", choices=["f64", "f32", "f16s"])
+    ap.add_argument("--storage", default="f64", choices=["f64", "f32"])
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -646,7 +646,7 @@ def main():
         line = {
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "f16s": "f16 storage / f32"}[args.storage],
+            "vs_baseline": None, "dtype": args.storage,
             "data": "synthetic", "config": config_of(args, wl), "iterations_per_step": args.inner,
             "kernel_config": kernel_config(cav, pkg),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

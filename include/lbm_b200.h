@@ -49,8 +49,9 @@ extern "C" {
 #define LBM_STORE_F64   0  /* FP64 storage, FP64 arithmetic: the drop-in */
 #define LBM_STORE_F32   1  /* FP32 storage and arithmetic on deviations: f - w*rho0 and
                               g - wT*Tc (Tc: the conduction profile between the walls) */
-#define LBM_STORE_F16S  2  /* the same deviations stored as binary16 (scaled by 2^12),
-                              FP32 arithmetic; inaccurate for steady states */
+#define LBM_STORE_F16S  2  /* retired: the same deviations stored as binary16 gave Nu_avg errors
+                              of order one against FP64 and no speed-up over FP32 storage on
+                              B200; lbm_create rejects it with LBM_ERR_UNSUPPORTED */
 
 /* arithmetic mode (FP64 storage only) */
 #define LBM_MODE_FAST   0  /* multiply-add contraction, reciprocal constants */
@@ -68,7 +69,7 @@ extern "C" {
                                barrier between iterations.  Measured at 128^2 on B200: 3.87 us per
                                iteration in FP32 (4.10 with graph-replayed launches) but 4.85 us
                                in FP64, hence opt-in.  Batch members always step per iteration. */
-#define LBM_OPT_TILEY    6  /* 3D march kernel tile rows: 0 automatic, 4 (two blocks per SM) or 8 */
+#define LBM_OPT_TILEY    6  /* 3D march kernel tile rows: 0 automatic (4), 4 (two blocks per SM) or 8 */
 #define LBM_OPT_PLAN     7  /* 3D march work plan: 0 (default) every tile column in equal z-chunks
                                run side by side (neighbours share halo rows through L2), the blocks
                                left over taking the chunks' last slices in lockstep rounds;
@@ -254,11 +255,11 @@ int64_t lbm_kernel_launches(void);
 /* ------------------------------------------------------------------------ */
 typedef struct lbm_batch lbm_batch;
 
-#define LBM_BATCH_OPT_TILE        1  /* tile width of the 2D batch kernel: 32, 64, 128 (3D: 32 x 8) */
+#define LBM_BATCH_OPT_TILE        1  /* tile width of the 2D batch kernel: 32, 64, 128 (3D: 32 x 4) */
 #define LBM_BATCH_OPT_NBLOCKS     2  /* persistent blocks (0 = one full wave) */
 #define LBM_BATCH_OPT_PERSISTENT  3  /* 1: one persistent kernel per step (2D and 3D; a 3D batch with a
-                                        member whose ny % 8 == 1 steps per member), 0: one launch per
-                                        cavity */
+                                        member whose ny % 4 == 1, or whose tile rows were changed,
+                                        steps per member), 0: one launch per cavity */
 #define LBM_BATCH_OPT_GRAPHS      4  /* 1: replay steps from CUDA graphs */
 #define LBM_BATCH_OPT_GROWTH      5  /* lbm_batch_run stops a member whose residual is not finite or
                                         exceeds this factor x its smallest one in the run and reports

@@ -175,17 +175,18 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
         if (e == cudaSuccess) e = cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e)));
     }
-    // the 3D batch kernel has 32 x 8 tiles: a last tile row of a single y-row
-    // (its one-sided stencil would reach two rows below the box) is not covered
+    // the 3D batch kernel has 32 x kBatchTileY tiles: a last tile row of a
+    // single y-row (its one-sided stencil would reach two rows below the box)
+    // is not covered
     if (b->dim == 3)
         for (int i = 0; i < n; ++i)
-            if (b->cav[i]->geo.ny % 8 == 1 || b->cav[i]->tiley != 8) b->march_ok = false;
+            if (b->cav[i]->geo.ny % kBatchTileY == 1 || b->cav[i]->tiley != kBatchTileY) b->march_ok = false;
     *out = b;
     return LBM_OK;
 }
 
 // descriptors for the tile width, and the work list of the active cavities.
-// A column is one march: 2D a TX-wide strip of rows, 3D a 32 x 8 tile of slices.
+// A column is one march: 2D a TX-wide strip of rows, 3D a 32 x kBatchTileY tile of slices.
 static int build_tables(lbm_batch *b)
 {
     drop_graphs(b);
@@ -207,7 +208,7 @@ static int build_tables(lbm_batch *b)
         if (!b->active[i]) continue;
         const Geo &g = b->cav[i]->geo;
         if (d3) {
-            const int nt = ((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+            const int nt = ((g.nx + 31) / 32) * ((g.ny + kBatchTileY - 1) / kBatchTileY);
             for (int t = 0; t < nt; ++t) cols.push_back({i, t, g.nz});
             total += (int64_t)nt * g.nz;
         } else {
@@ -692,7 +693,7 @@ static int tune_storage(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nbl
     BCU(cudaSetDevice(b->device));
     int sms = 0;
     BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    const int tiles2[3] = {32, 64, 128}, tiles3[1] = {32};  // 3D: the tile is fixed at 32 x 8
+    const int tiles2[3] = {32, 64, 128}, tiles3[1] = {32};  // 3D: the tile is fixed at 32 x kBatchTileY
     const int *tiles = b->dim == 3 ? tiles3 : tiles2;
     const int ntile = b->dim == 3 ? 1 : 3;
     double best = -1.0;

@@ -43,7 +43,7 @@ struct lbm_handle {
     int nblocks_opt = 0;         // LBM_OPT_NBLOCKS as set
     int nblocks = 0;             // resolved persistent grid
     int tiley_opt = 0;           // LBM_OPT_TILEY as set (0: automatic)
-    int tiley = 8;               // resolved tile rows of the 3D march kernel (4 or 8)
+    int tiley = 4;               // resolved tile rows of the 3D march kernel (4 or 8)
     int plan_opt = 0;            // LBM_OPT_PLAN: 0 balanced z-lockstep, 1 contiguous shares
     int64_t wait_limit = 0;      // LBM_OPT_WAIT_LIMIT as last set through this handle
     int4 *d_msegs = nullptr;     // 3D march work plan: segments (tile, z0, z1, -)

@@ -24,7 +24,6 @@
 // every node, rows of `pitch` elements, z-planes of `slab` elements.  Planes
 // 0..Q-1 are f, Q..Q+QT-1 are g.
 #include <cuda.h>
-#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "lbm_internal.h"
@@ -45,24 +44,20 @@ template <int ST> struct Tr;
 // conduction profile (tc_value)
 template <> struct Tr<kF64> { using S = double; using C = double; static constexpr bool kShift = false, kDevT = false; };
 template <> struct Tr<kF32> { using S = float;  using C = float;  static constexpr bool kShift = true, kDevT = true; };
-template <> struct Tr<kF16S> { using S = __half; using C = float; static constexpr bool kShift = true, kDevT = true; };
 
 __device__ __forceinline__ double tocomp(double x) { return x; }
 __device__ __forceinline__ float tocomp(float x) { return x; }
-__device__ __forceinline__ float tocomp(__half x) { return __half2float(x) * kF16InvScale; }
 
 template <class S> __device__ __forceinline__ S fromcomp(double x);
 template <> __device__ __forceinline__ double fromcomp<double>(double x) { return x; }
 template <class S> __device__ __forceinline__ S fromcompf(float x);
 template <> __device__ __forceinline__ float fromcompf<float>(float x) { return x; }
-template <> __device__ __forceinline__ __half fromcompf<__half>(float x) { return __float2half_rn(x * kF16Scale); }
 
 template <class S, class C> __device__ __forceinline__ S tostore(C x);
 template <> __device__ __forceinline__ double tostore<double, double>(double x) { return x; }
 template <> __device__ __forceinline__ float tostore<float, float>(float x) { return x; }
-template <> __device__ __forceinline__ __half tostore<__half, float>(float x) { return __float2half_rn(x * kF16Scale); }
 
-// Reduced-precision storage (FP32, shifted FP16) keeps f - w*rho0 (rho0 = 1)
+// Reduced-precision storage (FP32) keeps f - w*rho0 (rho0 = 1)
 // and g - wT*Tc (Tc: the linear conduction profile between the isothermal
 // walls), and both stay in that deviation form through streaming and
 // collision:
@@ -1103,7 +1098,6 @@ static cudaError_t launch_step(const Geo &g, const void *pin, const void *Fin, v
     switch (store) {                                       \
     case kF64: return CALL(kF64);                          \
     case kF32: return CALL(kF32);                          \
-    case kF16S: return CALL(kF16S);                        \
     default: return cudaErrorNotSupported;                 \
     }
 #endif
@@ -1146,7 +1140,7 @@ int resident_blocks(const Geo &g, int store, int device)
     switch (store) {
     case kF64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF64>, 256, 0); break;
     case kF32: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF32>, 256, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_steps2d_resident<kF16S>, 256, 0); break;
+    default: break;
     }
     if (e != cudaSuccess || bps <= 0) return 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
@@ -1379,8 +1373,8 @@ static cudaError_t prepare_batch3d()
 {
     static bool done = false;
     if (!done) {
-        cudaError_t e = cudaFuncSetAttribute(k_march3d_batch<ST, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             L3<ST, 8>::smem());
+        cudaError_t e = cudaFuncSetAttribute(k_march3d_batch<ST, kBatchTileY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L3<ST, kBatchTileY>::smem());
         if (e != cudaSuccess) return e;
         done = true;
     }
@@ -1392,7 +1386,7 @@ static cudaError_t launch_batch3d(const BatchDev &D, int nblocks, int cur, int w
 {
     cudaError_t e = prepare_batch3d<ST>();
     if (e != cudaSuccess) return e;
-    k_march3d_batch<ST, 8><<<nblocks, L3<ST, 8>::NT, L3<ST, 8>::smem(), s>>>(D, cur, wm, err);
+    k_march3d_batch<ST, kBatchTileY><<<nblocks, L3<ST, kBatchTileY>::NT, L3<ST, kBatchTileY>::smem(), s>>>(D, cur, wm, err);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -1402,8 +1396,8 @@ static int batch3d_bps()
 {
     if (prepare_batch3d<ST>() != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d_batch<ST, 8>, L3<ST, 8>::NT,
-                                                         L3<ST, 8>::smem()) == cudaSuccess
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d_batch<ST, kBatchTileY>, L3<ST, kBatchTileY>::NT,
+                                                         L3<ST, kBatchTileY>::smem()) == cudaSuccess
                ? n
                : 0;
 }
@@ -1449,13 +1443,13 @@ MarchShape march_shape(int dim, int store, int tx, int ty)
             switch (store) {
             case kF64: fill(fast::L3<kF64, 4>{}, 3); break;
             case kF32: fill(fast::L3<kF32, 4>{}, 3); break;
-            default: fill(fast::L3<kF16S, 4>{}, 3); break;
+            default: fill(fast::L3<kF32, 4>{}, 3); break;
             }
         } else {
             switch (store) {
             case kF64: fill(fast::L3<kF64, 8>{}, 3); break;
             case kF32: fill(fast::L3<kF32, 8>{}, 3); break;
-            default: fill(fast::L3<kF16S, 8>{}, 3); break;
+            default: fill(fast::L3<kF32, 8>{}, 3); break;
             }
         }
         for (int c = 0; c < 4; ++c) {
@@ -1467,7 +1461,7 @@ MarchShape march_shape(int dim, int store, int tx, int ty)
         switch (store) {                                                  \
         case kF64: fill(fast::L2<kF64, TXV>{}, 2); break;                 \
         case kF32: fill(fast::L2<kF32, TXV>{}, 2); break;                 \
-        default: fill(fast::L2<kF16S, TXV>{}, 2); break;                  \
+        default: fill(fast::L2<kF32, TXV>{}, 2); break;                   \
         }
         if (tx == 32) { LBM_FILL2(32) }
         else if (tx == 64) { LBM_FILL2(64) }

@@ -60,9 +60,34 @@ __device__ __forceinline__ uint32_t mbar_test(uint64_t *b, uint32_t parity)
     return ok;
 }
 
+// non-blocking test of the phase of parity `parity` (try_wait may suspend
+// the thread for a while before it reports an incomplete phase)
+__device__ __forceinline__ uint32_t mbar_probe(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(saddr(b)), "r"(parity)
+        : "memory");
+    return ok;
+}
+
+// limits below this poll with mbar_probe, so that they can run out before a
+// copy in flight lands (the error path's tests)
+static constexpr long long kShortWait = 1000000LL;
+
 // bounded wait for the phase of parity `parity`; false after `limit` cycles
 __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, long long limit = kWaitCycles)
 {
+    if (limit < kShortWait) {
+        const long long t0 = clock64();
+        while (!mbar_probe(b, parity))
+            if (clock64() - t0 > limit) return false;
+        return true;
+    }
     if (mbar_test(b, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_test(b, parity))

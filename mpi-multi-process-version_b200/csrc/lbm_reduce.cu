@@ -5,7 +5,6 @@
 // shared memory into one partial per block, and a single block then sums the
 // partials in block order.  The result does not depend on timing, only on
 // the grid size (fixed by the node count).
-#include <cuda_fp16.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -317,8 +316,7 @@ __global__ void k_aos_to_planes(const Geo G, int q0, int nq, const double *__res
     const int64_t dst = (int64_t)q * G.plane + pidx(G, n);
     const double val = aos[e];
     if (ST == kF64) ((double *)pop)[dst] = val;
-    else if (ST == kF32) ((float *)pop)[dst] = float(val - shift_of(G, q, n));
-    else ((__half *)pop)[dst] = __float2half_rn(float(val - shift_of(G, q, n)) * kF16Scale);
+    else ((float *)pop)[dst] = float(val - shift_of(G, q, n));
 }
 
 template <int ST>
@@ -331,8 +329,7 @@ __global__ void k_planes_to_aos(const Geo G, int q0, int nq, const void *pop, do
     const int64_t src = (int64_t)q * G.plane + pidx(G, n);
     double val;
     if (ST == kF64) val = ((const double *)pop)[src];
-    else if (ST == kF32) val = double(((const float *)pop)[src]) + shift_of(G, q, n);
-    else val = double(__half2float(((const __half *)pop)[src]) * kF16InvScale) + shift_of(G, q, n);
+    else val = double(((const float *)pop)[src]) + shift_of(G, q, n);
     aos[e] = val;
 }
 
@@ -341,8 +338,7 @@ cudaError_t aos_to_planes(const Geo &g, int store, int q0, int nq, const double 
     const int64_t n = g.nnode * nq;
     const unsigned nb = unsigned((n + 255) / 256);
     if (store == kF64) k_aos_to_planes<kF64><<<nb, 256, 0, s>>>(g, q0, nq, aos, pop);
-    else if (store == kF32) k_aos_to_planes<kF32><<<nb, 256, 0, s>>>(g, q0, nq, aos, pop);
-    else k_aos_to_planes<kF16S><<<nb, 256, 0, s>>>(g, q0, nq, aos, pop);
+    else k_aos_to_planes<kF32><<<nb, 256, 0, s>>>(g, q0, nq, aos, pop);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -352,8 +348,7 @@ cudaError_t planes_to_aos(const Geo &g, int store, int q0, int nq, const void *p
     const int64_t n = g.nnode * nq;
     const unsigned nb = unsigned((n + 255) / 256);
     if (store == kF64) k_planes_to_aos<kF64><<<nb, 256, 0, s>>>(g, q0, nq, pop, aos);
-    else if (store == kF32) k_planes_to_aos<kF32><<<nb, 256, 0, s>>>(g, q0, nq, pop, aos);
-    else k_planes_to_aos<kF16S><<<nb, 256, 0, s>>>(g, q0, nq, pop, aos);
+    else k_planes_to_aos<kF32><<<nb, 256, 0, s>>>(g, q0, nq, pop, aos);
     ++g_launches;
     return cudaGetLastError();
 }
@@ -371,19 +366,16 @@ __global__ void k_convert_planes(const Geo G, int nq, const void *src, void *dst
     const int64_t a = (int64_t)q * G.plane + pidx(G, n);
     double val;
     if (SRC == kF64) val = ((const double *)src)[a];
-    else if (SRC == kF32) val = double(((const float *)src)[a]) + shift_of(G, q, n);
-    else val = double(__half2float(((const __half *)src)[a]) * kF16InvScale) + shift_of(G, q, n);
+    else val = double(((const float *)src)[a]) + shift_of(G, q, n);
     if (DST == kF64) ((double *)dst)[a] = val;
-    else if (DST == kF32) ((float *)dst)[a] = float(val - shift_of(G, q, n));
-    else ((__half *)dst)[a] = __float2half_rn(float(val - shift_of(G, q, n)) * kF16Scale);
+    else ((float *)dst)[a] = float(val - shift_of(G, q, n));
 }
 
 template <int SRC>
 static void convert_from(const Geo &g, int dst_store, int nq, const void *src, void *dst, unsigned nb, cudaStream_t s)
 {
     if (dst_store == kF64) k_convert_planes<SRC, kF64><<<nb, 256, 0, s>>>(g, nq, src, dst);
-    else if (dst_store == kF32) k_convert_planes<SRC, kF32><<<nb, 256, 0, s>>>(g, nq, src, dst);
-    else k_convert_planes<SRC, kF16S><<<nb, 256, 0, s>>>(g, nq, src, dst);
+    else k_convert_planes<SRC, kF32><<<nb, 256, 0, s>>>(g, nq, src, dst);
 }
 
 // the carried force, one compute-type value per cell of a plane
@@ -402,8 +394,7 @@ cudaError_t convert_state(const Geo &g, int src_store, int dst_store, int nq, co
     const int64_t n = g.nnode * nq;
     const unsigned nb = unsigned((n + 255) / 256);
     if (src_store == kF64) convert_from<kF64>(g, dst_store, nq, pop_src, pop_dst, nb, s);
-    else if (src_store == kF32) convert_from<kF32>(g, dst_store, nq, pop_src, pop_dst, nb, s);
-    else convert_from<kF16S>(g, dst_store, nq, pop_src, pop_dst, nb, s);
+    else convert_from<kF32>(g, dst_store, nq, pop_src, pop_dst, nb, s);
     k_convert_force<<<unsigned((g.plane + 255) / 256), 256, 0, s>>>(g.plane, src_store == kF64, dst_store == kF64,
                                                                     F_src, F_dst);
     g_launches += 2;
@@ -423,8 +414,7 @@ __global__ void k_macro_from_pops(const Geo G, const void *pop, const Bufs B)
     auto ld = [&](int q) -> double {
         const int64_t a = (int64_t)q * G.plane + id;
         if (ST == kF64) return ((const double *)pop)[a];
-        if (ST == kF32) return double(((const float *)pop)[a]) + shift_of(G, q, n);
-        return double(__half2float(((const __half *)pop)[a]) * kF16InvScale) + shift_of(G, q, n);
+        return double(((const float *)pop)[a]) + shift_of(G, q, n);
     };
     const int ex2[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
     const int ey2[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
@@ -456,8 +446,7 @@ cudaError_t macro_from_pops(const Geo &g, int store, const void *pop, const Bufs
 {
     const unsigned nb = unsigned((g.nnode + 255) / 256);
     if (store == kF64) k_macro_from_pops<kF64><<<nb, 256, 0, s>>>(g, pop, b);
-    else if (store == kF32) k_macro_from_pops<kF32><<<nb, 256, 0, s>>>(g, pop, b);
-    else k_macro_from_pops<kF16S><<<nb, 256, 0, s>>>(g, pop, b);
+    else k_macro_from_pops<kF32><<<nb, 256, 0, s>>>(g, pop, b);
     ++g_launches;
     return cudaGetLastError();
 }

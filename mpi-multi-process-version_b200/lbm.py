@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblbm_b200.so")
 
 LBM_OK = 0
-STORE = {"f64": 0, "f32": 1, "f16s": 2}
+STORE = {"f64": 0, "f32": 1}  # 2 (binary16 storage) is retired: the library rejects it
 MODE = {"fast": 0, "exact": 1}
 GRID = {"erf": 0, "tanh": 1, "uniform": 2}
 

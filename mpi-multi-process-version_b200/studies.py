@@ -26,7 +26,7 @@ def _max_abs(m, keys):
 
 
 def precision_errors(dim, shape, Ra, Pr=0.71, steps=20000, grid="tanh", stretch=1.5, noise=0.0, seed=0,
-                     storages=("f64", "f32", "f16s")):
+                     storages=("f64", "f32")):
     """Run the same cavity in each storage precision from the same initial
     state for `steps` iterations; report Nu_avg, max |u|, max |v| (max |w|)
     and their errors against FP64, plus the throughput of each variant."""
@@ -69,7 +69,7 @@ def main(argv=None):
     argv = list(sys.argv[1:] if argv is None else argv)
     what = argv[0] if argv else "precision3d"
     if what == "precision3d":
-        # 3D differentially heated cube, 128^3, tanh 1.5, Ra 1e5: FP64 vs FP32 vs shifted FP16
+        # 3D differentially heated cube, 128^3, tanh 1.5, Ra 1e5: FP64 vs FP32 storage
         rows = precision_errors(3, (128, 128, 128), 1e5, steps=int(argv[1]) if len(argv) > 1 else 20000)
     elif what == "precision2d":
         # 2D 2048^2, tanh 1.5, Ra in {1e6, 1e7, 1e8}, seeded temperature noise 1e-4

@@ -301,7 +301,7 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
     prediction (or `predictions`, a list of node-field dicts) through
     lbm_init_warm.  Members whose residual diverges (not finite, or growth x
     above its smallest value) restart cold and their steps add up.
-    storage "f64" / "f32" / "f16s", "mixed": FP32 storage until the residuals
+    storage "f64" / "f32", "mixed": FP32 storage until the residuals
     reach `switch_eps`, then the batch converts in place to FP64
     (lbm_batch_set_storage) and runs to `eps`, so the result is the FP64 fixed
     point; or "auto": like "mixed", with the first phase's storage picked by

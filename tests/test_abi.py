@@ -91,6 +91,15 @@ def test_bad_parameters_rejected_without_device(pkg, bad):
     assert pkg.lib().lbm_last_error()
 
 
+def test_retired_binary16_storage_is_rejected(pkg):
+    # LBM_STORE_F16S (2) is retired: its errors against FP64 were of order one
+    p = _params(pkg, storage=2)
+    out = np.zeros(9)
+    st = pkg.lib().lbm_derived_params(ctypes.byref(p), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert st == -8
+    assert b"retired" in pkg.lib().lbm_last_error()
+
+
 def test_create_without_gpu_reports_no_device(pkg, has_gpu):
     if has_gpu:
         pytest.skip("a GPU is present")

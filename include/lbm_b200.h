@@ -303,6 +303,18 @@ int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double e
  * warm-start driver restarts those from the conduction state). */
 int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
                          double eps, int32_t *converged, int64_t *steps_done);
+/* Mixed precision, member by member: every member on the mask starts in FP32
+ * storage and runs to errorU, errorT <= switch_eps; each member that gets
+ * there is converted alone to FP64 in place (its FP64 finish overlaps the
+ * others' FP32 transients) and runs on to eps, so its result is the FP64
+ * fixed point.  max_steps bounds each member's iterations over both phases;
+ * steps_low[i] (optional) reports its FP32 iterations; converged[] and
+ * LBM_BATCH_OPT_GROWTH as lbm_batch_run_masked.  Members may end in different
+ * storages (LBM_BATCH_OPT_STORAGE then reports -1).  Not in exact mode.  No
+ * counterpart in the reference (FP64 throughout). */
+int lbm_batch_run_mixed(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
+                        double switch_eps, double eps, int32_t *converged, int64_t *steps_done,
+                        int64_t *steps_low);
 /* The autotuner: time each storage LBM_BATCH_OPT_STORAGES allows (the
  * batch's state is converted in place, lbm_batch_set_storage) x each tile
  * width and grid size on the batch itself (the timed steps advance the

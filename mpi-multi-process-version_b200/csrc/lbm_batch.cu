@@ -59,15 +59,23 @@ struct lbm_batch {
     Geo *d_geo = nullptr;
     TmapSet *d_maps = nullptr;
     Bufs *d_bufs = nullptr;
-    int4 *d_segs = nullptr;
-    int *d_segoff = nullptr;
+    // one work list per population storage (members may differ while a
+    // mixed-precision run hands them from FP32 to FP64 one by one)
+    struct WorkList {
+        int4 *d_segs = nullptr;
+        int *d_segoff = nullptr;
+        size_t segs_cap = 0, segoff_cap = 0;
+        int nblocks = 0;
+        BatchDev dev{};
+    } wl[2];
     int *d_err = nullptr;
-    size_t segs_cap = 0, segoff_cap = 0;
-    BatchDev dev{};
+    BatchDev dev{};                // the tables (segment fields unused) for the batched check
     bool dirty = true;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     cudaGraphExec_t run_graph[2] = {nullptr, nullptr};  // check periods of lbm_batch_run from cur = 0 / 1
     int run_graph_period = 0;
+    int64_t run_graph_launches = 0;  // kernels one replay of a check-period graph launches
+    int64_t graph_launches = 0;      // kernels one replay of a 2-step graph launches
     int64_t active_nodes = 0;
     RunCtl *d_ctl = nullptr;       // run state of every member (member i's bufs.ctl = d_ctl + i)
     int *d_idx = nullptr;          // members on the work list, for the batched check
@@ -95,7 +103,8 @@ extern "C" int lbm_batch_destroy(lbm_batch *b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
     for (lbm_handle *h : b->cav) lbm_destroy(h);
-    void *ptrs[] = {b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff, b->d_err, b->d_ctl, b->d_idx};
+    void *ptrs[] = {b->d_geo, b->d_maps,        b->d_bufs,         b->d_err,        b->d_ctl,
+                    b->d_idx, b->wl[0].d_segs,  b->wl[0].d_segoff, b->wl[1].d_segs, b->wl[1].d_segoff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -197,6 +206,12 @@ static int build_tables(lbm_batch *b)
         if (!encode_maps_tx(b->cav[i], d3 ? 0 : TX, &maps[2 * (size_t)i]))
             return set_error(LBM_ERR_UNSUPPORTED, "batch: TMA descriptors for cavity %d could not be encoded", i);
     BCU(cudaMemcpyAsync(b->d_maps, maps.data(), sizeof(TmapSet) * maps.size(), cudaMemcpyHostToDevice, b->stream));
+    {
+        // the members' buffers (a storage change gives a member new ones)
+        std::vector<Bufs> bufs(b->n);
+        for (int i = 0; i < b->n; ++i) bufs[i] = b->cav[i]->bufs;
+        BCU(cudaMemcpyAsync(b->d_bufs, bufs.data(), sizeof(Bufs) * b->n, cudaMemcpyHostToDevice, b->stream));
+    }
 
     struct Col {
         int cav, pos, ny;  // pos: 2D the strip's x-offset, 3D the tile index; ny: items (rows or slices)
@@ -217,52 +232,68 @@ static int build_tables(lbm_batch *b)
         }
         b->active_nodes += g.nnode;
     }
-    const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(b->storage)
-                                                     : fast::march_batch3d_blocks_per_sm(b->storage))
-                       : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(b->storage, TX)
-                                                    : fast::march_batch_blocks_per_sm(b->storage, TX));
-    if (bps <= 0) return set_error(LBM_ERR_UNSUPPORTED, "batch kernel with tile %d cannot be resident", TX);
+    (void)total;
     int sms = 0;
     BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
-    int64_t G = b->nblocks_opt > 0 ? b->nblocks_opt : (int64_t)bps * sms;
-    if (G > total) G = total;
-    if (G < 1) G = 1;
-    b->nblocks = (int)G;
-    // equal contiguous shares of the (column, row) items
-    std::vector<int4> segs;
-    std::vector<int> off(G + 1, 0);
-    size_t c = 0;
-    int64_t colbase = 0;  // first item of column c
-    for (int64_t blk = 0; blk < G; ++blk) {
-        off[blk] = (int)segs.size();
-        const int64_t lo = total * blk / G, hi = total * (blk + 1) / G;
-        int64_t u = lo;
-        while (u < hi) {
-            while (c < cols.size() && colbase + cols[c].ny <= u) colbase += cols[c++].ny;
-            const int64_t end = std::min<int64_t>(hi, colbase + cols[c].ny);
-            if (d3)
-                segs.push_back(make_int4(cols[c].pos, (int)(u - colbase), (int)(end - colbase), cols[c].cav));
-            else
-                segs.push_back(make_int4(cols[c].cav, cols[c].pos, (int)(u - colbase), (int)(end - colbase)));
-            u = end;
+    b->nblocks = 0;
+    for (int sto = 0; sto < 2; ++sto) {
+        lbm_batch::WorkList &W = b->wl[sto];
+        W.nblocks = 0;
+        // this storage's columns
+        std::vector<Col> sc;
+        int64_t stotal = 0;
+        for (const Col &c : cols)
+            if (b->cav[c.cav]->p.storage == sto) {
+                sc.push_back(c);
+                stotal += c.ny;
+            }
+        if (sc.empty()) continue;
+        const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(sto)
+                                                         : fast::march_batch3d_blocks_per_sm(sto))
+                           : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(sto, TX)
+                                                        : fast::march_batch_blocks_per_sm(sto, TX));
+        if (bps <= 0) return set_error(LBM_ERR_UNSUPPORTED, "batch kernel with tile %d cannot be resident", TX);
+        int64_t G = b->nblocks_opt > 0 ? b->nblocks_opt : (int64_t)bps * sms;
+        if (G > stotal) G = stotal;
+        if (G < 1) G = 1;
+        // equal contiguous shares of the (column, item) items
+        std::vector<int4> segs;
+        std::vector<int> off(G + 1, 0);
+        size_t c = 0;
+        int64_t colbase = 0;  // first item of column c
+        for (int64_t blk = 0; blk < G; ++blk) {
+            off[blk] = (int)segs.size();
+            const int64_t lo = stotal * blk / G, hi = stotal * (blk + 1) / G;
+            int64_t u = lo;
+            while (u < hi) {
+                while (c < sc.size() && colbase + sc[c].ny <= u) colbase += sc[c++].ny;
+                const int64_t end = std::min<int64_t>(hi, colbase + sc[c].ny);
+                if (d3)
+                    segs.push_back(make_int4(sc[c].pos, (int)(u - colbase), (int)(end - colbase), sc[c].cav));
+                else
+                    segs.push_back(make_int4(sc[c].cav, sc[c].pos, (int)(u - colbase), (int)(end - colbase)));
+                u = end;
+            }
         }
+        off[G] = (int)segs.size();
+        if (segs.size() > W.segs_cap) {
+            if (W.d_segs) cudaFree(W.d_segs);
+            W.segs_cap = segs.size() * 2 + 16;
+            BCU(cudaMalloc(&W.d_segs, sizeof(int4) * W.segs_cap));
+        }
+        if (off.size() > W.segoff_cap) {
+            if (W.d_segoff) cudaFree(W.d_segoff);
+            W.segoff_cap = off.size() * 2 + 16;
+            BCU(cudaMalloc(&W.d_segoff, sizeof(int) * W.segoff_cap));
+        }
+        BCU(cudaMemcpyAsync(W.d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, b->stream));
+        BCU(cudaMemcpyAsync(W.d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
+        W.nblocks = (int)G;
+        W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, W.d_segoff};
+        b->nblocks += (int)G;
     }
-    off[G] = (int)segs.size();
-    if (segs.size() > b->segs_cap) {
-        if (b->d_segs) cudaFree(b->d_segs);
-        b->segs_cap = segs.size() * 2 + 16;
-        BCU(cudaMalloc(&b->d_segs, sizeof(int4) * b->segs_cap));
-    }
-    if (off.size() > b->segoff_cap) {
-        if (b->d_segoff) cudaFree(b->d_segoff);
-        b->segoff_cap = off.size() * 2 + 16;
-        BCU(cudaMalloc(&b->d_segoff, sizeof(int) * b->segoff_cap));
-    }
-    if (!segs.empty())
-        BCU(cudaMemcpyAsync(b->d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, b->stream));
-    BCU(cudaMemcpyAsync(b->d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
-    b->dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, b->d_segs, b->d_segoff};
+    b->dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, nullptr, nullptr};
     {
         std::vector<int> idx;
         for (int i = 0; i < b->n; ++i)
@@ -275,15 +306,24 @@ static int build_tables(lbm_batch *b)
     return LBM_OK;
 }
 
+// one step of every member on the work lists: one persistent kernel per
+// population storage present
 static cudaError_t launch_step(lbm_batch *b, int cur, int wm)
 {
-    if (b->dim == 3)
-        return b->mode == LBM_MODE_EXACT
-                   ? exact::march_batch3d(b->storage, b->dev, b->nblocks, cur, wm, b->d_err, b->stream)
-                   : fast::march_batch3d(b->storage, b->dev, b->nblocks, cur, wm, b->d_err, b->stream);
-    return b->mode == LBM_MODE_EXACT
-               ? exact::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream)
-               : fast::march_batch(b->storage, b->tile, b->dev, b->nblocks, cur, wm, b->d_err, b->stream);
+    for (int sto = 0; sto < 2; ++sto) {
+        const lbm_batch::WorkList &W = b->wl[sto];
+        if (W.nblocks <= 0) continue;
+        cudaError_t e;
+        if (b->dim == 3)
+            e = b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, b->stream)
+                                          : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, b->stream);
+        else
+            e = b->mode == LBM_MODE_EXACT
+                    ? exact::march_batch(sto, b->tile, W.dev, W.nblocks, cur, wm, b->d_err, b->stream)
+                    : fast::march_batch(sto, b->tile, W.dev, W.nblocks, cur, wm, b->d_err, b->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // a 2-step graph starting from buffer `cur`
@@ -291,11 +331,13 @@ static int get_graph(lbm_batch *b, int cur, cudaGraphExec_t *out)
 {
     if (!b->graph[cur]) {
         cudaGraph_t g = nullptr;
+        const int64_t launches0 = g_launches;
         BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e1 = launch_step(b, cur, 0);
         cudaError_t e2 = launch_step(b, 1 - cur, 0);
         cudaError_t e3 = cudaStreamEndCapture(b->stream, &g);
-        g_launches -= 2;  // counted when replayed
+        b->graph_launches = g_launches - launches0;
+        g_launches = launches0;  // counted when replayed
         if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             return set_error(LBM_ERR_CUDA, "batch graph capture failed: %s",
@@ -348,7 +390,7 @@ extern "C" int lbm_batch_step(lbm_batch *b, int32_t nsteps)
             int st = get_graph(b, cur, &g);
             if (st) return st;
             BCU(cudaGraphLaunch(g, b->stream));
-            g_launches += 2;
+            g_launches += b->graph_launches;
             done += 2;
         }
     }
@@ -448,12 +490,14 @@ static int batch_period_graph(lbm_batch *b, int cur, int period, cudaGraphExec_t
     }
     if (!b->run_graph[cur]) {
         cudaGraph_t g = nullptr;
+        const int64_t launches0 = g_launches;
         BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int i = 0; i < period && e == cudaSuccess; ++i) e = launch_step(b, (cur + i) & 1, i == period - 1);
         if (e == cudaSuccess) e = run_check_batch(b->dev, b->d_idx, b->nidx, period, b->stream);
         const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
-        g_launches -= period + 2;  // counted when replayed
+        b->run_graph_launches = g_launches - launches0;
+        g_launches = launches0;  // counted when replayed
         if (e != cudaSuccess || e2 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             return set_error(LBM_ERR_CUDA, "batch check-period graph capture: %s",
@@ -470,11 +514,21 @@ static int batch_period_graph(lbm_batch *b, int cur, int period, cudaGraphExec_t
 // check periods a batch run queues between two reads of the members' run state
 static constexpr int kBatchPeriodsPerRead = 4;
 
-extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
-                                    double eps, int32_t *converged, int64_t *steps_done)
+// The batch's run loop.  Every member on the mask runs the reference's stop
+// test on the device after each check (run_decide).  Single phase
+// (two_phase false): criterion eps1.  Two phases (mixed precision): every
+// member starts in FP32 storage with criterion eps1; when it meets it, the host
+// (at its next read) converts that member alone to FP64 in place, into the
+// batch's current ping-pong buffer, and it goes on with criterion eps2 while
+// the others continue in FP32: each member's FP64 finish overlaps the other
+// members' FP32 transients.  max_steps bounds each member's iterations.
+static int batch_run(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every, double eps1,
+                     double eps2, bool two_phase, int32_t *converged, int64_t *steps_done, int64_t *steps_low)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
     if (max_steps < 0 || check_every < 1) return set_error(LBM_ERR_PARAM, "need max_steps >= 0, check_every >= 1");
+    if (two_phase && b->mode == LBM_MODE_EXACT)
+        return set_error(LBM_ERR_UNSUPPORTED, "mixed precision: exact mode computes in FP64 storage only");
     BCU(cudaSetDevice(b->device));
     const int n = b->n;
     int remaining = 0;
@@ -482,6 +536,7 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
         const bool on = !mask || mask[i] != 0;
         if (converged) converged[i] = 0;
         if (steps_done) steps_done[i] = 0;
+        if (steps_low) steps_low[i] = 0;
         b->active[i] = on ? 1 : 0;
         remaining += on ? 1 : 0;
     }
@@ -492,28 +547,43 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
         if (b->active[i]) {
             int st = first_collision(b->cav[i]);
             if (st) return st;
+            if (two_phase && (st = change_storage(b->cav[i], LBM_STORE_F32))) return st;
         }
-    // the stop test of every member runs on the device (run_decide): the
-    // reference's criterion (errorU, errorT <= eps, 2M:307) and, with
-    // LBM_BATCH_OPT_GROWTH, a residual that stops being finite or grows past
-    // growth x its smallest value in this run stops the member (status -1)
+    if (two_phase) {
+        std::vector<Bufs> bufs(n);
+        for (int i = 0; i < n; ++i) bufs[i] = b->cav[i]->bufs;
+        BCU(cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice));
+    }
+    // the common parity of the members on the mask
+    int cur = -1;
+    for (int i = 0; i < n; ++i)
+        if (b->active[i]) {
+            if (cur < 0) cur = b->cav[i]->cur;
+            if (b->cav[i]->cur != cur)
+                return set_error(LBM_ERR_STATE, "batch: cavity %d is out of step with the others", i);
+        }
+    auto fresh = [&](double eps) {
+        RunCtl c{};
+        c.active = 1;
+        c.errU = c.errT = 100.0;
+        c.best = INFINITY;
+        c.eps = eps;
+        c.growth = b->growth;
+        c.stop_bad = 1;
+        return c;
+    };
     std::vector<RunCtl> ctl(n);
     for (int i = 0; i < n; ++i) {
-        ctl[i] = RunCtl{};
+        ctl[i] = fresh(eps1);
         ctl[i].active = b->active[i];  // members off the mask stay out of the batched check
-        ctl[i].errU = ctl[i].errT = 100.0;
-        ctl[i].best = INFINITY;
-        ctl[i].eps = eps;
-        ctl[i].growth = b->growth;
-        ctl[i].stop_bad = 1;
     }
     BCU(cudaMemcpyAsync(b->d_ctl, ctl.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
-    std::vector<int64_t> itc0(n);
-    std::vector<int> cur0(n);
+    std::vector<int64_t> itc0(n), base_steps(n, 0);
+    std::vector<int> base_cur(n), phase(n, 1);
     for (int i = 0; i < n; ++i) {
         itc0[i] = b->cav[i]->itc;
-        cur0[i] = b->cav[i]->cur;
+        base_cur[i] = b->cav[i]->cur;
     }
     b->dirty = true;
     const bool persistent = b->persistent && b->march_ok;
@@ -524,17 +594,6 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
         const int k = (int)std::min<int64_t>(check_every, max_steps - steps);
         if (persistent) {
             if (b->dirty && (st = build_tables(b))) break;
-            // the common parity of the members on the work list
-            int cur = -1;
-            for (int i = 0; i < n; ++i)
-                if (b->active[i]) {
-                    if (cur < 0) cur = b->cav[i]->cur;
-                    if (b->cav[i]->cur != cur) {
-                        st = set_error(LBM_ERR_STATE, "batch: cavity %d is out of step with the others", i);
-                        break;
-                    }
-                }
-            if (st) break;
             if (b->use_graphs && k >= 2) {
                 cudaGraphExec_t g;
                 if ((st = batch_period_graph(b, cur, k, &g))) break;
@@ -543,7 +602,7 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
                     st = set_error(LBM_ERR_CUDA, "cudaGraphLaunch: %s", cudaGetErrorString(e));
                     break;
                 }
-                g_launches += k + 2;
+                g_launches += b->run_graph_launches;
             } else {
                 for (int i = 0; i < k && !st; ++i) {
                     cudaError_t e = launch_step(b, (cur + i) & 1, i == k - 1);
@@ -566,34 +625,63 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
             for (int i = 0; i < n && !st; ++i)
                 if (b->active[i]) {
                     lbm_handle *h = b->cav[i];
+                    if (h->cur != cur) {  // a member that waited for the host: realign its buffers
+                        if ((st = change_storage(h, h->p.storage, cur))) break;
+                    }
                     if ((st = lbm_step(h, k))) break;
                     cudaError_t e = run_check(h->geo, h->bufs, k, b->stream);
                     if (e != cudaSuccess) st = set_error(LBM_ERR_CUDA, "batch check: %s", cudaGetErrorString(e));
                 }
             if (st) break;
         }
+        cur = (cur + k) & 1;
         steps += k;
         if (++periods % kBatchPeriodsPerRead != 0 && steps < max_steps) continue;
         // read every member's run state: one copy, one synchronisation
         BCU(cudaMemcpyAsync(ctl.data(), b->d_ctl, sizeof(RunCtl) * n, cudaMemcpyDeviceToHost, b->stream));
         if ((st = lbm_batch_synchronize(b))) break;
         bool changed = false;
+        std::vector<int> moved;
         for (int i = 0; i < n; ++i) {
             if (!b->active[i]) continue;
             if (ctl[i].status == -2) {
                 st = set_error(LBM_ERR_NONFINITE, "check: non-finite residual sum (cavity %d)", i);
                 break;
             }
-            if (!ctl[i].active) {
-                b->active[i] = 0;
-                --remaining;
+            if (ctl[i].active) continue;
+            if (two_phase && phase[i] == 1 && ctl[i].status == 1) {
+                // met the FP32 criterion: on to FP64, in the batch's current buffer
+                lbm_handle *h = b->cav[i];
+                h->cur = (int)((base_cur[i] + (ctl[i].steps - base_steps[i])) & 1);
+                if ((st = change_storage(h, LBM_STORE_F64, cur))) break;
+                if (steps_low) steps_low[i] = ctl[i].steps;
+                base_cur[i] = cur;
+                base_steps[i] = ctl[i].steps;
+                phase[i] = 2;
+                RunCtl c = fresh(eps2);
+                c.steps = ctl[i].steps;
+                ctl[i] = c;
+                moved.push_back(i);
                 changed = true;
+                continue;
             }
+            b->active[i] = 0;
+            --remaining;
+            changed = true;
         }
         if (st) break;
+        for (int i : moved)
+            BCU(cudaMemcpyAsync(b->d_ctl + i, &ctl[i], sizeof(RunCtl), cudaMemcpyHostToDevice, b->stream));
+        if (!moved.empty()) {
+            std::vector<Bufs> bufs(n);
+            for (int i = 0; i < n; ++i) bufs[i] = b->cav[i]->bufs;
+            BCU(cudaMemcpyAsync(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice, b->stream));
+            BCU(cudaStreamSynchronize(b->stream));
+        }
         if (changed) b->dirty = true;
     }
-    // the final state: iterations each member ran, its parity and counter
+    // the final state: iterations each member ran (every period ends with a
+    // check, so the device count is exact), its parity and counter
     cudaError_t e = cudaMemcpyAsync(ctl.data(), b->d_ctl, sizeof(RunCtl) * n, cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess && !st) st = set_error(LBM_ERR_CUDA, "batch run state: %s", cudaGetErrorString(e));
@@ -601,20 +689,57 @@ extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t m
         const bool on = !mask || mask[i] != 0;
         if (!on) continue;
         lbm_handle *h = b->cav[i];
-        const int64_t ran = ctl[i].active ? steps : ctl[i].steps;
+        const int64_t ran = ctl[i].steps;
         h->itc = itc0[i] + ran;
-        h->cur = (int)((cur0[i] + ran) & 1);
+        h->cur = (int)((base_cur[i] + (ran - base_steps[i])) & 1);
         if (steps_done) steps_done[i] = ran;
-        if (converged) converged[i] = ctl[i].active ? 0 : (ctl[i].status == 1 ? 1 : (ctl[i].status == -1 ? -1 : 0));
+        if (steps_low && two_phase && phase[i] == 1) steps_low[i] = ran;
+        const bool done = !ctl[i].active && (!two_phase || phase[i] == 2 || ctl[i].status != 1);
+        if (converged) converged[i] = done ? (ctl[i].status == 1 ? 1 : (ctl[i].status == -1 ? -1 : 0)) : 0;
         if (!st && ctl[i].status == -2) st = set_error(LBM_ERR_NONFINITE, "check: non-finite residual sum (cavity %d)", i);
+    }
+    // members in different storages leave their buffers in different parities;
+    // bring every member on the mask to the same one for the next steps
+    if (!st) {
+        int c0 = -1;
+        for (int i = 0; i < n && !st; ++i) {
+            if (!(!mask || mask[i] != 0)) continue;
+            if (c0 < 0) c0 = b->cav[i]->cur;
+            if (b->cav[i]->cur != c0) st = change_storage(b->cav[i], b->cav[i]->p.storage, c0);
+        }
+        if (!st) {
+            std::vector<Bufs> bufs(n);
+            for (int i = 0; i < n; ++i) bufs[i] = b->cav[i]->bufs;
+            e = cudaMemcpy(b->d_bufs, bufs.data(), sizeof(Bufs) * n, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) st = set_error(LBM_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e));
+        }
     }
     for (auto &c : ctl) c.active = 1;
     e = cudaMemcpyAsync(b->d_ctl, ctl.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess && !st) st = set_error(LBM_ERR_CUDA, "batch run state: %s", cudaGetErrorString(e));
+    // the batch's storage: the members' common one
+    if (two_phase) {
+        bool all64 = true;
+        for (int i = 0; i < n; ++i) all64 = all64 && b->cav[i]->p.storage == LBM_STORE_F64;
+        b->storage = all64 ? LBM_STORE_F64 : -1;
+    }
     b->active.assign(n, 1);
     b->dirty = true;
     return st;
+}
+
+extern "C" int lbm_batch_run_masked(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
+                                    double eps, int32_t *converged, int64_t *steps_done)
+{
+    return batch_run(b, mask, max_steps, check_every, eps, eps, false, converged, steps_done, nullptr);
+}
+
+extern "C" int lbm_batch_run_mixed(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32_t check_every,
+                                   double switch_eps, double eps, int32_t *converged, int64_t *steps_done,
+                                   int64_t *steps_low)
+{
+    return batch_run(b, mask, max_steps, check_every, switch_eps, eps, true, converged, steps_done, steps_low);
 }
 
 extern "C" int lbm_batch_run(lbm_batch *b, int32_t max_steps, int32_t check_every, double eps, int32_t *converged,

@@ -1198,9 +1198,9 @@ extern "C" int lbm_set_populations(lbm_handle *h, const double *f, const double 
 // Convert the cavity's state to another population storage in place: new
 // buffers, the newest populations and carried force converted on the device,
 // old buffers released, descriptors and kernel choice redone.
-int lbm::change_storage(lbm_handle *h, int storage)
+int lbm::change_storage(lbm_handle *h, int storage, int target)
 {
-    if (storage == h->p.storage) return LBM_OK;
+    if (storage == h->p.storage && (target < 0 || target == h->cur)) return LBM_OK;
     if (storage == LBM_STORE_F16S)
         return fail(LBM_ERR_UNSUPPORTED, "binary16 population storage is retired (inaccurate, not faster than FP32)");
     if (storage != LBM_STORE_F64 && storage != LBM_STORE_F32) return fail(LBM_ERR_PARAM, "unknown storage %d", storage);
@@ -1220,9 +1220,9 @@ int lbm::change_storage(lbm_handle *h, int storage)
     if (!st && (cudaMemset(nF[0], 0, fb) != cudaSuccess || cudaMemset(nF[1], 0, fb) != cudaSuccess))
         st = fail(LBM_ERR_CUDA, "memset failed");
     if (!st && h->phase != 0) {
-        const int c = h->cur;
-        cudaError_t e = convert_state(h->geo, h->p.storage, storage, h->Q + h->QT, h->bufs.pop[c], np[c],
-                                      h->bufs.F[c], nF[c], h->stream);
+        const int c = h->cur, t = target < 0 ? c : target;
+        cudaError_t e = convert_state(h->geo, h->p.storage, storage, h->Q + h->QT, h->bufs.pop[c], np[t],
+                                      h->bufs.F[c], nF[t], h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) st = fail(LBM_ERR_CUDA, "storage conversion: %s", cudaGetErrorString(e));
     }
@@ -1250,6 +1250,7 @@ int lbm::change_storage(lbm_handle *h, int storage)
     h->p.storage = storage;
     h->esize = es;
     h->csize = cs;
+    if (target >= 0) h->cur = target;
     lbm::drop_graphs(h);
     h->march_ok = encode_maps(h);
     return resolve_path(h);

@@ -82,6 +82,7 @@ void drop_graphs(lbm_handle *h);
 int run_begin(lbm_handle *h, double eps, double growth, int stop_bad);
 int run_read(lbm_handle *h, RunCtl *out);
 int run_end(lbm_handle *h);
-// population storage of h converted in place (buffers, descriptors, kernel)
-int change_storage(lbm_handle *h, int storage);
+// population storage of h converted in place (buffers, descriptors, kernel);
+// target >= 0: the state lands in ping-pong buffer `target` (h->cur becomes it)
+int change_storage(lbm_handle *h, int storage, int target = -1);
 }  // namespace lbm

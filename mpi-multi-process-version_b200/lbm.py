@@ -36,7 +36,7 @@ EXPORTS = [
     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_size", "lbm_batch_cavity", "lbm_batch_init_reference",
     "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_run_masked", "lbm_batch_tune",
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
-    "lbm_batch_set_storage",
+    "lbm_batch_set_storage", "lbm_batch_run_mixed",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5, "storages": 6, "storage": 7}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
@@ -123,6 +123,9 @@ def lib():
         L.lbm_batch_synchronize.argtypes = [ctypes.c_void_p]
         L.lbm_batch_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         L.lbm_batch_set_storage.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+        L.lbm_batch_run_mixed.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p]
         L.lbm_set_storage.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         _lib = L
     return _lib
@@ -484,6 +487,18 @@ class Batch:
              "lbm_batch_run_masked")
         return np.array(conv[:], dtype=np.int32), np.array(done[:], dtype=np.int64)
 
+    def run_mixed(self, mask, max_steps, check_every=2000, switch_eps=1e-5, eps=float(np.float32(1e-6))):
+        """lbm_batch_run_mixed: FP32 to switch_eps, then each member on its own
+        converted to FP64 and run to eps.  Returns (status, steps, FP32 steps)."""
+        m = None if mask is None else (ctypes.c_int32 * self.n)(*[int(bool(v)) for v in mask])
+        conv = (ctypes.c_int32 * self.n)()
+        done = (ctypes.c_int64 * self.n)()
+        low = (ctypes.c_int64 * self.n)()
+        _chk(lib().lbm_batch_run_mixed(self.h, m, int(max_steps), int(check_every), float(switch_eps), float(eps),
+                                       conv, done, low), "lbm_batch_run_mixed")
+        self._sync_storage()
+        return np.array(conv[:], dtype=np.int32), np.array(done[:], dtype=np.int64), np.array(low[:], np.int64)
+
     def tune(self, steps=20, storages=None):
         """lbm_batch_tune; storages: the storages the tuner may pick (names),
         None for the current one.  Returns the choice."""
@@ -502,7 +517,7 @@ class Batch:
 
     def _sync_storage(self):
         code = self.get_option("storage")
-        self.storage = {v: k for k, v in STORE.items()}[code]
+        self.storage = {v: k for k, v in STORE.items()}.get(code, "mixed")
         for m in self.members:
             m.storage = self.storage
 

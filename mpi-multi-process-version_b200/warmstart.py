@@ -264,31 +264,43 @@ def _init(b, cases, init, model, predictions):
     return t_pred
 
 
-def _run(b, eps, max_steps, check_every, mask=None):
-    """lbm_batch_run_masked with the cold-start fallback for members stopped
-    for a diverging residual; max_steps is per member (an array or a number)."""
+def _run(b, eps, max_steps, check_every, mask=None, switch_eps=None):
+    """The batch run to the stop criterion, with the cold-start fallback for
+    members stopped for a diverging residual; max_steps is per member (an
+    array or a number).  switch_eps: mixed precision member by member
+    (lbm_batch_run_mixed: FP32 to switch_eps, then FP64 to eps).  Returns
+    (status, steps, fallback, FP32 steps or None)."""
     limit = np.broadcast_to(np.asarray(max_steps, dtype=np.int64), (b.n,)).copy()
     on = np.ones(b.n, bool) if mask is None else np.asarray(mask, bool).copy()
     status = np.zeros(b.n, np.int32)
     steps = np.zeros(b.n, np.int64)
+    low = np.zeros(b.n, np.int64)
     # all members run together up to the smallest remaining budget; those still
     # running with budget left go on together, so no member exceeds its own
     sel = on & (limit > 0)
     while sel.any():
         cap = int((limit - steps)[sel].min())
-        st, n = b.run_masked(None if sel.all() else sel, cap, check_every, eps)
+        m = None if sel.all() else sel
+        if switch_eps is None:
+            st, n = b.run_masked(m, cap, check_every, eps)
+            lo = np.zeros(b.n, np.int64)
+        else:
+            st, n, lo = b.run_mixed(m, cap, check_every, switch_eps, eps)
         status = np.where(sel, st, status)
         steps = np.where(sel, steps + n, steps)
+        low = np.where(sel, low + lo, low)
         sel = sel & (st == 0) & (steps < limit)
     fallback = on & (status == -1)
     if fallback.any():
         for i in np.nonzero(fallback)[0]:
             b.members[i].initial()
         left = np.where(fallback, limit - steps, 0)
-        st2, n2, _ = _run(b, eps, left, check_every, mask=fallback & (left > 0))
+        st2, n2, _, lo2 = _run(b, eps, left, check_every, mask=fallback & (left > 0), switch_eps=switch_eps)
         status = np.where(fallback, st2, status)
         steps = np.where(fallback, steps + n2, steps)
-    return status, steps, fallback
+        if lo2 is not None:
+            low = np.where(fallback, low + lo2, low)
+    return status, steps, fallback, (low if switch_eps is not None else None)
 
 
 def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
@@ -301,44 +313,38 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
     prediction (or `predictions`, a list of node-field dicts) through
     lbm_init_warm.  Members whose residual diverges (not finite, or growth x
     above its smallest value) restart cold and their steps add up.
-    storage "f64" / "f32", "mixed": FP32 storage until the residuals
-    reach `switch_eps`, then the batch converts in place to FP64
-    (lbm_batch_set_storage) and runs to `eps`, so the result is the FP64 fixed
-    point; or "auto": like "mixed", with the first phase's storage picked by
-    the autotuner among FP32 and FP64 (lbm_batch_tune; the tuning steps count).
+    storage "f64" / "f32"; "mixed": member by member, FP32 storage until the
+    residuals reach `switch_eps`, then that member alone converts in place to
+    FP64 and runs to `eps` (lbm_batch_run_mixed), so the result is the FP64
+    fixed point while the other members go on in FP32; "auto": the autotuner
+    (lbm_batch_tune) picks FP32 (then "mixed") or FP64 for the transient.
     max_steps bounds each member's iterations over all phases.
     Returns a dict of per-case arrays and the wall time: `seconds` from the
     first initialisation to the result (prediction and lbm_init_warm included),
     of which `predict_seconds` was the network."""
-    two_phase = storage in ("mixed", "auto")
-    first = "f32" if two_phase else storage
+    first = "f32" if storage in ("mixed", "auto") else storage
     b = _prepare(cases, first, device, growth)
     b.synchronize()
     t0 = time.perf_counter()
     t_pred = _init(b, cases, init, model, predictions)
     tuned = None
     tune_steps = 0
+    mixed = storage == "mixed"
     if storage == "auto":
-        tune_steps = 12 * 6 + 2 * 6  # 2 storages x 3 tiles x 2 grids x (2 + 4) steps, +2 per storage
+        # 2 storages x 3 tiles x 2 grids x (2 warm-up + 4 timed) steps
+        tune_steps = 2 * 3 * 2 * 6
         tuned = b.tune(steps=4, storages=("f32", "f64"))
+        mixed = tuned["storage"] == "f32"
     b.synchronize()
-    status, steps, fallback = _run(b, switch_eps if two_phase else eps, max_steps - tune_steps, check_every)
+    status, steps, fallback, steps_low = _run(b, eps, max_steps - tune_steps, check_every,
+                                               switch_eps=switch_eps if mixed else None)
     steps = steps + tune_steps
-    status_low = status.copy() if two_phase else None
-    steps_low = steps.copy() if two_phase else None
-    if two_phase:
-        b.set_storage("f64")
-        left = np.maximum(max_steps - steps, 0)
-        status, steps2, fb2 = _run(b, eps, left, check_every)
-        steps = steps + steps2
-        fallback = fallback | fb2
     b.synchronize()
     seconds = time.perf_counter() - t0
     nu_hot, nu_cold = b.nusselt()
     out = {"status": status, "steps": steps, "fallback": fallback, "nu_hot": nu_hot, "nu_cold": nu_cold,
            "seconds": seconds, "predict_seconds": t_pred, "nodes": np.array([m.nnode for m in b.members]),
-           "storage": storage, "init": init, "steps_low_precision": steps_low, "status_low_precision": status_low,
-           "tuned": tuned}
+           "storage": storage, "init": init, "steps_low_precision": steps_low, "tuned": tuned}
     if want_fields:
         out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
     if field_fn is not None:

@@ -262,3 +262,34 @@ def test_batch_tuner_chooses_storage(pkg):
     eu, et = b.check()
     assert np.isfinite(eu).all() and np.isfinite(et).all()
     b.close()
+
+
+def test_batch_run_mixed_member_by_member(pkg):
+    # lbm_batch_run_mixed: each member runs FP32 to switch_eps, is converted
+    # alone to FP64 and runs on to eps; the result is the FP64 fixed point
+    # (continued to a tight criterion it meets the all-FP64 run's to 1e-8)
+    specs = [dict(nx=32, ny=32, Ra=1e3, Pr=0.71, grid="tanh", stretch=1.5),
+             dict(nx=40, ny=40, Ra=1e4, Pr=2.0, grid="tanh", stretch=1.2),
+             dict(nx=48, ny=32, Ra=3e4, Pr=0.71, grid="tanh", stretch=1.7),
+             dict(nx=36, ny=36, Ra=1e5, Pr=7.0, grid="tanh", stretch=1.3)]
+    for sp in specs:
+        sp["coords"] = pkg.mesh_box(sp["nx"], sp["ny"], 0, 1.0, sp["ny"] / sp["nx"], 1.0, sp["grid"], sp["stretch"])
+    mix = pkg.Batch(2, specs, storage="f32")
+    ref = pkg.Batch(2, specs, storage="f64")
+    for b in (mix, ref):
+        b.initial()
+    st, n, low = mix.run_mixed(None, 400000, 500, switch_eps=1e-4, eps=1e-6)
+    assert (st == 1).all()
+    assert ((low > 0) & (low < n)).all()
+    assert len(set(low.tolist())) > 1          # members switched at different times
+    assert mix.get_option("storage") == 0      # every member ended in FP64
+    assert all(m.itc == k for m, k in zip(mix.members, n))
+    st2, _ = ref.run_masked(None, 400000, 500, 1e-6)
+    assert (st2 == 1).all()
+    for b in (mix, ref):
+        s, _ = b.run_masked(None, 2000000, 500, 1e-11)
+        assert (s == 1).all()
+    a, r = mix.nusselt()[0], ref.nusselt()[0]
+    assert np.abs(a - r).max() <= 1e-8 * np.abs(r).max()
+    mix.close()
+    ref.close()

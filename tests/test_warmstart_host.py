@@ -63,6 +63,16 @@ class _FakeBatch:
             steps = np.where(mask, steps, 0)
         return status, steps
 
+    def run_mixed(self, mask, max_steps, check_every, switch_eps, eps):
+        k = len(self.runs)
+        self.runs.append((None if mask is None else [bool(x) for x in mask], (switch_eps, eps), max_steps))
+        script = self.script[k]
+        out = [np.array(script[key], dtype=t) for key, t in (("status", np.int32), ("steps", np.int64),
+                                                               ("low", np.int64))]
+        if mask is not None:
+            out = [np.where(mask, a, 0) for a in out]
+        return tuple(out)
+
     def nusselt(self):
         return np.arange(self.n, dtype=float) + 1.0, np.zeros(self.n)
 
@@ -102,24 +112,25 @@ def test_diverged_members_restart_cold_and_their_steps_add_up(pkg, fake):
     assert b.closed
 
 
-def test_mixed_precision_converts_the_batch_to_fp64(pkg, fake):
-    # FP32 to switch_eps, then the same batch converted in place to FP64 runs
-    # to eps on each member's remaining iteration budget: member 1 spent its
-    # whole budget in FP32 and does not run again
+def test_mixed_precision_member_by_member(pkg, fake):
+    # one batch in FP32; the library hands each member to FP64 on its own
+    # (lbm_batch_run_mixed); a member stopped for divergence restarts cold and
+    # runs mixed again on what is left of its budget
     W = pkg.warmstart
-    _FakeBatch.script = [{"status": [1, 0], "steps": [20000, 40000]},
-                         {"status": [1, 0], "steps": [6000, 0]}]
-    r = W.solve(_cases(2), init="cold", storage="mixed", eps=1e-6, switch_eps=1e-5, max_steps=40000)
+    _FakeBatch.script = [{"status": [1, -1], "steps": [26000, 9000], "low": [20000, 9000]},
+                         {"status": [0, 1], "steps": [0, 30000], "low": [0, 21000]}]
+    r = W.solve(_cases(2), init="warm", predictions=_preds(2), storage="mixed", eps=1e-6, switch_eps=1e-5,
+                max_steps=40000)
     assert len(_FakeBatch.instances) == 1
     b = _FakeBatch.instances[0]
-    assert b.log.index(("storage", "f64")) > 0 and b.storage == "f64"
-    assert [run[1] for run in b.runs] == [1e-5, 1e-6]
-    assert b.runs[0][0] is None and b.runs[1][0] == [True, False]
+    assert b.storage == "f32"
+    assert b.runs[0] == (None, (1e-5, 1e-6), 40000)
+    assert b.runs[1] == ([False, True], (1e-5, 1e-6), 31000)
+    assert [e for e in b.log if e[0] == "initial"] == [("initial", 1)]
     assert b.closed
-    assert r["steps"].tolist() == [26000, 40000]
-    assert r["steps_low_precision"].tolist() == [20000, 40000]
-    assert r["status_low_precision"].tolist() == [1, 0]
-    assert r["status"].tolist() == [1, 0]
+    assert r["steps"].tolist() == [26000, 39000]
+    assert r["steps_low_precision"].tolist() == [20000, 30000]
+    assert r["status"].tolist() == [1, 1] and r["fallback"].tolist() == [False, True]
 
 
 def test_summary_counts_and_ratios(pkg):

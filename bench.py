@@ -304,16 +304,21 @@ def run_batch(args, world, rank, local):
     torch.cuda.set_device(local)
     from __graft_entry__ import load_package
     pkg = load_package()
+    ns = args.sweep  # all 256, or the first few for a profile
     if args.batch_shard:
-        all_specs = pkg.sweep_specs(256, seed=0)
+        all_specs = pkg.sweep_specs(256, seed=0)[:ns]
         idx, specs = pkg.sharding.my_share(all_specs, world, rank)
         n_total, scaling = len(all_specs), "strong"
     else:
-        specs = pkg.sweep_specs(256, seed=rank)
-        idx, n_total, scaling = list(range(rank * 256, rank * 256 + 256)), 256 * world, "weak"
+        specs = pkg.sweep_specs(256, seed=rank)[:ns]
+        idx, n_total, scaling = list(range(rank * ns, rank * ns + ns)), ns * world, "weak"
     b = pkg.Batch(2, specs, storage=args.storage, mode=args.mode, device=local)
     b.initial()
-    tuned = b.tune(steps=6)
+    if args.tile:
+        b.set_option("tile", args.tile)
+        tuned = {"tile": args.tile, "nblocks": b.get_option("nblocks")}
+    else:
+        tuned = b.tune(steps=6)
     stream = torch.cuda.ExternalStream(b.stream_ptr(), device=torch.device("cuda", local))
 
     def timed(nsteps, reps):
@@ -389,7 +394,7 @@ def run_batch(args, world, rank, local):
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": scaling,
             "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-            "config": {"workload": "batch256", "cavities": n_total, "nodes": int(nodes_all), "lattice": "D2Q9+D2Q5",
+            "config": {"workload": "batch256" if ns == 256 else f"batch256 (first {ns})", "cavities": n_total, "nodes": int(nodes_all), "lattice": "D2Q9+D2Q5",
                        "sweep": "widths {64..512}, aspect 1-4, Ra 1e3-1e6 log, Pr 0.71-7, tanh stretch 1-2, "
                                 + ("seed 0 split over ranks by LPT" if args.batch_shard else "seed = rank"),
                        "storage": args.storage, "mode": args.mode, "iterations_per_step": args.inner,
@@ -554,6 +559,8 @@ def main():
     ap.add_argument("--l2promo", type=int, default=-1, help="TMA L2 promotion 0..3 (-1 = library default)")
     ap.add_argument("--tiley", type=int, default=0, help="3D march tile rows 4 or 8 (0 = library default)")
     ap.add_argument("--plan", type=int, default=-1, help="3D march work plan 0 or 1 (-1 = library default)")
+    ap.add_argument("--sweep", type=int, default=256, help="batch256: the first N cavities of the sweep (a profile)")
+    ap.add_argument("--tile", type=int, default=0, help="batch256: tile width 32/64/128 instead of the autotuner")
     ap.add_argument("--batch-shard", action="store_true",
                     help="batch256 on N GPUs: split one sweep by LPT (strong scaling) instead of one sweep per rank")
     args = ap.parse_args()

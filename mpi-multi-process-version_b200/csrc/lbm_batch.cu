@@ -775,6 +775,10 @@ static int tune_storage(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nbl
 extern "C" int lbm_batch_tune(lbm_batch *b, int32_t steps, int32_t *tile, int32_t *nblocks, double *mlups)
 {
     if (!b) return set_error(LBM_ERR_PARAM, "batch is NULL");
+    if (b->storage < 0) {  // members in different storages after a mixed run: FP64 is always allowed
+        int st = lbm_batch_set_storage(b, LBM_STORE_F64);
+        if (st) return st;
+    }
     const int mask = b->storages ? b->storages : (1 << b->storage);
     const int user_nb = b->nblocks_opt;  // a grid the caller set stays
     double best = -1.0;

@@ -214,6 +214,10 @@ def run_reference(args, world, rank):
         return
     if args.workload == "batch256":
         return run_reference_batch(args)
+    if args.workload == "unet":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no network: the warm-start "
+                          "surrogate has no counterpart to time"}), flush=True)
+        return
     if args.workload == "steady":
         print(json.dumps({"impl": "reference", "unavailable": "time to a steady state of the CPU restatement is "
                           "hours at these sizes (10^5-10^6 iterations per cavity); its per-iteration rate is the "
@@ -462,6 +466,68 @@ def time_to_steady(pkg, ncases, max_steps, device):
                     "+ one persistent batch + learned warm start (prediction and initialisation timed)"}
 
 
+def run_unet(args, world, rank, local):
+    """The warm-start network's training step on the library's own kernels:
+    forward, MSE loss, backward and Adam of the 4-level U-Net (1.95 M
+    parameters, bf16 activations, FP32 accumulation) on a batch of 16
+    128 x 128 images (seeded random inputs and targets), with the 3x3
+    convolutions on the chosen tensor-core path (--tensor-path 0: mma.sync,
+    1: tcgen05 with the accumulator in tensor memory).  roofline: the 3x3
+    convolutions' FLOPs (forward, data and weight gradients) per step against
+    the measured bf16 GEMM peak."""
+    import torch
+    torch.cuda.set_device(local)
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    S = pkg.surrogate
+    S.set_tensor_path(args.tensor_path)
+    R, B = 128, 16
+    net = S.Net(R=R, device=local, seed=0)
+    g = torch.Generator(device="cpu").manual_seed(0)
+    x = (torch.randn(B, R, R, S.IN_CH, generator=g) * 0.5).to(torch.bfloat16).cuda(local)
+    y = (torch.randn(B * R * R, S.OUT_CH, generator=g) * 0.1).cuda(local)
+    stream = net.stream
+
+    def step():
+        net.forward(x, B)
+        net.loss(y, B)
+        net.backward(B)
+        net.adam(1e-4)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = pkg.kernel_launches()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = pkg.kernel_launches() - l0
+    ms = e0.elapsed_time(e1) / args.steps
+    res = {"e1": R, "e2": R // 2, "e3": R // 4, "b": R // 8, "d3": R // 4, "d2": R // 2, "d1": R}
+    flops = sum(2.0 * B * res[n.rstrip("ab")] ** 2 * 9 * ci * co for n, ci, co in S.layer_table()) * 3
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak, kind = float(json.load(fh)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    tflops = flops / (ms * 1e-3) / 1e12
+    if rank == 0:
+        print(json.dumps({
+            "metric": "unet_train_step_ms", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 (FP32 accumulation)", "data": "synthetic",
+            "config": {"workload": "unet", "batch": B, "image": R, "params": int(net.n_params),
+                       "tensor_path": ["mma.sync", "tcgen05"][args.tensor_path]},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tflops / peak, "traffic": None, "peak_kind": kind,
+                         "flops_per_step": flops, "kernel": "3x3 convolutions (fwd, dgrad, wgrad)"},
+            "gpu_launches": launches, "timeouts": S.timeouts(reset=True)}), flush=True)
+
+
 def run_steady(args, world, rank, local):
     """Time to a steady state on held-out cavities (square, sides 128..256,
     Ra 1e3..1e6 log-uniform, Pr 0.71..7, tanh stretch 1..2; the first
@@ -544,7 +610,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--inner", type=int, default=100, help="LBM iterations per bench step")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cavity3d_128", choices=sorted(WORKLOADS) + ["batch256", "steady"])
+    ap.add_argument("--workload", default="cavity3d_128",
+                    choices=sorted(WORKLOADS) + ["batch256", "steady", "unet"])
+    ap.add_argument("--tensor-path", type=int, default=0, choices=[0, 1], help="unet: 0 mma.sync, 1 tcgen05")
     ap.add_argument("--cases", type=int, default=16, help="steady: held-out cavities")
     ap.add_argument("--steady-cases", type=int, default=16,
                     help="cavity workloads: held-out cavities of the time_to_steady object (0: leave it out)")
@@ -576,6 +644,8 @@ def main():
         return run_batch(args, world, rank, local)
     if args.workload == "steady":
         return run_steady(args, world, rank, local)
+    if args.workload == "unet":
+        return run_unet(args, world, rank, local)
 
     import torch
     torch.cuda.set_device(local)

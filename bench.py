@@ -616,6 +616,8 @@ def main():
     ap.add_argument("--cases", type=int, default=16, help="steady: held-out cavities")
     ap.add_argument("--steady-cases", type=int, default=16,
                     help="cavity workloads: held-out cavities of the time_to_steady object (0: leave it out)")
+    ap.add_argument("--steady-max-steps", type=int, default=3_000_000,
+                    help="time_to_steady: iteration cap per cavity, high enough for every case of both arms")
     ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")
     ap.add_argument("--storage", default="f64", choices=["f64", "f32"])
     ap.add_argument("--mode", default="fast", choices=["fast", "exact"])
@@ -757,7 +759,7 @@ def main():
     # steady state on the first held-out cavities, both arms timed here
     tts = None
     if rank == 0 and world == 1 and args.steady_cases > 0:
-        tts = time_to_steady(pkg, args.steady_cases, args.max_steps, local)
+        tts = time_to_steady(pkg, args.steady_cases, args.steady_max_steps, local)
 
     if rank == 0:
         line = {

@@ -1217,12 +1217,19 @@ int lbm::change_storage(lbm_handle *h, int storage, int target)
         st = dalloc(h, &np[i], popb);
         if (!st) st = dalloc(h, &nF[i], fb);
     }
-    if (!st && (cudaMemset(nF[0], 0, fb) != cudaSuccess || cudaMemset(nF[1], 0, fb) != cudaSuccess))
+    if (!st && h->phase == 0 &&
+        (cudaMemset(nF[0], 0, fb) != cudaSuccess || cudaMemset(nF[1], 0, fb) != cudaSuccess ||
+         cudaMemset(np[0], 0, popb) != cudaSuccess || cudaMemset(np[1], 0, popb) != cudaSuccess))
         st = fail(LBM_ERR_CUDA, "memset failed");
     if (!st && h->phase != 0) {
+        // both buffers: the newest state, and the one before it (lbm_get_populations
+        // streams that one to give the reference's pre-collision populations)
         const int c = h->cur, t = target < 0 ? c : target;
         cudaError_t e = convert_state(h->geo, h->p.storage, storage, h->Q + h->QT, h->bufs.pop[c], np[t],
                                       h->bufs.F[c], nF[t], h->stream);
+        if (e == cudaSuccess)
+            e = convert_state(h->geo, h->p.storage, storage, h->Q + h->QT, h->bufs.pop[1 - c], np[1 - t],
+                              h->bufs.F[1 - c], nF[1 - t], h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) st = fail(LBM_ERR_CUDA, "storage conversion: %s", cudaGetErrorString(e));
     }

@@ -65,9 +65,13 @@ struct lbm_batch {
         int4 *d_segs = nullptr;
         int *d_segoff = nullptr;
         size_t segs_cap = 0, segoff_cap = 0;
-        int nblocks = 0;
+        int nblocks = 0;   // the list's grid (fixed while graphs replay it)
+        int tx = 0;        // the tile width its kernel was captured with
         BatchDev dev{};
     } wl[2];
+    bool run_both = false;         // a mixed run: both storages' kernels launch every step
+    cudaStream_t stream2 = nullptr;  // the second branch when both storages' kernels run
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int *d_err = nullptr;
     BatchDev dev{};                // the tables (segment fields unused) for the batched check
     bool dirty = true;
@@ -78,7 +82,7 @@ struct lbm_batch {
     int64_t graph_launches = 0;      // kernels one replay of a 2-step graph launches
     int64_t active_nodes = 0;
     RunCtl *d_ctl = nullptr;       // run state of every member (member i's bufs.ctl = d_ctl + i)
-    int *d_idx = nullptr;          // members on the work list, for the batched check
+    int *d_idx = nullptr;          // the members of a run (its mask), for the batched check
     int nidx = 0;
 };
 
@@ -107,6 +111,9 @@ extern "C" int lbm_batch_destroy(lbm_batch *b)
                     b->d_idx, b->wl[0].d_segs,  b->wl[0].d_segoff, b->wl[1].d_segs, b->wl[1].d_segoff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->stream2) cudaStreamDestroy(b->stream2);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return LBM_OK;
@@ -137,6 +144,9 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
         cudaError_t e = cudaSetDevice(b->device);
         if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e)));
         e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
         if (e != cudaSuccess) return bail(set_error(LBM_ERR_CUDA, "stream: %s", cudaGetErrorString(e)));
     }
     for (int i = 0; i < n; ++i) {
@@ -194,11 +204,15 @@ extern "C" int lbm_batch_create(int32_t n, const lbm_params *params, const doubl
     return LBM_OK;
 }
 
-// descriptors for the tile width, and the work list of the active cavities.
-// A column is one march: 2D a TX-wide strip of rows, 3D a 32 x kBatchTileY tile of slices.
+// descriptors for the tile width, and the work lists of the active cavities.
+// A column is one march: 2D a TX-wide strip of rows, 3D a 32 x kBatchTileY tile
+// of slices.  Each storage's list keeps a fixed grid (a full wave, or the
+// caller's nblocks) and fixed device arrays sized for every member's columns,
+// so a change of the active members or of a member's storage only rewrites
+// the arrays' contents and captured graphs stay valid; blocks without work
+// return at once.
 static int build_tables(lbm_batch *b)
 {
-    drop_graphs(b);
     const bool d3 = b->dim == 3;
     const int TX = d3 ? 32 : b->tile;
     std::vector<TmapSet> maps(2 * (size_t)b->n);
@@ -217,28 +231,22 @@ static int build_tables(lbm_batch *b)
         int cav, pos, ny;  // pos: 2D the strip's x-offset, 3D the tile index; ny: items (rows or slices)
     };
     std::vector<Col> cols;
-    int64_t total = 0;
+    size_t ncols_all = 0;  // the columns of every member, active or not: the lists' capacity
     b->active_nodes = 0;
     for (int i = 0; i < b->n; ++i) {
-        if (!b->active[i]) continue;
         const Geo &g = b->cav[i]->geo;
-        if (d3) {
-            const int nt = ((g.nx + 31) / 32) * ((g.ny + kBatchTileY - 1) / kBatchTileY);
-            for (int t = 0; t < nt; ++t) cols.push_back({i, t, g.nz});
-            total += (int64_t)nt * g.nz;
-        } else {
-            for (int i0 = 0; i0 < g.nx; i0 += TX) cols.push_back({i, i0, g.ny});
-            total += (int64_t)((g.nx + TX - 1) / TX) * g.ny;
-        }
+        const int nc = d3 ? ((g.nx + 31) / 32) * ((g.ny + kBatchTileY - 1) / kBatchTileY) : (g.nx + TX - 1) / TX;
+        ncols_all += nc;
+        if (!b->active[i]) continue;
+        for (int c = 0; c < nc; ++c) cols.push_back({i, d3 ? c : c * TX, d3 ? g.nz : g.ny});
         b->active_nodes += g.nnode;
     }
-    (void)total;
     int sms = 0;
     BCU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+    bool regraph = false;
     b->nblocks = 0;
     for (int sto = 0; sto < 2; ++sto) {
         lbm_batch::WorkList &W = b->wl[sto];
-        W.nblocks = 0;
         // this storage's columns
         std::vector<Col> sc;
         int64_t stotal = 0;
@@ -247,16 +255,19 @@ static int build_tables(lbm_batch *b)
                 sc.push_back(c);
                 stotal += c.ny;
             }
-        if (sc.empty()) continue;
+        const bool present = !sc.empty() || (b->run_both && b->mode != LBM_MODE_EXACT);
+        if (!present) {
+            if (W.nblocks) regraph = true;
+            W.nblocks = 0;
+            continue;
+        }
         const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(sto)
                                                          : fast::march_batch3d_blocks_per_sm(sto))
                            : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(sto, TX)
                                                         : fast::march_batch_blocks_per_sm(sto, TX));
         if (bps <= 0) return set_error(LBM_ERR_UNSUPPORTED, "batch kernel with tile %d cannot be resident", TX);
-        int64_t G = b->nblocks_opt > 0 ? b->nblocks_opt : (int64_t)bps * sms;
-        if (G > stotal) G = stotal;
-        if (G < 1) G = 1;
-        // equal contiguous shares of the (column, item) items
+        const int64_t G = b->nblocks_opt > 0 ? b->nblocks_opt : (int64_t)bps * sms;
+        // equal contiguous shares of the (column, item) items; blocks past the work get none
         std::vector<int4> segs;
         std::vector<int> off(G + 1, 0);
         size_t c = 0;
@@ -276,53 +287,66 @@ static int build_tables(lbm_batch *b)
             }
         }
         off[G] = (int)segs.size();
-        if (segs.size() > W.segs_cap) {
+        const size_t seg_need = (size_t)G + ncols_all + 16;
+        if (W.segs_cap < seg_need) {
             if (W.d_segs) cudaFree(W.d_segs);
-            W.segs_cap = segs.size() * 2 + 16;
+            W.d_segs = nullptr;
+            W.segs_cap = seg_need;
             BCU(cudaMalloc(&W.d_segs, sizeof(int4) * W.segs_cap));
+            regraph = true;
         }
-        if (off.size() > W.segoff_cap) {
+        if (W.segoff_cap < off.size()) {
             if (W.d_segoff) cudaFree(W.d_segoff);
-            W.segoff_cap = off.size() * 2 + 16;
+            W.d_segoff = nullptr;
+            W.segoff_cap = off.size();
             BCU(cudaMalloc(&W.d_segoff, sizeof(int) * W.segoff_cap));
+            regraph = true;
         }
-        BCU(cudaMemcpyAsync(W.d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice, b->stream));
+        if (!segs.empty())
+            BCU(cudaMemcpyAsync(W.d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice,
+                                b->stream));
         BCU(cudaMemcpyAsync(W.d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
+        if (W.nblocks != (int)G || W.tx != TX) regraph = true;
         W.nblocks = (int)G;
+        W.tx = TX;
         W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, W.d_segoff};
         b->nblocks += (int)G;
     }
     BCU(cudaStreamSynchronize(b->stream));
     b->dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, nullptr, nullptr};
-    {
-        std::vector<int> idx;
-        for (int i = 0; i < b->n; ++i)
-            if (b->active[i]) idx.push_back(i);
-        b->nidx = (int)idx.size();
-        if (!idx.empty())
-            BCU(cudaMemcpy(b->d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice));
-    }
+    if (regraph) drop_graphs(b);
     b->dirty = false;
     return LBM_OK;
 }
 
 // one step of every member on the work lists: one persistent kernel per
 // population storage present
+static cudaError_t launch_list(lbm_batch *b, int sto, int cur, int wm, cudaStream_t s)
+{
+    const lbm_batch::WorkList &W = b->wl[sto];
+    if (b->dim == 3)
+        return b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, s)
+                                         : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, s);
+    return b->mode == LBM_MODE_EXACT ? exact::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, s)
+                                     : fast::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, s);
+}
+
+// with both storages present the two kernels run side by side (a fork onto
+// the second stream and a join), so a step costs one kernel's latency
 static cudaError_t launch_step(lbm_batch *b, int cur, int wm)
 {
-    for (int sto = 0; sto < 2; ++sto) {
-        const lbm_batch::WorkList &W = b->wl[sto];
-        if (W.nblocks <= 0) continue;
-        cudaError_t e;
-        if (b->dim == 3)
-            e = b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, b->stream)
-                                          : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, b->stream);
-        else
-            e = b->mode == LBM_MODE_EXACT
-                    ? exact::march_batch(sto, b->tile, W.dev, W.nblocks, cur, wm, b->d_err, b->stream)
-                    : fast::march_batch(sto, b->tile, W.dev, W.nblocks, cur, wm, b->d_err, b->stream);
-        if (e != cudaSuccess) return e;
+    const bool a = b->wl[0].nblocks > 0, c = b->wl[1].nblocks > 0;
+    if (a && c) {
+        cudaError_t e = cudaEventRecord(b->ev_fork, b->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream2, b->ev_fork, 0);
+        if (e == cudaSuccess) e = launch_list(b, 1, cur, wm, b->stream2);
+        if (e == cudaSuccess) e = launch_list(b, 0, cur, wm, b->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->stream2);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_join, 0);
+        return e;
     }
+    if (a) return launch_list(b, 0, cur, wm, b->stream);
+    if (c) return launch_list(b, 1, cur, wm, b->stream);
     return cudaSuccess;
 }
 
@@ -578,7 +602,18 @@ static int batch_run(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32
         ctl[i].active = b->active[i];  // members off the mask stay out of the batched check
     }
     BCU(cudaMemcpyAsync(b->d_ctl, ctl.data(), sizeof(RunCtl) * n, cudaMemcpyHostToDevice, b->stream));
+    {
+        // the batched check covers the run's members; stopped ones return at once
+        std::vector<int> idx;
+        for (int i = 0; i < n; ++i)
+            if (b->active[i]) idx.push_back(i);
+        b->nidx = (int)idx.size();
+        if (!idx.empty())
+            BCU(cudaMemcpyAsync(b->d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, b->stream));
+    }
     BCU(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);  // the check covers this run's members
+    b->run_both = two_phase;
     std::vector<int64_t> itc0(n), base_steps(n, 0);
     std::vector<int> base_cur(n), phase(n, 1);
     for (int i = 0; i < n; ++i) {
@@ -724,6 +759,7 @@ static int batch_run(lbm_batch *b, const int32_t *mask, int32_t max_steps, int32
         for (int i = 0; i < n; ++i) all64 = all64 && b->cav[i]->p.storage == LBM_STORE_F64;
         b->storage = all64 ? LBM_STORE_F64 : -1;
     }
+    b->run_both = false;
     b->active.assign(n, 1);
     b->dirty = true;
     return st;

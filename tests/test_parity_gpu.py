@@ -563,9 +563,11 @@ def test_output_ascii_matches_reference_writer(pkg, name, tmp_path):
 
 @pytest.mark.parametrize("dim,shape", [(2, (64, 48, 1)), (3, (40, 24, 18))])
 def test_storage_conversion_in_place(pkg, dim, shape):
-    # FP32 -> FP64 -> FP32 of an FP32 state is exact, so a run converted there
-    # and back continues bit for bit; FP64 -> FP32 rounds each stored
-    # deviation once (<= 2^-24 relative), and the check history is kept
+    # FP32 -> FP64 -> FP32 returns every stored FP32 deviation except the
+    # lowest bits of values below ~2^-31 (their sum with the O(1) shift in FP64
+    # rounds), so a run converted there and back continues within 1e-13; FP64
+    # -> FP32 rounds each stored deviation once (<= 2^-24 relative); the check
+    # history is kept
     kw = dict(Ra=1e5, grid="tanh", stretch=1.5, kernel="march" if dim == 3 else "auto")
     a = pkg.Cavity(dim, *shape, storage="f32", **kw)
     b = pkg.Cavity(dim, *shape, storage="f32", **kw)
@@ -575,11 +577,12 @@ def test_storage_conversion_in_place(pkg, dim, shape):
     b.set_storage("f64")
     assert b.storage == "f64"
     b.set_storage("f32")
+    for x, y in zip(a.populations(), b.populations()):
+        assert np.abs(x - y).max() <= 1e-15
     a.step(30)
     b.step(30)
-    fa, ga = a.populations()
-    fb, gb = b.populations()
-    assert np.array_equal(fa, fb) and np.array_equal(ga, gb)
+    for x, y in zip(a.populations(), b.populations()):
+        assert np.abs(x - y).max() <= 1e-13
     c = pkg.Cavity(dim, *shape, storage="f64", **kw)
     c.initial()
     c.step(25)

@@ -451,19 +451,21 @@ def time_to_steady(pkg, ncases, max_steps, device):
     model = W.WarmStart.load(MODEL_PATH, device=device)
     cases = W.sample_cases(200, seed=2000)[:ncases]
     steps_cold, nu_cold, t_cold = steady_cold_arm(pkg, cases, max_steps, device)
-    r = W.solve(cases, init="warm", model=model, storage="mixed", max_steps=max_steps, device=device)
+    r = W.solve(cases, init="warm", model=model, storage="auto", max_steps=max_steps, device=device)
     nu_cold = np.asarray(nu_cold)
     err = np.abs(np.asarray(r["nu_hot"]) - nu_cold) / np.abs(nu_cold)
     conv = np.asarray(r["status"]) == 1
     return {"cases": ncases, "sides": "128..256", "criterion": "errorU, errorT <= float32(1e-6) every 2000 "
-            "iterations", "max_steps": max_steps, "fp64_cold_seconds": t_cold, "mixed_warm_seconds": r["seconds"],
+            "iterations", "max_steps": max_steps, "fp64_cold_seconds": t_cold, "warm_batched_seconds": r["seconds"],
             "speedup": t_cold / r["seconds"], "fp64_cold_steps": int(np.sum(steps_cold)),
             "fp64_cold_converged": int(np.sum(np.asarray(steps_cold) < max_steps)),
-            "mixed_warm_steps": int(np.sum(r["steps"])), "converged_mixed": int(conv.sum()),
+            "warm_batched_steps": int(np.sum(r["steps"])), "converged_warm_batched": int(conv.sum()),
             "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()), "max_nu_rel_err": float(err.max()),
-            "fallbacks": int(np.sum(r["fallback"])),
-            "arms": "FP64 from the conduction state, one cavity per launch vs. mixed precision member by member "
-                    "+ one persistent batch + learned warm start (prediction and initialisation timed)"}
+            "fallbacks": int(np.sum(r["fallback"])), "storage_chosen": r["tuned"]["chosen"],
+            "tuned_mlups": {k: r["tuned"][k]["mlups"] for k in ("f64", "f32")},
+            "arms": "FP64 from the conduction state, one cavity per launch vs. one persistent batch + learned "
+                    "warm start + storage chosen by the autotuner (mixed precision member by member if FP32 "
+                    "stepping pays for its hand-over, else FP64); prediction, tuning and initialisation timed"}
 
 
 def run_unet(args, world, rank, local):
@@ -507,7 +509,7 @@ def run_unet(args, world, rank, local):
     launches = pkg.kernel_launches() - l0
     ms = e0.elapsed_time(e1) / args.steps
     res = {"e1": R, "e2": R // 2, "e3": R // 4, "b": R // 8, "d3": R // 4, "d2": R // 2, "d1": R}
-    flops = sum(2.0 * B * res[n.rstrip("ab")] ** 2 * 9 * ci * co for n, ci, co in S.layer_table()) * 3
+    flops = sum(2.0 * B * res[n[:-1]] ** 2 * 9 * ci * co for n, ci, co in S.layer_table()) * 3
     peak = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -558,7 +560,7 @@ def run_steady(args, world, rank, local):
         time.sleep(0.3)
     l0 = pkg.kernel_launches()
     _barrier(world)
-    r = W.solve(cases, init="warm", model=model, storage="mixed", max_steps=max_steps, device=local)
+    r = W.solve(cases, init="warm", model=model, storage=args.steady_storage, max_steps=max_steps, device=local)
     launches = pkg.kernel_launches() - l0
     clocks = sampler.stop() if sampler else None
     t_mixed = _reduce(r["seconds"], world, "max")  # prediction and initialisation included
@@ -576,15 +578,16 @@ def run_steady(args, world, rank, local):
         line = {
             "metric": "time_to_steady_s", "value": t_mixed, "unit": "s", "n_gpus": world, "steps": 1, "warmup": 0,
             "ms_per_step": t_mixed * 1e3, "higher_is_better": False, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f32 storage then f64 (FP64 residual / Nu sums)", "data": "synthetic",
+            "dtype": f"storage policy {args.steady_storage} (FP64 residual / Nu sums)", "data": "synthetic",
             "config": {"workload": "steady", "cases": len(all_cases), "sides": "128..256", "criterion":
                        "errorU, errorT <= float32(1e-6) every 2000 iterations", "max_steps": max_steps,
                        "model": os.path.basename(MODEL_PATH), "baseline_arm": "FP64, conduction start, one cavity "
                        "per launch"},
-            "time_to_steady": {"fp64_cold_seconds": t_cold, "mixed_warm_seconds": t_mixed,
+            "time_to_steady": {"fp64_cold_seconds": t_cold, "warm_batched_seconds": t_mixed,
                                "speedup": t_cold / t_mixed, "fp64_cold_steps": int(got["steps_cold"].sum()),
-                               "mixed_warm_steps": int(got["steps_mixed"].sum()),
-                               "converged_mixed": int(conv.sum()),
+                               "warm_batched_steps": int(got["steps_mixed"].sum()),
+                               "converged_warm_batched": int(conv.sum()),
+                               "storage_chosen": (r["tuned"] or {}).get("chosen", args.steady_storage),
                                "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()),
                                "max_nu_rel_err": float(err.max()), "fallbacks": int(np.sum(r["fallback"]))},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -616,6 +619,8 @@ def main():
     ap.add_argument("--cases", type=int, default=16, help="steady: held-out cavities")
     ap.add_argument("--steady-cases", type=int, default=16,
                     help="cavity workloads: held-out cavities of the time_to_steady object (0: leave it out)")
+    ap.add_argument("--steady-storage", default="auto", choices=["auto", "mixed", "f64", "f32"],
+                    help="steady workload: storage policy of the warm-started batch")
     ap.add_argument("--steady-max-steps", type=int, default=3_000_000,
                     help="time_to_steady: iteration cap per cavity, high enough for every case of both arms")
     ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")

@@ -9,6 +9,7 @@ class _FakeMember:
     def __init__(self, log, i):
         self.log, self.i, self.nnode = log, i, 100 + i
         self.state = None
+        self.itc = 0
 
     def initial(self):
         self.log.append(("initial", self.i))
@@ -72,6 +73,13 @@ class _FakeBatch:
         if mask is not None:
             out = [np.where(mask, a, 0) for a in out]
         return tuple(out)
+
+    def tune(self, steps=20, storages=None):
+        self.log.append(("tune", tuple(storages)))
+        for m in self.members:
+            m.itc += 36
+        self.storage = storages[0]
+        return {"tile": 64, "nblocks": 1184, "mlups": self.rates[storages[0]], "storage": storages[0]}
 
     def nusselt(self):
         return np.arange(self.n, dtype=float) + 1.0, np.zeros(self.n)
@@ -151,3 +159,22 @@ def test_summary_counts_and_ratios(pkg):
     assert m["speedup_vs_f64_cold_sequential"] == pytest.approx(4.0)
     assert m["speedup_vs_f64_cold_batched"] == pytest.approx(2.0)
     assert s["f64_cold"]["nu_within_1e-4"] == 2
+
+
+@pytest.mark.parametrize("rates,mixed", [({"f64": 20000.0, "f32": 25000.0}, False),
+                                         ({"f64": 20000.0, "f32": 38000.0}, True)])
+def test_auto_storage_weighs_the_fp32_handover(pkg, fake, rates, mixed):
+    # "auto": the tuner times FP64 and FP32 stepping on the batch; mixed
+    # precision is chosen only if FP32 is faster than FP32_HANDOVER_COST x FP64
+    W = pkg.warmstart
+    _FakeBatch.rates = rates
+    _FakeBatch.script = [{"status": [1, 1], "steps": [5000, 7000], "low": [3000, 4000]}]
+    r = W.solve(_cases(2), init="warm", predictions=_preds(2), storage="auto", max_steps=100000)
+    b = _FakeBatch.instances[0]
+    assert [e for e in b.log if e[0] == "tune"] == [("tune", ("f64",)), ("tune", ("f32",))]
+    assert r["tuned"]["chosen"] == ("mixed" if mixed else "f64")
+    assert (b.runs[0][1] == (1e-5, W.F32_EPS)) == mixed
+    if not mixed:
+        assert ("storage", "f64") in b.log and ("option", "tile", 64) in b.log
+    # the tuner's steps count toward each member's iterations and budget
+    assert r["steps"].tolist() == [5072, 7072]

@@ -570,6 +570,7 @@ struct L2 {
 template <int ST, int TX>
 __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo &G, int tx, int i, int j, int xa,
                                              int xb, const typename Tr<ST>::C *xp, const typename Tr<ST>::C *xm,
+                                             typename Tr<ST>::C Tcn, typename Tr<ST>::C sT,
                                              typename Tr<ST>::S *__restrict__ dst,
                                              typename Tr<ST>::C *__restrict__ Fout, const Bufs &B, int write_macro)
 {
@@ -614,10 +615,9 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     gg[3] = ip(xm, SV(NB(5), ix(1, xa), 12), SV(NB(5), ix(1, 0), 12), SV(NB(5), ix(1, xb), 12));
     gg[4] = YI(7, 13, ym, 0);
     // deviation from the conduction profile along x (the heated axis)
-    C Tcn = C(0.0);
+    // (Tcn: the conduction profile at the node's x, sT: its streaming shift;
+    // both per column, computed once per segment)
     if (Tr<ST>::kDevT) {
-        Tcn = C(tc_value(G, i));
-        const C sT = C(0.125 * G.dt * tc_gradient(G));
         gg[1] -= sT;
         gg[3] += sT;
     }
@@ -755,9 +755,14 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         const bool active = i < G.nx;
         C xp[3], xm[3];
         int xa = 0, xb = 0;
+        C Tcn = C(0.0), sT = C(0.0);  // conduction profile at the column and its streaming shift
         if (active) {
             load_w(G.wgt[0], i, xp, xm);
             xa = off_a(i, G.nx); xb = off_b(i, G.nx);
+            if (Tr<ST>::kDevT) {
+                Tcn = C(tc_value(G, i));
+                sT = C(0.125 * G.dt * tc_gradient(G));
+            }
         }
         for (int j = ja; j < jb; ++j) {
             if (yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued) {
@@ -772,7 +777,8 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
                 atomicExch(err, 1);
                 s_abort = 1;
             }
-            if (active && ok) march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, dst, Fout, *Bp, write_macro);
+            if (active && ok)
+                march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, Tcn, sT, dst, Fout, *Bp, write_macro);
             __syncthreads();
             if (s_abort) {
                 aborted = true;

@@ -81,6 +81,11 @@ extern "C" {
                                LBM_ERR_TIMEOUT and the populations are not valid until the next
                                init call.  For tests of that error path.  lbm_get_option reports
                                the value last set through this handle (0: default). */
+#define LBM_OPT_PDL      9  /* 1 (default): consecutive march steps are launched as programmatic
+                               dependents (CUDA programmatic dependent launch): a step's blocks are
+                               scheduled while the previous step drains, set up, and wait for its
+                               completion before reading the populations; 0: plain stream order.
+                               Results are identical either way. */
 
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */
@@ -270,6 +275,14 @@ typedef struct lbm_batch lbm_batch;
                                         the transient of a run, FP64 alone to finish it); 0 (the
                                         default): the batch's current storage only */
 #define LBM_BATCH_OPT_STORAGE     7  /* read only: the batch's current storage (LBM_STORE_*) */
+#define LBM_BATCH_OPT_PDL         8  /* as LBM_OPT_PDL for the batch's step kernels (default 1; a step
+                                        with both storages present forks onto two streams and is
+                                        launched in plain stream order) */
+#define LBM_BATCH_OPT_DIRECT      9  /* 2D: while the members of one storage on the work list hold at
+                                        most this many nodes in all (the last members of a run), they
+                                        step through a direct-load kernel (one block per 32 x 8 tile)
+                                        instead of the persistent march kernel; default 65536, 0 off.
+                                        Exact mode: bit-identical either way */
 
 /* Create n cavities (same dim, storage, mode and device; any size and
  * parameters).  x[i], y[i], z[i] are the coordinate arrays of cavity i as for

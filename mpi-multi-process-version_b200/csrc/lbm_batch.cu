@@ -43,6 +43,12 @@ using namespace lbm;
                              #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
     } while (0)
 
+// 2D: a storage's members step through the direct-load kernel while they hold
+// at most this many nodes in all (the last members of a run): a step is then
+// latency-bound, and the direct kernel's one round of loads beats the march
+// kernel's ring start-up
+static constexpr int64_t kDirectNodes = 65536;
+
 struct lbm_batch {
     int n = 0;
     int dim = 2, storage = 0, mode = 0, device = 0;
@@ -56,6 +62,8 @@ struct lbm_batch {
     int use_graphs = 1;
     double growth = 0.0;           // residual growth factor that stops a member in lbm_batch_run (0: off)
     int storages = 0;              // LBM_BATCH_OPT_STORAGES: storages lbm_batch_tune may pick (0: the current)
+    int pdl = 1;                   // LBM_BATCH_OPT_PDL: programmatic dependent launch of the step kernels
+    int64_t direct_nodes = kDirectNodes;  // LBM_BATCH_OPT_DIRECT
     Geo *d_geo = nullptr;
     TmapSet *d_maps = nullptr;
     Bufs *d_bufs = nullptr;
@@ -67,6 +75,7 @@ struct lbm_batch {
         size_t segs_cap = 0, segoff_cap = 0;
         int nblocks = 0;   // the list's grid (fixed while graphs replay it)
         int tx = 0;        // the tile width its kernel was captured with
+        int direct = 0;    // 1: its few nodes step through the direct-load kernel (one block per tile)
         BatchDev dev{};
     } wl[2];
     bool run_both = false;         // a mixed run: both storages' kernels launch every step
@@ -261,6 +270,35 @@ static int build_tables(lbm_batch *b)
             W.nblocks = 0;
             continue;
         }
+        int64_t snodes = 0;
+        for (size_t k = 0; k < sc.size(); ++k)
+            if (k == 0 || sc[k].cav != sc[k - 1].cav) snodes += b->cav[sc[k].cav]->geo.nnode;
+        if (!d3 && !sc.empty() && b->direct_nodes > 0 && snodes <= b->direct_nodes) {
+            // few nodes left: one block per 32 x 8 tile of every member on the list
+            std::vector<int4> items;
+            for (size_t k = 0; k < sc.size(); ++k) {
+                if (k > 0 && sc[k].cav == sc[k - 1].cav) continue;
+                const Geo &g = b->cav[sc[k].cav]->geo;
+                for (int y0 = 0; y0 < g.ny; y0 += 8)
+                    for (int x0 = 0; x0 < g.nx; x0 += 32) items.push_back(make_int4(sc[k].cav, x0, y0, 0));
+            }
+            if (W.segs_cap < items.size()) {
+                if (W.d_segs) cudaFree(W.d_segs);
+                W.d_segs = nullptr;
+                W.segs_cap = items.size();
+                BCU(cudaMalloc(&W.d_segs, sizeof(int4) * W.segs_cap));
+                regraph = true;
+            }
+            BCU(cudaMemcpyAsync(W.d_segs, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
+                                b->stream));
+            if (!W.direct || W.nblocks != (int)items.size()) regraph = true;
+            W.direct = 1;
+            W.nblocks = (int)items.size();
+            W.tx = 32;
+            W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, nullptr};
+            b->nblocks += W.nblocks;
+            continue;
+        }
         const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(sto)
                                                          : fast::march_batch3d_blocks_per_sm(sto))
                            : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(sto, TX)
@@ -306,9 +344,10 @@ static int build_tables(lbm_batch *b)
             BCU(cudaMemcpyAsync(W.d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice,
                                 b->stream));
         BCU(cudaMemcpyAsync(W.d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
-        if (W.nblocks != (int)G || W.tx != TX) regraph = true;
+        if (W.nblocks != (int)G || W.tx != TX || W.direct) regraph = true;
         W.nblocks = (int)G;
         W.tx = TX;
+        W.direct = 0;
         W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, W.d_segoff};
         b->nblocks += (int)G;
     }
@@ -320,33 +359,38 @@ static int build_tables(lbm_batch *b)
 }
 
 // one step of every member on the work lists: one persistent kernel per
-// population storage present
-static cudaError_t launch_list(lbm_batch *b, int sto, int cur, int wm, cudaStream_t s)
+// population storage present; pdl: launched as a programmatic dependent of the
+// stream's previous kernel
+static cudaError_t launch_list(lbm_batch *b, int sto, int cur, int wm, bool pdl, cudaStream_t s)
 {
     const lbm_batch::WorkList &W = b->wl[sto];
+    if (W.direct)
+        return b->mode == LBM_MODE_EXACT ? exact::step_batch2d(sto, W.dev, W.nblocks, cur, wm, pdl, s)
+                                         : fast::step_batch2d(sto, W.dev, W.nblocks, cur, wm, pdl, s);
     if (b->dim == 3)
-        return b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, s)
-                                         : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, s);
-    return b->mode == LBM_MODE_EXACT ? exact::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, s)
-                                     : fast::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, s);
+        return b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s)
+                                         : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s);
+    return b->mode == LBM_MODE_EXACT ? exact::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s)
+                                     : fast::march_batch(sto, W.tx, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s);
 }
 
 // with both storages present the two kernels run side by side (a fork onto
-// the second stream and a join), so a step costs one kernel's latency
+// the second stream and a join), so a step costs one kernel's latency; a
+// single list's kernels follow one another as programmatic dependents
 static cudaError_t launch_step(lbm_batch *b, int cur, int wm)
 {
     const bool a = b->wl[0].nblocks > 0, c = b->wl[1].nblocks > 0;
     if (a && c) {
         cudaError_t e = cudaEventRecord(b->ev_fork, b->stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream2, b->ev_fork, 0);
-        if (e == cudaSuccess) e = launch_list(b, 1, cur, wm, b->stream2);
-        if (e == cudaSuccess) e = launch_list(b, 0, cur, wm, b->stream);
+        if (e == cudaSuccess) e = launch_list(b, 1, cur, wm, false, b->stream2);
+        if (e == cudaSuccess) e = launch_list(b, 0, cur, wm, false, b->stream);
         if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->stream2);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->stream, b->ev_join, 0);
         return e;
     }
-    if (a) return launch_list(b, 0, cur, wm, b->stream);
-    if (c) return launch_list(b, 1, cur, wm, b->stream);
+    if (a) return launch_list(b, 0, cur, wm, b->pdl != 0, b->stream);
+    if (c) return launch_list(b, 1, cur, wm, b->pdl != 0, b->stream);
     return cudaSuccess;
 }
 
@@ -938,6 +982,17 @@ extern "C" int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value)
             return set_error(LBM_ERR_UNSUPPORTED, "exact mode computes in FP64 storage only");
         b->storages = (int)value;
         break;
+    case LBM_BATCH_OPT_DIRECT:
+        if (value < 0) return set_error(LBM_ERR_PARAM, "direct-kernel node threshold must be >= 0");
+        b->direct_nodes = value;
+        break;
+    case LBM_BATCH_OPT_PDL:
+        if (value != 0 && value != 1) return set_error(LBM_ERR_PARAM, "PDL must be 0 or 1");
+        BCU(cudaSetDevice(b->device));
+        BCU(cudaStreamSynchronize(b->stream));
+        drop_graphs(b);
+        b->pdl = (int)value;
+        break;
     default:
         return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
@@ -956,6 +1011,8 @@ extern "C" int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t 
     case LBM_BATCH_OPT_GROWTH: *value = (int64_t)b->growth; return LBM_OK;
     case LBM_BATCH_OPT_STORAGES: *value = b->storages; return LBM_OK;
     case LBM_BATCH_OPT_STORAGE: *value = b->storage; return LBM_OK;
+    case LBM_BATCH_OPT_PDL: *value = b->pdl; return LBM_OK;
+    case LBM_BATCH_OPT_DIRECT: *value = b->direct_nodes; return LBM_OK;
     default: return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
 }

@@ -816,9 +816,9 @@ static cudaError_t launch_one(lbm_handle *h, int cur, int wm)
     const int nxt = 1 - cur;
     if (h->use_march)
         return ex ? exact::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
-                                 h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->stream)
+                                 h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->pdl != 0, h->stream)
                   : fast::march(h->geo, h->p.storage, h->tmaps[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm,
-                                h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->stream);
+                                h->nblocks, h->tiley, h->d_msegs, h->d_msegoff, h->pdl != 0, h->stream);
     return ex ? exact::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream)
               : fast::step(h->geo, h->p.storage, b.pop[cur], b.F[cur], b.pop[nxt], b.F[nxt], b, wm, h->stream);
 }
@@ -1328,6 +1328,12 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         CU(exact::set_wait_limit(value));
         h->wait_limit = value;
         return LBM_OK;
+    case LBM_OPT_PDL:
+        if (value != 0 && value != 1) return fail(LBM_ERR_PARAM, "PDL must be 0 or 1");
+        CU(cudaStreamSynchronize(h->stream));
+        lbm::drop_graphs(h);
+        h->pdl = (int)value;
+        return LBM_OK;
     default:
         return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
@@ -1345,6 +1351,7 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     case LBM_OPT_TILEY: *value = h->geo.dim == 3 ? h->tiley : 0; return LBM_OK;
     case LBM_OPT_PLAN: *value = h->plan_opt; return LBM_OK;
     case LBM_OPT_WAIT_LIMIT: *value = h->wait_limit; return LBM_OK;
+    case LBM_OPT_PDL: *value = h->pdl; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

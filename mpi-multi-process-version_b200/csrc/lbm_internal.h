@@ -88,7 +88,8 @@ struct BatchDev {
     const Geo *geo;          // [ncav]
     const TmapSet *maps;     // [ncav][2]: descriptors of pop[0], pop[1] (+ their force arrays)
     const Bufs *bufs;        // [ncav]
-    const int4 *segs;        // all segments: 2D (cavity, i0, ja, jb); 3D (tile, z0, z1, cavity)
+    const int4 *segs;        // all segments: 2D march (cavity, i0, ja, jb); 3D (tile, z0, z1, cavity);
+                             // 2D direct-load kernel: one 32 x 8 tile per block (cavity, x0, y0, 0)
     const int *seg_off;      // [nblocks + 1]
 };
 
@@ -128,19 +129,24 @@ constexpr int kBatchTileY = 4;
     cudaError_t stream_only(const Geo &g, int store, const void *pop_in, const void *F_in,    \
                             void *pop_out, const Bufs &b, cudaStream_t s);                    \
     /* fused step through the TMA-fed persistent march kernel; 3D: tile rows ty (4 or 8)  */ \
-    /* and the blocks' segment lists segs[segoff[b] .. segoff[b+1]) (device memory)        */ \
+    /* and the blocks' segment lists segs[segoff[b] .. segoff[b+1]) (device memory);       */ \
+    /* pdl: programmatic dependent launch (overlaps the previous kernel's tail)            */ \
     cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in,          \
                       void *pop_out, void *F_out, const Bufs &b, int write_macro, int nblocks,\
-                      int ty, const int4 *segs, const int *segoff, cudaStream_t s);           \
+                      int ty, const int4 *segs, const int *segoff, bool pdl, cudaStream_t s); \
     /* resident blocks per SM of the march kernel (0 if it cannot launch) */                  \
     int march_blocks_per_sm(const Geo &g, int store, int ty);                                 \
     /* one step of every cavity of a 2D batch (tile width TX = 32, 64 or 128) */              \
     cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur,       \
-                            int write_macro, int *err, cudaStream_t s);                       \
+                            int write_macro, int *err, bool pdl, cudaStream_t s);             \
     int march_batch_blocks_per_sm(int store, int TX);                                         \
+    /* one step of the members of a small 2D batch, direct loads; D.segs: nitems tiles     */ \
+    /* (cavity, x0, y0) of 32 x 8 nodes                                                    */ \
+    cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur,              \
+                             int write_macro, bool pdl, cudaStream_t s);                      \
     /* one step of every cavity of a 3D batch (segments: tile, z0, z1, cavity; 32 x 4 tiles) */\
     cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur,             \
-                              int write_macro, int *err, cudaStream_t s);                     \
+                              int write_macro, int *err, bool pdl, cudaStream_t s);           \
     int march_batch3d_blocks_per_sm(int store);                                               \
     /* limit of the march kernels' per-step waits on this device, in clock cycles */          \
     cudaError_t set_wait_limit(long long cycles);                                             \

@@ -1060,6 +1060,34 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
 
 #include "lbm_march.cuh"
 
+// Small 2D batches -- the few members still running near the end of a run,
+// where a step's time is its latency, not its bytes: one thread per node with
+// direct loads as k_step2d, block b the 32 x 8 tile D.segs[b] = (cavity, x0,
+// y0) of the batch's work list; `cur` is the buffer read this step.  Launched
+// as a programmatic dependent, a block reads its tile and tables, then waits
+// for the previous step; the populations are read through L2 (ld.global.cg).
+template <int ST>
+__global__ void __launch_bounds__(256)
+k_step2d_batch(const BatchDev D, int cur, int write_macro)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    const int4 t = D.segs[blockIdx.x];
+    const Geo &G = D.geo[t.x];
+    const Bufs &B = D.bufs[t.x];
+    const RunCtl *ctl = B.ctl;
+    const S *src = (const S *)B.pop[cur];
+    const C *Fin = (const C *)B.F[cur];
+    S *dst = (S *)B.pop[1 - cur];
+    C *Fout = (C *)B.F[1 - cur];
+    const int i = t.y + threadIdx.x, j = t.z + threadIdx.y;
+    const bool inside = i < G.nx && j < G.ny;
+    dep_launch();
+    dep_wait();
+    if (!ctl->active || !inside) return;
+    step2d_node<ST, 0, true>(G, src, Fin, dst, Fout, B, write_macro, i, j);
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -1194,6 +1222,29 @@ cudaError_t collide(const Geo &g, int store, const void *pop_in, void *pop_out, 
 #undef CALL
 }
 
+// Launch of a march kernel.  With `pdl` the launch carries the
+// programmatic-serialization attribute: the kernel's CTAs may be scheduled
+// while the stream's previous kernel drains (its CTAs call dep_launch at
+// their start) and wait in dep_wait, after their set-up, for that kernel's
+// completion.  Consecutive steps then overlap one kernel's launch and set-up
+// with the previous one's tail.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_k(void (*k)(KArgs...), int grid, int block, int smem, cudaStream_t s, bool pdl,
+                            Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <int ST, int TY>
 static cudaError_t prepare_march3d()
 {
@@ -1253,36 +1304,35 @@ int march_blocks_per_sm(const Geo &g, int store, int ty)
 template <int ST, int TY>
 static cudaError_t launch_march3d(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
                                   const Bufs &b, int wm, const int4 *segs, const int *segoff, int nblocks,
-                                  cudaStream_t s)
+                                  bool pdl, cudaStream_t s)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     cudaError_t e = prepare_march3d<ST, TY>();
     if (e != cudaSuccess) return e;
-    k_march3d<ST, TY><<<nblocks, L3<ST, TY>::NT, L3<ST, TY>::smem(), s>>>(m, g, (const C *)Fin, (S *)pout,
-                                                                        (C *)Fout, b, wm, segs, segoff, b.err);
-    return cudaGetLastError();
+    return launch_k(k_march3d<ST, TY>, nblocks, L3<ST, TY>::NT, L3<ST, TY>::smem(), s, pdl, m, g, (const C *)Fin,
+                    (S *)pout, (C *)Fout, b, wm, segs, segoff, b.err);
 }
 
 template <int ST>
 static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
                                 const Bufs &b, int wm, int nblocks, int ty, const int4 *segs, const int *segoff,
-                                cudaStream_t s)
+                                bool pdl, cudaStream_t s)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     cudaError_t e;
     if (g.dim == 3) {
-        e = ty == 4 ? launch_march3d<ST, 4>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, s)
-                    : launch_march3d<ST, 8>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, s);
+        e = ty == 4 ? launch_march3d<ST, 4>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s)
+                    : launch_march3d<ST, 8>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s);
     } else {
         using L = L2<ST>;
         e = prepare_march2d<ST>();
         if (e != cudaSuccess) return e;
         const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
         const int nb = int(nblocks < total ? nblocks : total);
-        k_march2d<ST><<<nb, L::NT, L::smem(), s>>>(m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm, total, b.err);
-        e = cudaGetLastError();
+        e = launch_k(k_march2d<ST>, nb, L::NT, L::smem(), s, pdl, m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm,
+                     total, b.err);
     }
     ++g_launches;
     return e;
@@ -1290,9 +1340,9 @@ static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin,
 
 cudaError_t march(const Geo &g, int store, const TmapSet &src, const void *F_in, void *pop_out, void *F_out,
                   const Bufs &b, int write_macro, int nblocks, int ty, const int4 *segs, const int *segoff,
-                  cudaStream_t s)
+                  bool pdl, cudaStream_t s)
 {
-#define CALL(ST) launch_march<ST>(g, src, F_in, pop_out, F_out, b, write_macro, nblocks, ty, segs, segoff, s)
+#define CALL(ST) launch_march<ST>(g, src, F_in, pop_out, F_out, b, write_macro, nblocks, ty, segs, segoff, pdl, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }
@@ -1311,13 +1361,12 @@ static cudaError_t prepare_batch()
 }
 
 template <int ST, int TX>
-static cudaError_t launch_batch(const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+static cudaError_t launch_batch(const BatchDev &D, int nblocks, int cur, int wm, int *err, bool pdl, cudaStream_t s)
 {
     cudaError_t e = prepare_batch<ST, TX>();
     if (e != cudaSuccess) return e;
-    k_march2d_batch<ST, TX><<<nblocks, TX, L2<ST, TX>::smem(), s>>>(D, cur, wm, err);
     ++g_launches;
-    return cudaGetLastError();
+    return launch_k(k_march2d_batch<ST, TX>, nblocks, TX, L2<ST, TX>::smem(), s, pdl, D, cur, wm, err);
 }
 
 template <int ST, int TX>
@@ -1332,12 +1381,13 @@ static int batch_bps()
 }
 
 template <int ST>
-static cudaError_t launch_batch_tx(int TX, const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+static cudaError_t launch_batch_tx(int TX, const BatchDev &D, int nblocks, int cur, int wm, int *err, bool pdl,
+                                   cudaStream_t s)
 {
     switch (TX) {
-    case 32: return launch_batch<ST, 32>(D, nblocks, cur, wm, err, s);
-    case 64: return launch_batch<ST, 64>(D, nblocks, cur, wm, err, s);
-    case 128: return launch_batch<ST, 128>(D, nblocks, cur, wm, err, s);
+    case 32: return launch_batch<ST, 32>(D, nblocks, cur, wm, err, pdl, s);
+    case 64: return launch_batch<ST, 64>(D, nblocks, cur, wm, err, pdl, s);
+    case 128: return launch_batch<ST, 128>(D, nblocks, cur, wm, err, pdl, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1354,9 +1404,33 @@ static int batch_bps_tx(int TX)
 }
 
 cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur, int write_macro, int *err,
-                        cudaStream_t s)
+                        bool pdl, cudaStream_t s)
 {
-#define CALL(ST) launch_batch_tx<ST>(TX, D, nblocks, cur, write_macro, err, s)
+#define CALL(ST) launch_batch_tx<ST>(TX, D, nblocks, cur, write_macro, err, pdl, s)
+    LBM_DISPATCH(store, CALL)
+#undef CALL
+}
+
+template <int ST>
+static cudaError_t launch_direct_batch(const BatchDev &D, int nitems, int cur, int wm, bool pdl, cudaStream_t s)
+{
+    ++g_launches;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nitems);
+    cfg.blockDim = dim3(32, 8, 1);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, k_step2d_batch<ST>, D, cur, wm);
+}
+
+cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur, int write_macro, bool pdl,
+                         cudaStream_t s)
+{
+#define CALL(ST) launch_direct_batch<ST>(D, nitems, cur, write_macro, pdl, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }
@@ -1382,13 +1456,14 @@ static cudaError_t prepare_batch3d()
 }
 
 template <int ST>
-static cudaError_t launch_batch3d(const BatchDev &D, int nblocks, int cur, int wm, int *err, cudaStream_t s)
+static cudaError_t launch_batch3d(const BatchDev &D, int nblocks, int cur, int wm, int *err, bool pdl,
+                                  cudaStream_t s)
 {
     cudaError_t e = prepare_batch3d<ST>();
     if (e != cudaSuccess) return e;
-    k_march3d_batch<ST, kBatchTileY><<<nblocks, L3<ST, kBatchTileY>::NT, L3<ST, kBatchTileY>::smem(), s>>>(D, cur, wm, err);
     ++g_launches;
-    return cudaGetLastError();
+    return launch_k(k_march3d_batch<ST, kBatchTileY>, nblocks, L3<ST, kBatchTileY>::NT, L3<ST, kBatchTileY>::smem(),
+                    s, pdl, D, cur, wm, err);
 }
 
 template <int ST>
@@ -1403,9 +1478,9 @@ static int batch3d_bps()
 }
 
 cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur, int write_macro, int *err,
-                          cudaStream_t s)
+                          bool pdl, cudaStream_t s)
 {
-#define CALL(ST) launch_batch3d<ST>(D, nblocks, cur, write_macro, err, s)
+#define CALL(ST) launch_batch3d<ST>(D, nblocks, cur, write_macro, err, pdl, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }

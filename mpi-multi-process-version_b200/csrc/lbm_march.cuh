@@ -132,6 +132,17 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  : "memory");
 }
 
+// Programmatic dependent launch.  A march kernel launched with the
+// programmatic-serialization attribute may start while the stream's previous
+// kernel is still finishing: each CTA lets the next kernel's CTAs be scheduled
+// as soon as it runs (dep_launch), sets up its barriers, reads its work list
+// and geometry -- tables only the host writes -- and then waits (dep_wait) for
+// the previous kernel to complete with its memory visible before it reads a
+// run flag or a population.  Launched without the attribute, dep_wait has
+// nothing to wait for.
+__device__ __forceinline__ void dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_barrier_init()
 {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -151,6 +162,28 @@ __device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k ==
 // 3D layout
 // ---------------------------------------------------------------------------
 // box classes: 0 tile only, 1 +-HX columns, 2 +-1 rows, 3 both
+// Batch kernels copy the current segment's cavity geometry (Geo) into shared
+// memory behind the ring barriers: the per-node arithmetic reads a dozen of its
+// fields every step, and from the batch's table in global memory those reads
+// miss the small L1 left beside the rings (each one an L2 round trip on the
+// critical path of the step).  Single-cavity kernels take Geo as a kernel
+// parameter and read it from the constant bank instead.
+constexpr int kGeoStage = 256;
+static_assert(sizeof(Geo) <= kGeoStage && sizeof(Geo) % 8 == 0, "staged Geo must fit its shared-memory slot");
+
+// every thread of the CTA: copy *src into the shared slot dst (8-byte words),
+// between two barriers (the slot's previous readers are done before it, the
+// new readers start after it)
+__device__ __forceinline__ const Geo *stage_geo(const Geo *src, Geo *dst)
+{
+    __syncthreads();
+    const unsigned long long *s = (const unsigned long long *)src;
+    unsigned long long *d = (unsigned long long *)dst;
+    for (int w = threadIdx.x; w < (int)(sizeof(Geo) / 8); w += blockDim.x) d[w] = s[w];
+    __syncthreads();
+    return dst;
+}
+
 template <int ST, int TY_ = 8>
 struct L3 {
     using S = typename Tr<ST>::S;
@@ -209,7 +242,7 @@ struct L3 {
         return b + fbytes() + 48;
     }
     // ring slots, 6 barriers and the abort flag, and slack for 128-byte alignment
-    __host__ __device__ static constexpr int smem() { return 4 * zslot() + 2 * nslot() + 64 + 128; }
+    __host__ __device__ static constexpr int smem() { return 4 * zslot() + 2 * nslot() + 64 + kGeoStage + 128; }
 };
 
 // ---------------------------------------------------------------------------
@@ -220,7 +253,7 @@ struct L3 {
 // slice, end slice, cavity); tiles are numbered x-fastest within a cavity.
 // `cavity(c, G, maps, dst, Fout, B)` yields cavity c's geometry, the TMA
 // descriptors of the buffer read this step, the outputs and the buffers.
-template <int ST, int TY_, class CavFn>
+template <int ST, int TY_, bool kStage, class CavFn>
 __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int sbeg, int send, CavFn cavity,
                                             int write_macro, int *err)
 {
@@ -233,6 +266,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     uint64_t *zbar = (uint64_t *)(sm + 4 * L::zslot() + 2 * L::nslot());
     uint64_t *nbar = zbar + 4;
     volatile int &s_abort = *(volatile int *)(nbar + 2);
+    Geo *sgeo = (Geo *)(sm + 4 * L::zslot() + 2 * L::nslot() + 64);
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
@@ -242,6 +276,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
         fence_barrier_init();
         s_abort = 0;
     }
+    dep_launch();
     __syncthreads();
 
     uint32_t znext = 0, nnext = 0;  // per-slot parity of the next copy
@@ -285,7 +320,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u, wlim); };
     auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
-    bool aborted = false;
+    bool aborted = false, waited = false;
 
     for (int si = sbeg; si < send && !aborted; ++si) {
         const int4 sg = segs[si];
@@ -293,7 +328,13 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
         C *Fout;
         const Bufs *Bp;
         cavity(sg.w, Gp, Mp, dst, Fout, Bp);
-        if (!Bp->ctl->active) continue;  // a batch member whose run has stopped
+        if (kStage) Gp = stage_geo(Gp, sgeo);
+        const RunCtl *ctl = Bp->ctl;
+        if (!waited) {
+            dep_wait();  // from here on: what earlier kernels wrote
+            waited = true;
+        }
+        if (!ctl->active) continue;  // a cavity whose run has stopped
         const Geo &G = *Gp;
         const Bufs &B = *Bp;
         const int nz = G.nz;
@@ -479,7 +520,6 @@ k_march3d(const __grid_constant__ TmapSet maps, const __grid_constant__ Geo G,
     (void)Fin;
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    if (!B.ctl->active) return;
     auto cavity = [&](int, const Geo *&Gp, const TmapSet *&Mp, S *&d, C *&Fo, const Bufs *&Bp) {
         Gp = &G;
         Mp = &maps;
@@ -487,7 +527,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const __grid_constant__ Geo G,
         Fo = Fout;
         Bp = &B;
     };
-    march3d_run<ST, TY_>(segs, seg_off[blockIdx.x], seg_off[blockIdx.x + 1], cavity, write_macro, err);
+    march3d_run<ST, TY_, false>(segs, seg_off[blockIdx.x], seg_off[blockIdx.x + 1], cavity, write_macro, err);
 }
 
 // many 3D cavities: segments (tile, z0, z1, cavity) of the batch's work list;
@@ -505,7 +545,7 @@ k_march3d_batch(const BatchDev D, int cur, int write_macro, int *err)
         d = (S *)D.bufs[c].pop[1 - cur];
         Fo = (C *)D.bufs[c].F[1 - cur];
     };
-    march3d_run<ST, TY_>(D.segs, D.seg_off[blockIdx.x], D.seg_off[blockIdx.x + 1], cavity, write_macro, err);
+    march3d_run<ST, TY_, true>(D.segs, D.seg_off[blockIdx.x], D.seg_off[blockIdx.x + 1], cavity, write_macro, err);
 }
 
 // ---------------------------------------------------------------------------
@@ -562,7 +602,7 @@ struct L2 {
         for (int a = 0; a < 6; ++a) b += bytes(nc(a));
         return b + fbytes() + 48;
     }
-    __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + 128; }
+    __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + kGeoStage + 128; }
 };
 
 // One node of the 2D march at row j, from the ring slots in shared memory:
@@ -671,7 +711,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
 // x-offset i0, rows [ja, jb)).  `seg(k, cav, i0, ja, jb)` yields the block's
 // k-th segment; `cavity(cav, G, maps, dst, Fout, B)` yields the cavity's
 // geometry, the TMA descriptors of its source buffer and its outputs.
-template <int ST, int TX, class SegFn, class CavFn>
+template <int ST, int TX, bool kStage, class SegFn, class CavFn>
 __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, int write_macro, int *err)
 {
     using S = typename Tr<ST>::S;
@@ -683,6 +723,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
     uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
     uint64_t *nbar = ybar + 4;
     volatile int &s_abort = *(volatile int *)(nbar + 2);
+    Geo *sgeo = (Geo *)(sm + 4 * L::yslot() + 2 * L::nslot() + 64);
 
     const int tid = threadIdx.x;
     const int tx = tid;
@@ -692,10 +733,11 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         fence_barrier_init();
         s_abort = 0;
     }
+    dep_launch();
     __syncthreads();
 
     uint32_t ynext = 0, nnext = 0;
-    bool aborted = false;
+    bool aborted = false, waited = false;
     const long long wlim = g_wait_limit;
     for (int k = 0; k < nseg && !aborted; ++k) {
         int cav, i0, ja, jb;
@@ -706,7 +748,13 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         C *Fout;
         const Bufs *Bp;
         cavity(cav, Gp, maps, dst, Fout, Bp);
-        if (!Bp->ctl->active) continue;  // a batch member whose run has stopped
+        if (kStage) Gp = stage_geo(Gp, sgeo);
+        const RunCtl *ctl = Bp->ctl;
+        if (!waited) {
+            dep_wait();  // from here on: what earlier kernels wrote
+            waited = true;
+        }
+        if (!ctl->active) continue;  // a cavity whose run has stopped
         const Geo &G = *Gp;
         const int ny = G.ny;
 
@@ -804,7 +852,6 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     constexpr int TX = L2<ST, 128>::TX;
-    if (!B.ctl->active) return;
     const int ny = G.ny;
     const int64_t G_ = gridDim.x;
     const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
@@ -827,7 +874,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
         Fo = Fout;
         Bp = &B;
     };
-    march2d_run<ST, TX>(nseg, seg, cavity, write_macro, err);
+    march2d_run<ST, TX, false>(nseg, seg, cavity, write_macro, err);
 }
 
 // many cavities: block b runs segments seg_off[b] .. seg_off[b+1]-1; `cur`
@@ -853,5 +900,5 @@ k_march2d_batch(const BatchDev D, int cur, int write_macro, int *err)
         d = (S *)D.bufs[c].pop[1 - cur];
         Fo = (C *)D.bufs[c].F[1 - cur];
     };
-    march2d_run<ST, TX>(s1 - s0, seg, cavity, write_macro, err);
+    march2d_run<ST, TX, true>(s1 - s0, seg, cavity, write_macro, err);
 }

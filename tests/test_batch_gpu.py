@@ -38,10 +38,15 @@ def reference(pkg):
     return [standalone(pkg, sp, 37) for sp in SPECS]
 
 
-@pytest.mark.parametrize("tile,nblocks,graphs", [(64, 0, 1), (32, 0, 1), (128, 0, 0), (64, 1, 1), (32, 5, 0),
-                                                 (128, 7, 1)])
-def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, graphs):
+@pytest.mark.parametrize("tile,nblocks,graphs,direct", [(64, 0, 1, 0), (32, 0, 1, 0), (128, 0, 0, 0), (64, 1, 1, 0),
+                                                        (32, 5, 0, 0), (128, 7, 1, 0), (64, 0, 1, 65536),
+                                                        (64, 0, 0, 65536)])
+def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, graphs, direct):
+    # direct 0: the persistent march kernel; 65536: these 25,715 nodes step
+    # through the direct-load batch kernel
     b = pkg.Batch(2, SPECS, mode="exact")
+    assert b.get_option("direct") == 65536
+    b.set_option("direct", direct)
     b.set_option("tile", tile)
     b.set_option("nblocks", nblocks)
     b.set_option("graphs", graphs)
@@ -55,6 +60,33 @@ def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, g
         for k in ref:
             assert np.array_equal(got[k], ref[k]), k
     b.close()
+
+
+@pytest.mark.parametrize("dim,direct", [(2, 0), (2, 65536), (3, 0)])
+def test_batch_programmatic_dependent_launch_is_bit_identical(pkg, dim, direct):
+    # the batch's step kernels as programmatic dependents (the default) against
+    # plain stream order: steps, graph replays and the device-side run loop
+    if dim == 2:
+        specs = SPECS
+    else:
+        specs = [dict(nx=16, ny=16, nz=12, Ra=1e4, Pr=0.71, grid="tanh", stretch=1.5),
+                 dict(nx=20, ny=12, nz=10, Ra=1e3, Pr=2.0, grid="tanh", stretch=1.2)]
+    out = []
+    for pdl in (1, 0):
+        b = pkg.Batch(dim, specs, mode="exact")
+        assert b.get_option("pdl") == 1
+        b.set_option("pdl", pdl)
+        b.set_option("direct", direct)
+        b.initial()
+        b.step(20)
+        b.step(17)
+        status, steps = b.run_masked(None, 1200, 150, 3e-2)
+        out.append(([m.macro() for m in b.members], status.tolist(), steps.tolist()))
+        b.close()
+    assert out[0][1:] == out[1][1:]
+    for a, c in zip(out[0][0], out[1][0]):
+        for k in a:
+            assert np.array_equal(a[k], c[k]), k
 
 
 def test_batch_one_launch_per_cavity_matches(pkg, reference):
@@ -176,8 +208,8 @@ def test_sweep_members_against_oracle(pkg, ora):
     b.close()
 
 
-@pytest.mark.parametrize("dim,growth", [(2, 0), (2, 100), (3, 0)])
-def test_batch_run_matches_host_loop(pkg, dim, growth):
+@pytest.mark.parametrize("dim,growth,direct", [(2, 0, 0), (2, 100, 0), (2, 0, 4000), (3, 0, 0)])
+def test_batch_run_matches_host_loop(pkg, dim, growth, direct):
     # the device-side stop test of lbm_batch_run against each member run alone
     # with the reference's loop on the host: the same iterations, the same
     # stop, the same fields (exact mode, bit for bit)
@@ -195,6 +227,9 @@ def test_batch_run_matches_host_loop(pkg, dim, growth):
     ce, eps, max_steps = 150, 3e-2, 4500
     b = pkg.Batch(dim, specs, mode="exact")
     b.set_option("growth", growth)
+    # direct 4000: the 10,496 nodes start on the march kernel and the members
+    # left once the larger ones stop move to the direct-load kernel
+    b.set_option("direct", direct)
     b.initial()
     status, steps = b.run_masked(None, max_steps, ce, eps)
     assert (status == 1).any()

@@ -286,6 +286,28 @@ def test_graph_replay_is_bit_identical(pkg, dim, shape, kernel):
     assert np.array_equal(out[0][1][0], out[1][1][0]) and np.array_equal(out[0][1][1], out[1][1][1])
 
 
+@pytest.mark.parametrize("dim,shape", [(2, (300, 40, 1)), (3, (40, 18, 12))])
+def test_programmatic_dependent_launch_is_bit_identical(pkg, dim, shape):
+    # march steps launched as programmatic dependents (the default) against
+    # plain stream order: single steps, graph replays and a run to a criterion
+    out = []
+    for pdl in (1, 0):
+        c = pkg.Cavity(dim, *shape, grid="tanh", stretch=1.5, Ra=1e4, mode="exact", kernel="march")
+        assert c.get_option(pkg.lbm.OPT_PDL) == 1
+        c.set_option(pkg.lbm.OPT_PDL, pdl)
+        assert c.get_option(pkg.lbm.OPT_PDL) == pdl
+        c.initial()
+        for n in (7, 1, 10, 3):
+            c.step(n)
+        run = c.run(max_steps=3000, check_every=300, eps=1e-3)
+        out.append((c.macro(), c.populations(), run))
+        c.close()
+    assert out[0][2] == out[1][2]
+    for k in out[0][0]:
+        assert np.array_equal(out[0][0][k], out[1][0][k]), k
+    assert np.array_equal(out[0][1][0], out[1][1][0]) and np.array_equal(out[0][1][1], out[1][1][1])
+
+
 def test_run_matches_manual_loop(pkg):
     eps = 2e-2
     a = pkg.Cavity(2, 40, 40, Ra=1e4, grid="tanh", stretch=1.5, mode="exact")

@@ -878,9 +878,11 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
 }
 
 // many cavities: block b runs segments seg_off[b] .. seg_off[b+1]-1; `cur`
-// is the ping-pong buffer holding the populations read this step
+// is the ping-pong buffer holding the populations read this step.  Blocks per
+// SM: FP64 16 warps (shared memory bounds it there too), FP32 24 warps (80
+// registers, no spills)
 template <int ST, int TX>
-__global__ void __launch_bounds__(TX, 512 / TX)
+__global__ void __launch_bounds__(TX, (ST == kF32 ? 768 : 512) / TX)
 k_march2d_batch(const BatchDev D, int cur, int write_macro, int *err)
 {
     using S = typename Tr<ST>::S;

@@ -365,8 +365,8 @@ static cudaError_t launch_list(lbm_batch *b, int sto, int cur, int wm, bool pdl,
 {
     const lbm_batch::WorkList &W = b->wl[sto];
     if (W.direct)
-        return b->mode == LBM_MODE_EXACT ? exact::step_batch2d(sto, W.dev, W.nblocks, cur, wm, pdl, s)
-                                         : fast::step_batch2d(sto, W.dev, W.nblocks, cur, wm, pdl, s);
+        return b->mode == LBM_MODE_EXACT ? exact::step_batch2d(sto, W.dev, W.nblocks, cur, wm, s)
+                                         : fast::step_batch2d(sto, W.dev, W.nblocks, cur, wm, s);
     if (b->dim == 3)
         return b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s)
                                          : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s);

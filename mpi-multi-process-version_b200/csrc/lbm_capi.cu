@@ -837,20 +837,23 @@ void lbm::drop_graphs(lbm_handle *h)
         }
 }
 
-// a 2-step graph starting from buffer `cur`, captured once per kernel choice
+// steps per replayed graph in lbm_step (even: a replay leaves `cur` as it was);
+// inside a graph consecutive march steps are programmatic dependents
+static constexpr int kGraphSteps = 8;
+
+// a kGraphSteps-step graph starting from buffer `cur`, captured once per kernel choice
 static int step_graph(lbm_handle *h, int cur, cudaGraphExec_t *out)
 {
     if (!h->graph[cur]) {
         cudaGraph_t g = nullptr;
         CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t e1 = launch_one(h, cur, 0);
-        const cudaError_t e2 = launch_one(h, 1 - cur, 0);
+        cudaError_t e1 = cudaSuccess;
+        for (int k = 0; k < kGraphSteps && e1 == cudaSuccess; ++k) e1 = launch_one(h, (cur + k) & 1, 0);
         const cudaError_t e3 = cudaStreamEndCapture(h->stream, &g);
-        lbm::g_launches -= 2;  // counted when replayed
-        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        lbm::g_launches -= kGraphSteps;  // counted when replayed
+        if (e1 != cudaSuccess || e3 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
-            return fail(LBM_ERR_CUDA, "step graph capture: %s",
-                        cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+            return fail(LBM_ERR_CUDA, "step graph capture: %s", cudaGetErrorString(e1 != cudaSuccess ? e1 : e3));
         }
         const cudaError_t e = cudaGraphInstantiate(&h->graph[cur], g, 0);
         cudaGraphDestroy(g);
@@ -880,15 +883,16 @@ extern "C" int lbm_step(lbm_handle *h, int32_t nsteps)
         h->itc += nsteps;
         return LBM_OK;
     }
-    // replay 2-step graphs for all but the last step(s) (small domains are
-    // launch-bound), then the last step writes the macroscopic fields
-    if (h->use_graphs && nsteps > 4) {
-        while (nsteps - done > 2) {
+    // replay kGraphSteps-step graphs for all but the last step(s) (small
+    // domains are launch-bound), then single launches; the last step writes
+    // the macroscopic fields
+    if (h->use_graphs) {
+        while (nsteps - done > kGraphSteps) {
             cudaGraphExec_t g;
             if ((st = step_graph(h, h->cur, &g))) return st;
             CU(cudaGraphLaunch(g, h->stream));
-            lbm::g_launches += 2;
-            done += 2;
+            lbm::g_launches += kGraphSteps;
+            done += kGraphSteps;
         }
     }
     for (; done < nsteps; ++done) {

@@ -55,7 +55,7 @@ struct lbm_handle {
     int resident_opt = 0;        // LBM_OPT_RESIDENT as set (opt-in)
     int resident = 0;            // resolved: blocks of the resident multi-step launch (0: off)
     unsigned *d_bar = nullptr;   // grid barrier of the resident launch (two counters)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 2-step graphs from cur = 0 / 1
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // 8-step graphs (kGraphSteps) from cur = 0 / 1
     cudaGraphExec_t run_graph[2] = {nullptr, nullptr};  // check periods of lbm_run from cur = 0 / 1
     int run_graph_period = 0;    // their length
     int cur = 0;                 // buffer holding the newest populations

@@ -143,7 +143,7 @@ constexpr int kBatchTileY = 4;
     /* one step of the members of a small 2D batch, direct loads; D.segs: nitems tiles     */ \
     /* (cavity, x0, y0) of 32 x 8 nodes                                                    */ \
     cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur,              \
-                             int write_macro, bool pdl, cudaStream_t s);                      \
+                             int write_macro, cudaStream_t s);                                \
     /* one step of every cavity of a 3D batch (segments: tile, z0, z1, cavity; 32 x 4 tiles) */\
     cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur,             \
                               int write_macro, int *err, bool pdl, cudaStream_t s);           \

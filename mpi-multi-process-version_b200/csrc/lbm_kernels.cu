@@ -1062,10 +1062,10 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
 
 // Small 2D batches -- the few members still running near the end of a run,
 // where a step's time is its latency, not its bytes: one thread per node with
-// direct loads as k_step2d, block b the 32 x 8 tile D.segs[b] = (cavity, x0,
-// y0) of the batch's work list; `cur` is the buffer read this step.  Launched
-// as a programmatic dependent, a block reads its tile and tables, then waits
-// for the previous step; the populations are read through L2 (ld.global.cg).
+// direct loads through the read-only path as k_step2d, block b the 32 x 8
+// tile D.segs[b] = (cavity, x0, y0) of the batch's work list; `cur` is the
+// buffer read this step.  Launched in plain stream order (its loads go
+// through L1, which a kernel boundary leaves coherent).
 template <int ST>
 __global__ void __launch_bounds__(256)
 k_step2d_batch(const BatchDev D, int cur, int write_macro)
@@ -1075,17 +1075,10 @@ k_step2d_batch(const BatchDev D, int cur, int write_macro)
     const int4 t = D.segs[blockIdx.x];
     const Geo &G = D.geo[t.x];
     const Bufs &B = D.bufs[t.x];
-    const RunCtl *ctl = B.ctl;
-    const S *src = (const S *)B.pop[cur];
-    const C *Fin = (const C *)B.F[cur];
-    S *dst = (S *)B.pop[1 - cur];
-    C *Fout = (C *)B.F[1 - cur];
     const int i = t.y + threadIdx.x, j = t.z + threadIdx.y;
-    const bool inside = i < G.nx && j < G.ny;
-    dep_launch();
-    dep_wait();
-    if (!ctl->active || !inside) return;
-    step2d_node<ST, 0, true>(G, src, Fin, dst, Fout, B, write_macro, i, j);
+    if (!B.ctl->active || i >= G.nx || j >= G.ny) return;
+    step2d_node<ST, 0>(G, (const S *)B.pop[cur], (const C *)B.F[cur], (S *)B.pop[1 - cur], (C *)B.F[1 - cur], B,
+                       write_macro, i, j);
 }
 
 // ---------------------------------------------------------------------------
@@ -1412,25 +1405,16 @@ cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int c
 }
 
 template <int ST>
-static cudaError_t launch_direct_batch(const BatchDev &D, int nitems, int cur, int wm, bool pdl, cudaStream_t s)
+static cudaError_t launch_direct_batch(const BatchDev &D, int nitems, int cur, int wm, cudaStream_t s)
 {
     ++g_launches;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(nitems);
-    cfg.blockDim = dim3(32, 8, 1);
-    cfg.stream = s;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = pdl ? at : nullptr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k_step2d_batch<ST>, D, cur, wm);
+    k_step2d_batch<ST><<<nitems, dim3(32, 8, 1), 0, s>>>(D, cur, wm);
+    return cudaGetLastError();
 }
 
-cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur, int write_macro, bool pdl,
-                         cudaStream_t s)
+cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur, int write_macro, cudaStream_t s)
 {
-#define CALL(ST) launch_direct_batch<ST>(D, nitems, cur, write_macro, pdl, s)
+#define CALL(ST) launch_direct_batch<ST>(D, nitems, cur, write_macro, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }

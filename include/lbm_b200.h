@@ -278,11 +278,6 @@ typedef struct lbm_batch lbm_batch;
 #define LBM_BATCH_OPT_PDL         8  /* as LBM_OPT_PDL for the batch's step kernels (default 1; a step
                                         with both storages present forks onto two streams and is
                                         launched in plain stream order) */
-#define LBM_BATCH_OPT_DIRECT      9  /* 2D: while the members of one storage on the work list hold at
-                                        most this many nodes in all (the last members of a run), they
-                                        step through a direct-load kernel (one block per 32 x 8 tile)
-                                        instead of the persistent march kernel; default 65536, 0 off.
-                                        Exact mode: bit-identical either way */
 
 /* Create n cavities (same dim, storage, mode and device; any size and
  * parameters).  x[i], y[i], z[i] are the coordinate arrays of cavity i as for

@@ -43,12 +43,6 @@ using namespace lbm;
                              #call, cudaGetErrorString(e_), __FILE__, __LINE__);                         \
     } while (0)
 
-// 2D: a storage's members step through the direct-load kernel while they hold
-// at most this many nodes in all (the last members of a run): a step is then
-// latency-bound, and the direct kernel's one round of loads beats the march
-// kernel's ring start-up
-static constexpr int64_t kDirectNodes = 65536;
-
 struct lbm_batch {
     int n = 0;
     int dim = 2, storage = 0, mode = 0, device = 0;
@@ -63,7 +57,6 @@ struct lbm_batch {
     double growth = 0.0;           // residual growth factor that stops a member in lbm_batch_run (0: off)
     int storages = 0;              // LBM_BATCH_OPT_STORAGES: storages lbm_batch_tune may pick (0: the current)
     int pdl = 1;                   // LBM_BATCH_OPT_PDL: programmatic dependent launch of the step kernels
-    int64_t direct_nodes = kDirectNodes;  // LBM_BATCH_OPT_DIRECT
     Geo *d_geo = nullptr;
     TmapSet *d_maps = nullptr;
     Bufs *d_bufs = nullptr;
@@ -75,7 +68,6 @@ struct lbm_batch {
         size_t segs_cap = 0, segoff_cap = 0;
         int nblocks = 0;   // the list's grid (fixed while graphs replay it)
         int tx = 0;        // the tile width its kernel was captured with
-        int direct = 0;    // 1: its few nodes step through the direct-load kernel (one block per tile)
         BatchDev dev{};
     } wl[2];
     bool run_both = false;         // a mixed run: both storages' kernels launch every step
@@ -270,35 +262,6 @@ static int build_tables(lbm_batch *b)
             W.nblocks = 0;
             continue;
         }
-        int64_t snodes = 0;
-        for (size_t k = 0; k < sc.size(); ++k)
-            if (k == 0 || sc[k].cav != sc[k - 1].cav) snodes += b->cav[sc[k].cav]->geo.nnode;
-        if (!d3 && !sc.empty() && b->direct_nodes > 0 && snodes <= b->direct_nodes) {
-            // few nodes left: one block per 32 x 8 tile of every member on the list
-            std::vector<int4> items;
-            for (size_t k = 0; k < sc.size(); ++k) {
-                if (k > 0 && sc[k].cav == sc[k - 1].cav) continue;
-                const Geo &g = b->cav[sc[k].cav]->geo;
-                for (int y0 = 0; y0 < g.ny; y0 += 8)
-                    for (int x0 = 0; x0 < g.nx; x0 += 32) items.push_back(make_int4(sc[k].cav, x0, y0, 0));
-            }
-            if (W.segs_cap < items.size()) {
-                if (W.d_segs) cudaFree(W.d_segs);
-                W.d_segs = nullptr;
-                W.segs_cap = items.size();
-                BCU(cudaMalloc(&W.d_segs, sizeof(int4) * W.segs_cap));
-                regraph = true;
-            }
-            BCU(cudaMemcpyAsync(W.d_segs, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice,
-                                b->stream));
-            if (!W.direct || W.nblocks != (int)items.size()) regraph = true;
-            W.direct = 1;
-            W.nblocks = (int)items.size();
-            W.tx = 32;
-            W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, nullptr};
-            b->nblocks += W.nblocks;
-            continue;
-        }
         const int bps = d3 ? (b->mode == LBM_MODE_EXACT ? exact::march_batch3d_blocks_per_sm(sto)
                                                          : fast::march_batch3d_blocks_per_sm(sto))
                            : (b->mode == LBM_MODE_EXACT ? exact::march_batch_blocks_per_sm(sto, TX)
@@ -344,10 +307,9 @@ static int build_tables(lbm_batch *b)
             BCU(cudaMemcpyAsync(W.d_segs, segs.data(), sizeof(int4) * segs.size(), cudaMemcpyHostToDevice,
                                 b->stream));
         BCU(cudaMemcpyAsync(W.d_segoff, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, b->stream));
-        if (W.nblocks != (int)G || W.tx != TX || W.direct) regraph = true;
+        if (W.nblocks != (int)G || W.tx != TX) regraph = true;
         W.nblocks = (int)G;
         W.tx = TX;
-        W.direct = 0;
         W.dev = BatchDev{b->d_geo, b->d_maps, b->d_bufs, W.d_segs, W.d_segoff};
         b->nblocks += (int)G;
     }
@@ -364,9 +326,6 @@ static int build_tables(lbm_batch *b)
 static cudaError_t launch_list(lbm_batch *b, int sto, int cur, int wm, bool pdl, cudaStream_t s)
 {
     const lbm_batch::WorkList &W = b->wl[sto];
-    if (W.direct)
-        return b->mode == LBM_MODE_EXACT ? exact::step_batch2d(sto, W.dev, W.nblocks, cur, wm, s)
-                                         : fast::step_batch2d(sto, W.dev, W.nblocks, cur, wm, s);
     if (b->dim == 3)
         return b->mode == LBM_MODE_EXACT ? exact::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s)
                                          : fast::march_batch3d(sto, W.dev, W.nblocks, cur, wm, b->d_err, pdl, s);
@@ -982,10 +941,6 @@ extern "C" int lbm_batch_set_option(lbm_batch *b, int32_t option, int64_t value)
             return set_error(LBM_ERR_UNSUPPORTED, "exact mode computes in FP64 storage only");
         b->storages = (int)value;
         break;
-    case LBM_BATCH_OPT_DIRECT:
-        if (value < 0) return set_error(LBM_ERR_PARAM, "direct-kernel node threshold must be >= 0");
-        b->direct_nodes = value;
-        break;
     case LBM_BATCH_OPT_PDL:
         if (value != 0 && value != 1) return set_error(LBM_ERR_PARAM, "PDL must be 0 or 1");
         BCU(cudaSetDevice(b->device));
@@ -1012,7 +967,6 @@ extern "C" int lbm_batch_get_option(const lbm_batch *b, int32_t option, int64_t 
     case LBM_BATCH_OPT_STORAGES: *value = b->storages; return LBM_OK;
     case LBM_BATCH_OPT_STORAGE: *value = b->storage; return LBM_OK;
     case LBM_BATCH_OPT_PDL: *value = b->pdl; return LBM_OK;
-    case LBM_BATCH_OPT_DIRECT: *value = b->direct_nodes; return LBM_OK;
     default: return set_error(LBM_ERR_PARAM, "unknown batch option %d", option);
     }
 }

@@ -88,8 +88,7 @@ struct BatchDev {
     const Geo *geo;          // [ncav]
     const TmapSet *maps;     // [ncav][2]: descriptors of pop[0], pop[1] (+ their force arrays)
     const Bufs *bufs;        // [ncav]
-    const int4 *segs;        // all segments: 2D march (cavity, i0, ja, jb); 3D (tile, z0, z1, cavity);
-                             // 2D direct-load kernel: one 32 x 8 tile per block (cavity, x0, y0, 0)
+    const int4 *segs;        // all segments: 2D (cavity, i0, ja, jb); 3D (tile, z0, z1, cavity)
     const int *seg_off;      // [nblocks + 1]
 };
 
@@ -140,10 +139,6 @@ constexpr int kBatchTileY = 4;
     cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int cur,       \
                             int write_macro, int *err, bool pdl, cudaStream_t s);             \
     int march_batch_blocks_per_sm(int store, int TX);                                         \
-    /* one step of the members of a small 2D batch, direct loads; D.segs: nitems tiles     */ \
-    /* (cavity, x0, y0) of 32 x 8 nodes                                                    */ \
-    cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur,              \
-                             int write_macro, cudaStream_t s);                                \
     /* one step of every cavity of a 3D batch (segments: tile, z0, z1, cavity; 32 x 4 tiles) */\
     cudaError_t march_batch3d(int store, const BatchDev &D, int nblocks, int cur,             \
                               int write_macro, int *err, bool pdl, cudaStream_t s);           \

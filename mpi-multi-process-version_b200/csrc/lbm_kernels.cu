@@ -1060,27 +1060,6 @@ __global__ void k_collide(const Geo G, const typename Tr<ST>::S *__restrict__ in
 
 #include "lbm_march.cuh"
 
-// Small 2D batches -- the few members still running near the end of a run,
-// where a step's time is its latency, not its bytes: one thread per node with
-// direct loads through the read-only path as k_step2d, block b the 32 x 8
-// tile D.segs[b] = (cavity, x0, y0) of the batch's work list; `cur` is the
-// buffer read this step.  Launched in plain stream order (its loads go
-// through L1, which a kernel boundary leaves coherent).
-template <int ST>
-__global__ void __launch_bounds__(256)
-k_step2d_batch(const BatchDev D, int cur, int write_macro)
-{
-    using S = typename Tr<ST>::S;
-    using C = typename Tr<ST>::C;
-    const int4 t = D.segs[blockIdx.x];
-    const Geo &G = D.geo[t.x];
-    const Bufs &B = D.bufs[t.x];
-    const int i = t.y + threadIdx.x, j = t.z + threadIdx.y;
-    if (!B.ctl->active || i >= G.nx || j >= G.ny) return;
-    step2d_node<ST, 0>(G, (const S *)B.pop[cur], (const C *)B.F[cur], (S *)B.pop[1 - cur], (C *)B.F[1 - cur], B,
-                       write_macro, i, j);
-}
-
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -1400,21 +1379,6 @@ cudaError_t march_batch(int store, int TX, const BatchDev &D, int nblocks, int c
                         bool pdl, cudaStream_t s)
 {
 #define CALL(ST) launch_batch_tx<ST>(TX, D, nblocks, cur, write_macro, err, pdl, s)
-    LBM_DISPATCH(store, CALL)
-#undef CALL
-}
-
-template <int ST>
-static cudaError_t launch_direct_batch(const BatchDev &D, int nitems, int cur, int wm, cudaStream_t s)
-{
-    ++g_launches;
-    k_step2d_batch<ST><<<nitems, dim3(32, 8, 1), 0, s>>>(D, cur, wm);
-    return cudaGetLastError();
-}
-
-cudaError_t step_batch2d(int store, const BatchDev &D, int nitems, int cur, int write_macro, cudaStream_t s)
-{
-#define CALL(ST) launch_direct_batch<ST>(D, nitems, cur, write_macro, s)
     LBM_DISPATCH(store, CALL)
 #undef CALL
 }

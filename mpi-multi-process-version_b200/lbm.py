@@ -39,7 +39,7 @@ EXPORTS = [
     "lbm_batch_set_storage", "lbm_batch_run_mixed",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5, "storages": 6, "storage": 7,
-             "pdl": 8, "direct": 9}
+             "pdl": 8}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
 OPT_TILEY, OPT_PLAN, OPT_WAIT_LIMIT, OPT_PDL = 6, 7, 8, 9
 KERNELS = {"auto": 0, "direct": 1, "march": 2}

@@ -33,9 +33,11 @@ from . import surrogate as S
 
 F32_EPS = float(np.float32(1e-6))   # the reference's epsU/epsT (single-precision literals, 2M:35)
 # how much faster FP32 stepping must be for the mixed run to pay off: its
-# hand-over to FP64 costs 9-25 % more iterations (measured on B200, first 16 and
-# 64 held-out cavities, warm start)
-FP32_HANDOVER_COST = 1.3
+# hand-over to FP64 costs 9-25 % more iterations, and while members of both
+# storages run every step launches two kernels side by side.  Measured on B200
+# (first 64 held-out cavities, warm start): FP32 batch stepping 1.40x FP64's,
+# yet the mixed run took 68.3 s against FP64's 62.0 s
+FP32_HANDOVER_COST = 1.6
 
 
 # ---------------------------------------------------------------------------

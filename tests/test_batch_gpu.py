@@ -38,15 +38,10 @@ def reference(pkg):
     return [standalone(pkg, sp, 37) for sp in SPECS]
 
 
-@pytest.mark.parametrize("tile,nblocks,graphs,direct", [(64, 0, 1, 0), (32, 0, 1, 0), (128, 0, 0, 0), (64, 1, 1, 0),
-                                                        (32, 5, 0, 0), (128, 7, 1, 0), (64, 0, 1, 65536),
-                                                        (64, 0, 0, 65536)])
-def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, graphs, direct):
-    # direct 0: the persistent march kernel; 65536: these 25,715 nodes step
-    # through the direct-load batch kernel
+@pytest.mark.parametrize("tile,nblocks,graphs", [(64, 0, 1), (32, 0, 1), (128, 0, 0), (64, 1, 1), (32, 5, 0),
+                                                 (128, 7, 1)])
+def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, graphs):
     b = pkg.Batch(2, SPECS, mode="exact")
-    assert b.get_option("direct") == 65536
-    b.set_option("direct", direct)
     b.set_option("tile", tile)
     b.set_option("nblocks", nblocks)
     b.set_option("graphs", graphs)
@@ -62,8 +57,8 @@ def test_batch_members_match_standalone_bitwise(pkg, reference, tile, nblocks, g
     b.close()
 
 
-@pytest.mark.parametrize("dim,direct", [(2, 0), (2, 65536), (3, 0)])
-def test_batch_programmatic_dependent_launch_is_bit_identical(pkg, dim, direct):
+@pytest.mark.parametrize("dim", [2, 3])
+def test_batch_programmatic_dependent_launch_is_bit_identical(pkg, dim):
     # the batch's step kernels as programmatic dependents (the default) against
     # plain stream order: steps, graph replays and the device-side run loop
     if dim == 2:
@@ -76,7 +71,6 @@ def test_batch_programmatic_dependent_launch_is_bit_identical(pkg, dim, direct):
         b = pkg.Batch(dim, specs, mode="exact")
         assert b.get_option("pdl") == 1
         b.set_option("pdl", pdl)
-        b.set_option("direct", direct)
         b.initial()
         b.step(20)
         b.step(17)
@@ -208,8 +202,8 @@ def test_sweep_members_against_oracle(pkg, ora):
     b.close()
 
 
-@pytest.mark.parametrize("dim,growth,direct", [(2, 0, 0), (2, 100, 0), (2, 0, 4000), (3, 0, 0)])
-def test_batch_run_matches_host_loop(pkg, dim, growth, direct):
+@pytest.mark.parametrize("dim,growth", [(2, 0), (2, 100), (3, 0)])
+def test_batch_run_matches_host_loop(pkg, dim, growth):
     # the device-side stop test of lbm_batch_run against each member run alone
     # with the reference's loop on the host: the same iterations, the same
     # stop, the same fields (exact mode, bit for bit)
@@ -227,9 +221,6 @@ def test_batch_run_matches_host_loop(pkg, dim, growth, direct):
     ce, eps, max_steps = 150, 3e-2, 4500
     b = pkg.Batch(dim, specs, mode="exact")
     b.set_option("growth", growth)
-    # direct 4000: the 10,496 nodes start on the march kernel and the members
-    # left once the larger ones stop move to the direct-load kernel
-    b.set_option("direct", direct)
     b.initial()
     status, steps = b.run_masked(None, max_steps, ce, eps)
     assert (status == 1).any()

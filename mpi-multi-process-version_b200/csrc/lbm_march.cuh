@@ -42,6 +42,13 @@ __device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t n)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
 }
 
+// one arrival (release: the arriving thread's earlier shared-memory reads are
+// ordered before the phase completes)
+__device__ __forceinline__ void mbar_arrive(uint64_t *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
@@ -169,7 +176,8 @@ __device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k ==
 // critical path of the step).  Single-cavity kernels take Geo as a kernel
 // parameter and read it from the constant bank instead.
 constexpr int kGeoStage = 256;
-static_assert(sizeof(Geo) <= kGeoStage && sizeof(Geo) % 8 == 0, "staged Geo must fit its shared-memory slot");
+static_assert(sizeof(Geo) + 8 <= kGeoStage && sizeof(Geo) % 8 == 0,
+              "staged Geo (and the 2D march's abort word behind it) must fit the slot");
 
 // every thread of the CTA: copy *src into the shared slot dst (8-byte words),
 // between two barriers (the slot's previous readers are done before it, the
@@ -720,16 +728,21 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
     constexpr int HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
+    // barriers: 4 y-ring slots, 2 plane-ring slots (copies landed), and 2
+    // row-done barriers (every warp finished row t, by t's parity)
     uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
     uint64_t *nbar = ybar + 4;
-    volatile int &s_abort = *(volatile int *)(nbar + 2);
+    uint64_t *done = nbar + 2;
     Geo *sgeo = (Geo *)(sm + 4 * L::yslot() + 2 * L::nslot() + 64);
+    volatile int &s_abort = *(volatile int *)((unsigned char *)sgeo + kGeoStage - 8);
+    constexpr int kWarps = TX / 32;
 
     const int tid = threadIdx.x;
     const int tx = tid;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
+        for (int s = 0; s < 2; ++s) mbar_init(&done[s], kWarps);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -738,6 +751,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
 
     uint32_t ynext = 0, nnext = 0;
     bool aborted = false, waited = false;
+    int t = 0;  // rows this block has processed, over all its segments
     const long long wlim = g_wait_limit;
     for (int k = 0; k < nseg && !aborted; ++k) {
         int cav, i0, ja, jb;
@@ -748,7 +762,12 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         C *Fout;
         const Bufs *Bp;
         cavity(cav, Gp, maps, dst, Fout, Bp);
-        if (kStage) Gp = stage_geo(Gp, sgeo);
+        // a block barrier at each segment start (stage_geo has two): every
+        // warp is done with the previous segment's ring slots
+        if (kStage)
+            Gp = stage_geo(Gp, sgeo);
+        else
+            __syncthreads();
         const RunCtl *ctl = Bp->ctl;
         if (!waited) {
             dep_wait();  // from here on: what earlier kernels wrote
@@ -812,28 +831,42 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
                 sT = C(0.125 * G.dt * tc_gradient(G));
             }
         }
-        for (int j = ja; j < jb; ++j) {
-            if (yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued) {
-                issue_y(j + 2);
+        // Rows are paced by barriers, not by a block barrier per row.  The
+        // copies issued at row j overwrite the y slot of row j-2 (last read at
+        // row j-1) and the plane slot of row j-1, so the issuing thread first
+        // waits until every warp has finished row j-1 (at a segment's first row
+        // the segment-start barrier stands in).  Row j's plane slot is issued at
+        // row j-1, after that wait for row j-2, so no warp runs more than one
+        // row ahead of another and each phase of a row-done barrier counts the
+        // arrivals of one row.  After a timeout (s_abort) a thread stops
+        // waiting, issuing and computing but still walks the rows and segment
+        // barriers with the others.
+        for (int j = ja; j < jb; ++j, ++t) {
+            const bool iy = yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued;
+            const bool in = j + 1 < jb;
+            bool ok = s_abort == 0;
+            if (ok && tid == 0 && (iy || in) && j > ja)
+                ok = mbar_wait(&done[(t - 1) & 1], ((t - 1) >> 1) & 1, wlim);
+            if (iy) {
+                if (ok) issue_y(j + 2);
                 yissued = j + 2;
             }
-            if (j + 1 < jb) issue_n(j + 1);
-            bool ok = true;
-            for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
-            ok = ok && wait_n(j);
-            if (!ok) {
-                atomicExch(err, 1);
-                s_abort = 1;
+            if (in && ok) issue_n(j + 1);
+            if (ok) {
+                for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
+                ok = ok && wait_n(j);
+                if (!ok) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
+                }
             }
             if (active && ok)
                 march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, Tcn, sT, dst, Fout, *Bp, write_macro);
-            __syncthreads();
-            if (s_abort) {
-                aborted = true;
-                break;
-            }
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(&done[t & 1]);
         }
     }
+    aborted = s_abort != 0;
     if (aborted && tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
         for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);

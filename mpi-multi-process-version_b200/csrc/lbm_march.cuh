@@ -271,16 +271,21 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     constexpr int TX = L::TX, TY = L::TY, HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
+    // barriers: 4 z-ring slots, 2 plane-ring slots (copies landed), and 2
+    // slice-done barriers (every warp finished slice step rt, by rt's parity)
     uint64_t *zbar = (uint64_t *)(sm + 4 * L::zslot() + 2 * L::nslot());
     uint64_t *nbar = zbar + 4;
-    volatile int &s_abort = *(volatile int *)(nbar + 2);
+    uint64_t *done = nbar + 2;
     Geo *sgeo = (Geo *)(sm + 4 * L::zslot() + 2 * L::nslot() + 64);
+    volatile int &s_abort = *(volatile int *)((unsigned char *)sgeo + kGeoStage - 8);
+    constexpr int kWarps = TX * TY / 32;
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&zbar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
+        for (int s = 0; s < 2; ++s) mbar_init(&done[s], kWarps);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -329,14 +334,20 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
     bool aborted = false, waited = false;
+    int rt = 0;  // slice steps this block has processed, over all its segments
 
-    for (int si = sbeg; si < send && !aborted; ++si) {
+    for (int si = sbeg; si < send; ++si) {
         const int4 sg = segs[si];
         S *dst;
         C *Fout;
         const Bufs *Bp;
         cavity(sg.w, Gp, Mp, dst, Fout, Bp);
-        if (kStage) Gp = stage_geo(Gp, sgeo);
+        // a block barrier at each segment start (stage_geo has two): every
+        // warp is done with the previous segment's ring slots
+        if (kStage)
+            Gp = stage_geo(Gp, sgeo);
+        else
+            __syncthreads();
         const RunCtl *ctl = Bp->ctl;
         if (!waited) {
             dep_wait();  // from here on: what earlier kernels wrote
@@ -374,21 +385,38 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
             ya = off_a(j, G.ny); yb = off_b(j, G.ny);
         }
 
-        for (int k = ka; k < kb; ++k) {
-            // prefetch: z-slice k+2 (its slot held k-2, done last step), plane slice k+1
-            if (zissued < seg_hi && k + 2 <= seg_hi && k + 2 > zissued) {
-                issue_z(k + 2);
+        // Slice steps are paced by barriers, not by a block barrier per step
+        // (the 2D march's scheme): the copies issued at step k overwrite the z
+        // slot of slice k-2 (last read at step k-1) and the plane slot of slice
+        // k-1, so the issuing thread first waits until every warp has finished
+        // step k-1 (at a segment's first step the segment-start barrier stands
+        // in).  Step k's plane slot is issued at step k-1, after that wait for
+        // step k-2, so no warp runs more than one step ahead of another and each
+        // phase of a slice-done barrier counts one step.  After a timeout
+        // (s_abort) a thread stops waiting, issuing and computing but still walks
+        // the steps and segment barriers with the others.
+        for (int k = ka; k < kb; ++k, ++rt) {
+            const bool iz = zissued < seg_hi && k + 2 <= seg_hi && k + 2 > zissued;
+            const bool in = k + 1 < kb;
+            bool ok = s_abort == 0;
+            if (ok && tid == 0 && (iz || in) && k > ka)
+                ok = mbar_wait(&done[(rt - 1) & 1], ((rt - 1) >> 1) & 1, wlim);
+            // prefetch: z-slice k+2, plane slice k+1 (only the issuing thread
+            // can have ok false here; it then issues nothing more)
+            if (iz) {
+                if (ok) issue_z(k + 2);
                 zissued = k + 2;
             }
-            if (k + 1 < kb) issue_n(k + 1);
+            if (in && ok) issue_n(k + 1);
 
             const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
-            bool ok = true;
-            for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
-            ok = ok && wait_n(k);
-            if (!ok) {
-                atomicExch(err, 1);
-                s_abort = 1;
+            if (ok) {
+                for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
+                ok = ok && wait_n(k);
+                if (!ok) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
+                }
             }
             if (active && ok) {
                 const int ka_ = k + off_a(k, nz), kb_ = k + off_b(k, nz);
@@ -504,13 +532,11 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
                     dst[(19 + q) * P + id] = tostore<S, C>(gp[q]);
                 }
             }
-            __syncthreads();
-            if (s_abort) {
-                aborted = true;
-                break;
-            }
+            __syncwarp();
+            if ((tid & 31) == 0) mbar_arrive(&done[rt & 1]);
         }
     }
+    aborted = s_abort != 0;
     if (aborted && tid == 0) {
         // let copies still in flight land before the CTA's shared memory is released
         for (int s = 0; s < 4; ++s) mbar_wait(&zbar[s], ((znext >> s) & 1u) ^ 1u);

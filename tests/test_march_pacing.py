@@ -1,7 +1,8 @@
-"""CPU model of the 2D march kernel's row pacing (csrc/lbm_march.cuh, march2d_run).
+"""CPU model of the march kernels' step pacing (csrc/lbm_march.cuh: march2d_run
+over rows, march3d_run over z-slices; the same protocol).
 
-The 2D march kernel paces its rows with mbarriers instead of a block barrier
-per row: one thread (in warp 0) issues the TMA copies of a y-ring of 4 slots
+The march kernels pace their steps with mbarriers instead of a block barrier
+per step (described here for rows): one thread (in warp 0) issues the TMA copies of a y-ring of 4 slots
 and a plane ring of 2 slots; before it overwrites the slots of rows j-2 / j-1
 it waits for a "row done" barrier that every warp arrives on after each row
 (two of them, by row parity); a block barrier starts each segment.  This model

@@ -35,6 +35,11 @@ static constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // limit of a step's waits, in clock cycles (set_wait_limit)
 __device__ long long g_wait_limit = kWaitCycles;
 
+// rows (2D) / slices (3D) beyond the ring's next copy at which the issuing
+// thread asks for the boxes to be fetched into L2 (set_l2_ahead; 0: off), so
+// that the ring's own copy, issued that many steps later, finds them there
+__device__ int g_l2_ahead = 2;
+
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t n)
@@ -119,6 +124,28 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, uint6
         " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(saddr(dst)),
         "l"(m), "r"(c0), "r"(c1), "r"(c2), "r"(saddr(bar))
         : "memory");
+}
+
+// L2 prefetch of a tiled box (no shared memory, no barrier; the box's
+// coordinates follow the loads' rules)
+__device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int c1, int c2, int c3)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(m), "r"(c0),
+                 "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch3(const CUtensorMap *m, int c0, int c1, int c2)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(m), "r"(c0), "r"(c1),
+                 "r"(c2)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch2(const CUtensorMap *m, int c0, int c1)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(m), "r"(c0), "r"(c1)
+                 : "memory");
 }
 
 __device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *m, uint64_t *bar, int c0, int c1)
@@ -330,6 +357,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
         nnext ^= 1u << slot;
     };
     const long long wlim = g_wait_limit;
+    const int ahead = g_l2_ahead;
     auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u, wlim); };
     auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
@@ -408,6 +436,24 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
                 zissued = k + 2;
             }
             if (in && ok) issue_n(k + 1);
+            if (tid == 0 && ok && ahead > 0) {
+                // the boxes `ahead` slices beyond these copies, into L2
+                const int rz = k + 2 + ahead, rn = k + 1 + ahead;
+                if (rz <= seg_hi)
+#pragma unroll
+                    for (int zi = 0; zi < 12; ++zi) {
+                        const int c = L::zc(zi);
+                        tma_prefetch4(&Mp->m[c], i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0), rz, L::zq(zi));
+                    }
+                if (rn < kb) {
+#pragma unroll
+                    for (int ni = 0; ni < 14; ++ni) {
+                        const int c = L::nc(ni);
+                        tma_prefetch4(&Mp->m[c], i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0), rn, L::nq(ni));
+                    }
+                    tma_prefetch3(&Mp->fmap, i0, j0, rn);
+                }
+            }
 
             const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
             if (ok) {
@@ -779,6 +825,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
     bool aborted = false, waited = false;
     int t = 0;  // rows this block has processed, over all its segments
     const long long wlim = g_wait_limit;
+    const int ahead = g_l2_ahead;
     for (int k = 0; k < nseg && !aborted; ++k) {
         int cav, i0, ja, jb;
         seg(k, cav, i0, ja, jb);
@@ -878,6 +925,24 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
                 yissued = j + 2;
             }
             if (in && ok) issue_n(j + 1);
+            if (tid == 0 && ok && ahead > 0) {
+                // the boxes `ahead` rows beyond these copies, into L2
+                const int ry = j + 2 + ahead, rn = j + 1 + ahead;
+                if (ry <= seg_hi)
+#pragma unroll
+                    for (int yi = 0; yi < 8; ++yi) {
+                        const int c = L::yc(yi);
+                        tma_prefetch3(&maps[c], i0 - (c ? HX : 0), ry, L::yq(yi));
+                    }
+                if (rn < jb) {
+#pragma unroll
+                    for (int ni = 0; ni < 6; ++ni) {
+                        const int c = L::nc(ni);
+                        tma_prefetch3(&maps[c], i0 - (c ? HX : 0), rn, L::nq(ni));
+                    }
+                    tma_prefetch2(&maps[4], i0, rn);
+                }
+            }
             if (ok) {
                 for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
                 ok = ok && wait_n(j);

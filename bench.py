@@ -274,8 +274,6 @@ def kernel_config(cav, pkg):
     if cav.kernel == "march":
         kc["march_blocks"] = cav.get_option(pkg.lbm.OPT_NBLOCKS)
         kc["l2_promotion"] = ["none", "64B", "128B", "256B"][cav.get_option(pkg.lbm.OPT_L2PROMO)]
-        ahead = cav.get_option(pkg.lbm.OPT_L2_AHEAD)
-        kc["l2_prefetch_ahead"] = ahead if ahead >= 0 else "library default"
         if cav.dim == 3:
             kc["tile_rows"] = cav.get_option(pkg.lbm.OPT_TILEY)
             kc["plan"] = ["z-lockstep, balanced tails", "contiguous shares"][cav.get_option(pkg.lbm.OPT_PLAN)]
@@ -646,8 +644,6 @@ def main():
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "march"])
     ap.add_argument("--nblocks", type=int, default=0, help="persistent blocks of the march kernel (0 = auto)")
     ap.add_argument("--l2promo", type=int, default=-1, help="TMA L2 promotion 0..3 (-1 = library default)")
-    ap.add_argument("--l2-ahead", type=int, default=-1,
-                    help="march kernels' L2 prefetch distance in steps (-1 = library default)")
     ap.add_argument("--tiley", type=int, default=0, help="3D march tile rows 4 or 8 (0 = library default)")
     ap.add_argument("--plan", type=int, default=-1, help="3D march work plan 0 or 1 (-1 = library default)")
     ap.add_argument("--sweep", type=int, default=256, help="batch256: the first N cavities of the sweep (a profile)")
@@ -680,8 +676,6 @@ def main():
                      mode=args.mode, device=local, kernel=args.kernel, nblocks=args.nblocks)
     if args.l2promo >= 0:
         cav.set_option(pkg.lbm.OPT_L2PROMO, args.l2promo)
-    if args.l2_ahead >= 0:
-        cav.set_option(pkg.lbm.OPT_L2_AHEAD, args.l2_ahead)
     if args.tiley and dim == 3:
         cav.set_option(pkg.lbm.OPT_TILEY, args.tiley)
     if args.plan >= 0 and dim == 3:

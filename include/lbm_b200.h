@@ -86,11 +86,6 @@ extern "C" {
                                scheduled while the previous step drains, set up, and wait for its
                                completion before reading the populations; 0: plain stream order.
                                Results are identical either way. */
-#define LBM_OPT_L2_AHEAD 10 /* march kernels: how many rows (2D) / slices (3D) beyond each ring copy the
-                               issuing thread prefetches the boxes into L2 (cp.async.bulk.prefetch),
-                               for every handle and batch on the handle's device; default 2, 0 off,
-                               at most 16.  lbm_get_option reports the value last set through this
-                               handle (-1: never set).  Results are identical for every value. */
 
 /* grid kinds for lbm_mesh */
 #define LBM_GRID_ERF     0  /* the reference's erf grid, constA = stretch (3.2) */

@@ -1332,13 +1332,6 @@ extern "C" int lbm_set_option(lbm_handle *h, int32_t option, int64_t value)
         CU(exact::set_wait_limit(value));
         h->wait_limit = value;
         return LBM_OK;
-    case LBM_OPT_L2_AHEAD:
-        if (value < 0 || value > 16) return fail(LBM_ERR_PARAM, "L2 prefetch distance must be 0..16");
-        CU(cudaStreamSynchronize(h->stream));
-        CU(fast::set_l2_ahead((int)value));
-        CU(exact::set_l2_ahead((int)value));
-        h->l2_ahead = (int)value;
-        return LBM_OK;
     case LBM_OPT_PDL:
         if (value != 0 && value != 1) return fail(LBM_ERR_PARAM, "PDL must be 0 or 1");
         CU(cudaStreamSynchronize(h->stream));
@@ -1363,7 +1356,6 @@ extern "C" int lbm_get_option(const lbm_handle *h, int32_t option, int64_t *valu
     case LBM_OPT_PLAN: *value = h->plan_opt; return LBM_OK;
     case LBM_OPT_WAIT_LIMIT: *value = h->wait_limit; return LBM_OK;
     case LBM_OPT_PDL: *value = h->pdl; return LBM_OK;
-    case LBM_OPT_L2_AHEAD: *value = h->l2_ahead; return LBM_OK;
     default: return fail(LBM_ERR_PARAM, "unknown option %d", option);
     }
 }

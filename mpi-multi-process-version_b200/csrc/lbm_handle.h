@@ -47,7 +47,6 @@ struct lbm_handle {
     int plan_opt = 0;            // LBM_OPT_PLAN: 0 balanced z-lockstep, 1 contiguous shares
     int64_t wait_limit = 0;      // LBM_OPT_WAIT_LIMIT as last set through this handle
     int pdl = 1;                 // LBM_OPT_PDL: programmatic dependent launch of march steps
-    int l2_ahead = -1;           // LBM_OPT_L2_AHEAD as last set through this handle (-1: never)
     int4 *d_msegs = nullptr;     // 3D march work plan: segments (tile, z0, z1, -)
     int *d_msegoff = nullptr;    // and each block's first segment
     size_t msegs_cap = 0, msegoff_cap = 0;

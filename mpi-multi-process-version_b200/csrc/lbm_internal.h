@@ -145,8 +145,6 @@ constexpr int kBatchTileY = 4;
     int march_batch3d_blocks_per_sm(int store);                                               \
     /* limit of the march kernels' per-step waits on this device, in clock cycles */          \
     cudaError_t set_wait_limit(long long cycles);                                             \
-    /* steps ahead of the rings at which the march kernels prefetch boxes into L2 (0 off)   */ \
-    cudaError_t set_l2_ahead(int steps);                                                      \
     }
 
 LBM_DECLARE_LAUNCHERS(fast)

@@ -1446,11 +1446,6 @@ cudaError_t set_wait_limit(long long cycles)
     return cudaMemcpyToSymbol(g_wait_limit, &cycles, sizeof cycles);
 }
 
-cudaError_t set_l2_ahead(int steps)
-{
-    return cudaMemcpyToSymbol(g_l2_ahead, &steps, sizeof steps);
-}
-
 }  // namespace LBM_NS
 
 #if !LBM_EXACT

@@ -35,23 +35,11 @@ static constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // limit of a step's waits, in clock cycles (set_wait_limit)
 __device__ long long g_wait_limit = kWaitCycles;
 
-// rows (2D) / slices (3D) beyond the ring's next copy at which the issuing
-// thread asks for the boxes to be fetched into L2 (set_l2_ahead; 0: off), so
-// that the ring's own copy, issued that many steps later, finds them there
-__device__ int g_l2_ahead = 2;
-
 __device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t n)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(b)), "r"(n) : "memory");
-}
-
-// one arrival (release: the arriving thread's earlier shared-memory reads are
-// ordered before the phase completes)
-__device__ __forceinline__ void mbar_arrive(uint64_t *b)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t *b, uint32_t bytes)
@@ -126,28 +114,6 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *m, uint6
         : "memory");
 }
 
-// L2 prefetch of a tiled box (no shared memory, no barrier; the box's
-// coordinates follow the loads' rules)
-__device__ __forceinline__ void tma_prefetch4(const CUtensorMap *m, int c0, int c1, int c2, int c3)
-{
-    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(m), "r"(c0),
-                 "r"(c1), "r"(c2), "r"(c3)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tma_prefetch3(const CUtensorMap *m, int c0, int c1, int c2)
-{
-    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(m), "r"(c0), "r"(c1),
-                 "r"(c2)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tma_prefetch2(const CUtensorMap *m, int c0, int c1)
-{
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(m), "r"(c0), "r"(c1)
-                 : "memory");
-}
-
 __device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *m, uint64_t *bar, int c0, int c1)
 {
     asm volatile(
@@ -203,8 +169,7 @@ __device__ __forceinline__ int need_hi(int k, int n) { return k == 0 ? 2 : (k ==
 // critical path of the step).  Single-cavity kernels take Geo as a kernel
 // parameter and read it from the constant bank instead.
 constexpr int kGeoStage = 256;
-static_assert(sizeof(Geo) + 8 <= kGeoStage && sizeof(Geo) % 8 == 0,
-              "staged Geo (and the 2D march's abort word behind it) must fit the slot");
+static_assert(sizeof(Geo) <= kGeoStage && sizeof(Geo) % 8 == 0, "staged Geo must fit its shared-memory slot");
 
 // every thread of the CTA: copy *src into the shared slot dst (8-byte words),
 // between two barriers (the slot's previous readers are done before it, the
@@ -298,21 +263,16 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     constexpr int TX = L::TX, TY = L::TY, HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
-    // barriers: 4 z-ring slots, 2 plane-ring slots (copies landed), and 2
-    // slice-done barriers (every warp finished slice step rt, by rt's parity)
     uint64_t *zbar = (uint64_t *)(sm + 4 * L::zslot() + 2 * L::nslot());
     uint64_t *nbar = zbar + 4;
-    uint64_t *done = nbar + 2;
+    volatile int &s_abort = *(volatile int *)(nbar + 2);
     Geo *sgeo = (Geo *)(sm + 4 * L::zslot() + 2 * L::nslot() + 64);
-    volatile int &s_abort = *(volatile int *)((unsigned char *)sgeo + kGeoStage - 8);
-    constexpr int kWarps = TX * TY / 32;
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&zbar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
-        for (int s = 0; s < 2; ++s) mbar_init(&done[s], kWarps);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -357,25 +317,18 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
         nnext ^= 1u << slot;
     };
     const long long wlim = g_wait_limit;
-    const int ahead = g_l2_ahead;
     auto wait_z = [&](int s) -> bool { return mbar_wait(&zbar[s & 3], ((znext >> (s & 3)) & 1u) ^ 1u, wlim); };
     auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
 
     bool aborted = false, waited = false;
-    int rt = 0;  // slice steps this block has processed, over all its segments
 
-    for (int si = sbeg; si < send; ++si) {
+    for (int si = sbeg; si < send && !aborted; ++si) {
         const int4 sg = segs[si];
         S *dst;
         C *Fout;
         const Bufs *Bp;
         cavity(sg.w, Gp, Mp, dst, Fout, Bp);
-        // a block barrier at each segment start (stage_geo has two): every
-        // warp is done with the previous segment's ring slots
-        if (kStage)
-            Gp = stage_geo(Gp, sgeo);
-        else
-            __syncthreads();
+        if (kStage) Gp = stage_geo(Gp, sgeo);
         const RunCtl *ctl = Bp->ctl;
         if (!waited) {
             dep_wait();  // from here on: what earlier kernels wrote
@@ -413,56 +366,21 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
             ya = off_a(j, G.ny); yb = off_b(j, G.ny);
         }
 
-        // Slice steps are paced by barriers, not by a block barrier per step
-        // (the 2D march's scheme): the copies issued at step k overwrite the z
-        // slot of slice k-2 (last read at step k-1) and the plane slot of slice
-        // k-1, so the issuing thread first waits until every warp has finished
-        // step k-1 (at a segment's first step the segment-start barrier stands
-        // in).  Step k's plane slot is issued at step k-1, after that wait for
-        // step k-2, so no warp runs more than one step ahead of another and each
-        // phase of a slice-done barrier counts one step.  After a timeout
-        // (s_abort) a thread stops waiting, issuing and computing but still walks
-        // the steps and segment barriers with the others.
-        for (int k = ka; k < kb; ++k, ++rt) {
-            const bool iz = zissued < seg_hi && k + 2 <= seg_hi && k + 2 > zissued;
-            const bool in = k + 1 < kb;
-            bool ok = s_abort == 0;
-            if (ok && tid == 0 && (iz || in) && k > ka)
-                ok = mbar_wait(&done[(rt - 1) & 1], ((rt - 1) >> 1) & 1, wlim);
-            // prefetch: z-slice k+2, plane slice k+1 (only the issuing thread
-            // can have ok false here; it then issues nothing more)
-            if (iz) {
-                if (ok) issue_z(k + 2);
+        for (int k = ka; k < kb; ++k) {
+            // prefetch: z-slice k+2 (its slot held k-2, done last step), plane slice k+1
+            if (zissued < seg_hi && k + 2 <= seg_hi && k + 2 > zissued) {
+                issue_z(k + 2);
                 zissued = k + 2;
             }
-            if (in && ok) issue_n(k + 1);
-            if (tid == 0 && ok && ahead > 0) {
-                // the boxes `ahead` slices beyond these copies, into L2
-                const int rz = k + 2 + ahead, rn = k + 1 + ahead;
-                if (rz <= seg_hi)
-#pragma unroll
-                    for (int zi = 0; zi < 12; ++zi) {
-                        const int c = L::zc(zi);
-                        tma_prefetch4(&Mp->m[c], i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0), rz, L::zq(zi));
-                    }
-                if (rn < kb) {
-#pragma unroll
-                    for (int ni = 0; ni < 14; ++ni) {
-                        const int c = L::nc(ni);
-                        tma_prefetch4(&Mp->m[c], i0 - ((c & 1) ? HX : 0), j0 - ((c & 2) ? 1 : 0), rn, L::nq(ni));
-                    }
-                    tma_prefetch3(&Mp->fmap, i0, j0, rn);
-                }
-            }
+            if (k + 1 < kb) issue_n(k + 1);
 
             const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
-            if (ok) {
-                for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
-                ok = ok && wait_n(k);
-                if (!ok) {
-                    atomicExch(err, 1);
-                    s_abort = 1;
-                }
+            bool ok = true;
+            for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
+            ok = ok && wait_n(k);
+            if (!ok) {
+                atomicExch(err, 1);
+                s_abort = 1;
             }
             if (active && ok) {
                 const int ka_ = k + off_a(k, nz), kb_ = k + off_b(k, nz);
@@ -578,11 +496,13 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
                     dst[(19 + q) * P + id] = tostore<S, C>(gp[q]);
                 }
             }
-            __syncwarp();
-            if ((tid & 31) == 0) mbar_arrive(&done[rt & 1]);
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
         }
     }
-    aborted = s_abort != 0;
     if (aborted && tid == 0) {
         // let copies still in flight land before the CTA's shared memory is released
         for (int s = 0; s < 4; ++s) mbar_wait(&zbar[s], ((znext >> s) & 1u) ^ 1u);
@@ -800,21 +720,16 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
     constexpr int HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
-    // barriers: 4 y-ring slots, 2 plane-ring slots (copies landed), and 2
-    // row-done barriers (every warp finished row t, by t's parity)
     uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
     uint64_t *nbar = ybar + 4;
-    uint64_t *done = nbar + 2;
+    volatile int &s_abort = *(volatile int *)(nbar + 2);
     Geo *sgeo = (Geo *)(sm + 4 * L::yslot() + 2 * L::nslot() + 64);
-    volatile int &s_abort = *(volatile int *)((unsigned char *)sgeo + kGeoStage - 8);
-    constexpr int kWarps = TX / 32;
 
     const int tid = threadIdx.x;
     const int tx = tid;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
-        for (int s = 0; s < 2; ++s) mbar_init(&done[s], kWarps);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -823,9 +738,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
 
     uint32_t ynext = 0, nnext = 0;
     bool aborted = false, waited = false;
-    int t = 0;  // rows this block has processed, over all its segments
     const long long wlim = g_wait_limit;
-    const int ahead = g_l2_ahead;
     for (int k = 0; k < nseg && !aborted; ++k) {
         int cav, i0, ja, jb;
         seg(k, cav, i0, ja, jb);
@@ -835,12 +748,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         C *Fout;
         const Bufs *Bp;
         cavity(cav, Gp, maps, dst, Fout, Bp);
-        // a block barrier at each segment start (stage_geo has two): every
-        // warp is done with the previous segment's ring slots
-        if (kStage)
-            Gp = stage_geo(Gp, sgeo);
-        else
-            __syncthreads();
+        if (kStage) Gp = stage_geo(Gp, sgeo);
         const RunCtl *ctl = Bp->ctl;
         if (!waited) {
             dep_wait();  // from here on: what earlier kernels wrote
@@ -904,60 +812,28 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
                 sT = C(0.125 * G.dt * tc_gradient(G));
             }
         }
-        // Rows are paced by barriers, not by a block barrier per row.  The
-        // copies issued at row j overwrite the y slot of row j-2 (last read at
-        // row j-1) and the plane slot of row j-1, so the issuing thread first
-        // waits until every warp has finished row j-1 (at a segment's first row
-        // the segment-start barrier stands in).  Row j's plane slot is issued at
-        // row j-1, after that wait for row j-2, so no warp runs more than one
-        // row ahead of another and each phase of a row-done barrier counts the
-        // arrivals of one row.  After a timeout (s_abort) a thread stops
-        // waiting, issuing and computing but still walks the rows and segment
-        // barriers with the others.
-        for (int j = ja; j < jb; ++j, ++t) {
-            const bool iy = yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued;
-            const bool in = j + 1 < jb;
-            bool ok = s_abort == 0;
-            if (ok && tid == 0 && (iy || in) && j > ja)
-                ok = mbar_wait(&done[(t - 1) & 1], ((t - 1) >> 1) & 1, wlim);
-            if (iy) {
-                if (ok) issue_y(j + 2);
+        for (int j = ja; j < jb; ++j) {
+            if (yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued) {
+                issue_y(j + 2);
                 yissued = j + 2;
             }
-            if (in && ok) issue_n(j + 1);
-            if (tid == 0 && ok && ahead > 0) {
-                // the boxes `ahead` rows beyond these copies, into L2
-                const int ry = j + 2 + ahead, rn = j + 1 + ahead;
-                if (ry <= seg_hi)
-#pragma unroll
-                    for (int yi = 0; yi < 8; ++yi) {
-                        const int c = L::yc(yi);
-                        tma_prefetch3(&maps[c], i0 - (c ? HX : 0), ry, L::yq(yi));
-                    }
-                if (rn < jb) {
-#pragma unroll
-                    for (int ni = 0; ni < 6; ++ni) {
-                        const int c = L::nc(ni);
-                        tma_prefetch3(&maps[c], i0 - (c ? HX : 0), rn, L::nq(ni));
-                    }
-                    tma_prefetch2(&maps[4], i0, rn);
-                }
-            }
-            if (ok) {
-                for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
-                ok = ok && wait_n(j);
-                if (!ok) {
-                    atomicExch(err, 1);
-                    s_abort = 1;
-                }
+            if (j + 1 < jb) issue_n(j + 1);
+            bool ok = true;
+            for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
+            ok = ok && wait_n(j);
+            if (!ok) {
+                atomicExch(err, 1);
+                s_abort = 1;
             }
             if (active && ok)
                 march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, Tcn, sT, dst, Fout, *Bp, write_macro);
-            __syncwarp();
-            if ((tid & 31) == 0) mbar_arrive(&done[t & 1]);
+            __syncthreads();
+            if (s_abort) {
+                aborted = true;
+                break;
+            }
         }
     }
-    aborted = s_abort != 0;
     if (aborted && tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
         for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);

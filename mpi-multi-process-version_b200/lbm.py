@@ -41,7 +41,7 @@ EXPORTS = [
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5, "storages": 6, "storage": 7,
              "pdl": 8}
 OPT_KERNEL, OPT_NBLOCKS, OPT_L2PROMO, OPT_GRAPHS, OPT_RESIDENT = 1, 2, 3, 4, 5
-OPT_TILEY, OPT_PLAN, OPT_WAIT_LIMIT, OPT_PDL, OPT_L2_AHEAD = 6, 7, 8, 9, 10
+OPT_TILEY, OPT_PLAN, OPT_WAIT_LIMIT, OPT_PDL = 6, 7, 8, 9
 KERNELS = {"auto": 0, "direct": 1, "march": 2}
 
 

@@ -308,28 +308,6 @@ def test_programmatic_dependent_launch_is_bit_identical(pkg, dim, shape):
     assert np.array_equal(out[0][1][0], out[1][1][0]) and np.array_equal(out[0][1][1], out[1][1][1])
 
 
-@pytest.mark.parametrize("dim,shape", [(2, (300, 40, 1)), (3, (40, 18, 12))])
-def test_l2_prefetch_distance_is_bit_identical(pkg, dim, shape):
-    # the march kernels' L2 prefetch is a hint: any distance (0 = off) gives the
-    # same populations; the setting is device-wide, so it is put back
-    out = []
-    try:
-        for ahead in (2, 0, 5):
-            c = pkg.Cavity(dim, *shape, grid="tanh", stretch=1.5, Ra=1e4, mode="exact", kernel="march")
-            c.set_option(pkg.lbm.OPT_L2_AHEAD, ahead)
-            assert c.get_option(pkg.lbm.OPT_L2_AHEAD) == ahead
-            c.initial()
-            c.step(23)
-            out.append(c.populations())
-            c.close()
-    finally:
-        c = pkg.Cavity(2, 32, 32)
-        c.set_option(pkg.lbm.OPT_L2_AHEAD, 2)
-        c.close()
-    for o in out[1:]:
-        assert np.array_equal(o[0], out[0][0]) and np.array_equal(o[1], out[0][1])
-
-
 def test_run_matches_manual_loop(pkg):
     eps = 2e-2
     a = pkg.Cavity(2, 40, 40, Ra=1e4, grid="tanh", stretch=1.5, mode="exact")

@@ -1248,7 +1248,7 @@ static int mbps3(void)
 {
     if (prepare_march3d<ST, TY>() != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d<ST, TY>, L3<ST, TY>::NTH,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d<ST, TY>, L3<ST, TY>::NT,
                                                          L3<ST, TY>::smem()) == cudaSuccess
                ? n
                : 0;
@@ -1282,7 +1282,7 @@ static cudaError_t launch_march3d(const Geo &g, const TmapSet &m, const void *Fi
     using C = typename Tr<ST>::C;
     cudaError_t e = prepare_march3d<ST, TY>();
     if (e != cudaSuccess) return e;
-    return launch_k(k_march3d<ST, TY>, nblocks, L3<ST, TY>::NTH, L3<ST, TY>::smem(), s, pdl, m, g, (const C *)Fin,
+    return launch_k(k_march3d<ST, TY>, nblocks, L3<ST, TY>::NT, L3<ST, TY>::smem(), s, pdl, m, g, (const C *)Fin,
                     (S *)pout, (C *)Fout, b, wm, segs, segoff, b.err);
 }
 
@@ -1410,7 +1410,7 @@ static cudaError_t launch_batch3d(const BatchDev &D, int nblocks, int cur, int w
     cudaError_t e = prepare_batch3d<ST>();
     if (e != cudaSuccess) return e;
     ++g_launches;
-    return launch_k(k_march3d_batch<ST, kBatchTileY>, nblocks, L3<ST, kBatchTileY>::NTH, L3<ST, kBatchTileY>::smem(),
+    return launch_k(k_march3d_batch<ST, kBatchTileY>, nblocks, L3<ST, kBatchTileY>::NT, L3<ST, kBatchTileY>::smem(),
                     s, pdl, D, cur, wm, err);
 }
 
@@ -1419,7 +1419,7 @@ static int batch3d_bps()
 {
     if (prepare_batch3d<ST>() != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d_batch<ST, kBatchTileY>, L3<ST, kBatchTileY>::NTH,
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march3d_batch<ST, kBatchTileY>, L3<ST, kBatchTileY>::NT,
                                                          L3<ST, kBatchTileY>::smem()) == cudaSuccess
                ? n
                : 0;

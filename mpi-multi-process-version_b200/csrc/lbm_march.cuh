@@ -190,9 +190,6 @@ struct L3 {
     using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
     static constexpr int TX = 32, TY = TY_, NT = TX * TY;
-    // threads launched: NT computing one node each, plus one producer warp
-    // whose first thread issues the TMA copies
-    static constexpr int NTH = NT + 32;
     static constexpr int HX = 16 / ES;
     __host__ __device__ static constexpr int bx(int c) { return TX + ((c & 1) ? 2 * HX : 0); }
     __host__ __device__ static constexpr int by(int c) { return TY + ((c & 2) ? 2 : 0); }
@@ -273,9 +270,6 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
 
     const int tid = threadIdx.x;
     const int tx = tid % TX, ty = tid / TX;
-    // thread NT (the producer warp's first) issues every copy and, on a
-    // timeout, drains them; threads 0 .. NT-1 compute
-    constexpr int kProd = L::NT;
     if (tid == 0) {
         for (int s = 0; s < 4; ++s) mbar_init(&zbar[s], 1);
         for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
@@ -292,7 +286,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
 
     auto issue_z = [&](int s) {
         const int slot = s & 3;
-        if (tid == kProd) {
+        if (tid == 0) {
             uint64_t *bar = &zbar[slot];
             mbar_arrive_tx(bar, L::ztx());
             unsigned char *base = sm + slot * L::zslot();
@@ -307,7 +301,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
     };
     auto issue_n = [&](int s) {
         const int slot = s & 1;
-        if (tid == kProd) {
+        if (tid == 0) {
             uint64_t *bar = &nbar[slot];
             mbar_arrive_tx(bar, L::ntx());
             unsigned char *base = sm + 4 * L::zslot() + slot * L::nslot();
@@ -357,7 +351,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
         int zissued = pre_hi;
 
         const int i = i0 + tx, j = j0 + ty;
-        const bool active = tid < L::NT && i < G.nx && j < G.ny;
+        const bool active = i < G.nx && j < G.ny;
         C xp[3], xm[3], yp[3], ym[3];
         int xa = 0, xb = 0, ya = 0, yb = 0;
         C Tcn = C(0.0), sTc = C(0.0);  // conduction profile at the node's y and its streaming shift
@@ -382,10 +376,8 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
 
             const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
             bool ok = true;
-            if (tid < L::NT) {
-                for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
-                ok = ok && wait_n(k);
-            }
+            for (int s = need_lo(k, nz); s <= need_hi(k, nz); ++s) ok = ok && wait_z(s);
+            ok = ok && wait_n(k);
             if (!ok) {
                 atomicExch(err, 1);
                 s_abort = 1;
@@ -511,7 +503,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
             }
         }
     }
-    if (aborted && tid == kProd) {
+    if (aborted && tid == 0) {
         // let copies still in flight land before the CTA's shared memory is released
         for (int s = 0; s < 4; ++s) mbar_wait(&zbar[s], ((znext >> s) & 1u) ^ 1u);
         for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
@@ -519,7 +511,7 @@ __device__ __forceinline__ void march3d_run(const int4 *__restrict__ segs, int s
 }
 
 template <int ST, int TY_>
-__global__ void __launch_bounds__(32 * TY_ + 32, TY_ == 8 ? 1 : 2)
+__global__ void __launch_bounds__(32 * TY_, TY_ == 8 ? 1 : 2)
 k_march3d(const __grid_constant__ TmapSet maps, const __grid_constant__ Geo G,
           const typename Tr<ST>::C *__restrict__ Fin, typename Tr<ST>::S *__restrict__ dst,
           typename Tr<ST>::C *__restrict__ Fout, const __grid_constant__ Bufs B, int write_macro,
@@ -541,7 +533,7 @@ k_march3d(const __grid_constant__ TmapSet maps, const __grid_constant__ Geo G,
 // many 3D cavities: segments (tile, z0, z1, cavity) of the batch's work list;
 // `cur` is the ping-pong buffer holding the populations read this step
 template <int ST, int TY_>
-__global__ void __launch_bounds__(32 * TY_ + 32, TY_ == 8 ? 1 : 2)
+__global__ void __launch_bounds__(32 * TY_, TY_ == 8 ? 1 : 2)
 k_march3d_batch(const BatchDev D, int cur, int write_macro, int *err)
 {
     using S = typename Tr<ST>::S;

@@ -551,6 +551,21 @@ k_march3d_batch(const BatchDev D, int cur, int write_macro, int *err)
 // ---------------------------------------------------------------------------
 // 2D layout: a tile is TX nodes of one row; the march runs along y
 // ---------------------------------------------------------------------------
+// 2D ring depths.  The y-ring holds kYS2 rows of the planes whose stencil
+// reaches along y, the plane ring kNS2 rows of the others; at row j the copies
+// of rows up to j + kYS2 - 2 (y-ring) and j + kNS2 - 1 (plane ring) are in
+// flight or landed, each refilling the slot of a row every warp has finished.
+#ifndef LBM_YS2
+#define LBM_YS2 4
+#endif
+#ifndef LBM_NS2
+#define LBM_NS2 2
+#endif
+constexpr int kYS2 = LBM_YS2, kNS2 = LBM_NS2;
+static_assert(kYS2 >= 4 && kNS2 >= 2 && kYS2 + kNS2 <= 30, "2D ring depths");
+// the barriers (kYS2 + kNS2) and the abort word, rounded up to 64 bytes
+constexpr int kBar2 = ((kYS2 + kNS2 + 1) * 8 + 63) / 64 * 64;
+
 template <int ST, int TX_ = 128>
 struct L2 {
     using S = typename Tr<ST>::S;
@@ -602,7 +617,7 @@ struct L2 {
         for (int a = 0; a < 6; ++a) b += bytes(nc(a));
         return b + fbytes() + 48;
     }
-    __host__ __device__ static constexpr int smem() { return 4 * yslot() + 2 * nslot() + 64 + kGeoStage + 128; }
+    __host__ __device__ static constexpr int smem() { return kYS2 * yslot() + kNS2 * nslot() + kBar2 + kGeoStage + 128; }
 };
 
 // One node of the 2D march at row j, from the ring slots in shared memory:
@@ -622,7 +637,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
     const int64_t P = G.plane;
     const int64_t id = (int64_t)j * G.pitch + i;
     const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
-    const unsigned char *nslot_j = sm + 4 * L::yslot() + (j & 1) * L::nslot();
+    const unsigned char *nslot_j = sm + kYS2 * L::yslot() + (j % kNS2) * L::nslot();
     const C Fy0 = ((const C *)(nslot_j + L::fo()))[tx];
     const double *wy = (const double *)(nslot_j + L::wo());
     const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
@@ -630,7 +645,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
         (void)q;
         return tocomp(((const S *)box)[idx]);
     };
-    auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s & 3) * L::yslot() + L::yoff(yi); };
+    auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s % kYS2) * L::yslot() + L::yoff(yi); };
     auto NB = [&](int ni) -> const unsigned char * { return nslot_j + L::noff(ni); };
     auto ix = [&](int c, int dx) -> int { return tx + (c ? HX : 0) + dx; };
     // y-interpolation of a y-ring plane at x-offset dx
@@ -720,16 +735,16 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
     constexpr int HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
-    uint64_t *ybar = (uint64_t *)(sm + 4 * L::yslot() + 2 * L::nslot());
-    uint64_t *nbar = ybar + 4;
-    volatile int &s_abort = *(volatile int *)(nbar + 2);
-    Geo *sgeo = (Geo *)(sm + 4 * L::yslot() + 2 * L::nslot() + 64);
+    uint64_t *ybar = (uint64_t *)(sm + kYS2 * L::yslot() + kNS2 * L::nslot());
+    uint64_t *nbar = ybar + kYS2;
+    volatile int &s_abort = *(volatile int *)(nbar + kNS2);
+    Geo *sgeo = (Geo *)(sm + kYS2 * L::yslot() + kNS2 * L::nslot() + kBar2);
 
     const int tid = threadIdx.x;
     const int tx = tid;
     if (tid == 0) {
-        for (int s = 0; s < 4; ++s) mbar_init(&ybar[s], 1);
-        for (int s = 0; s < 2; ++s) mbar_init(&nbar[s], 1);
+        for (int s = 0; s < kYS2; ++s) mbar_init(&ybar[s], 1);
+        for (int s = 0; s < kNS2; ++s) mbar_init(&nbar[s], 1);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -759,7 +774,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         const int ny = G.ny;
 
         auto issue_y = [&](int s) {
-            const int slot = s & 3;
+            const int slot = s % kYS2;
             if (tid == 0) {
                 uint64_t *bar = &ybar[slot];
                 mbar_arrive_tx(bar, L::ytx());
@@ -773,11 +788,11 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             ynext ^= 1u << slot;
         };
         auto issue_n = [&](int s) {
-            const int slot = s & 1;
+            const int slot = s % kNS2;
             if (tid == 0) {
                 uint64_t *bar = &nbar[slot];
                 mbar_arrive_tx(bar, L::ntx());
-                unsigned char *base = sm + 4 * L::yslot() + slot * L::nslot();
+                unsigned char *base = sm + kYS2 * L::yslot() + slot * L::nslot();
 #pragma unroll
                 for (int ni = 0; ni < 6; ++ni) {
                     const int c = L::nc(ni);
@@ -789,15 +804,21 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             nnext ^= 1u << slot;
         };
         auto wait_y = [&](int s) -> bool {
-            return mbar_wait(&ybar[s & 3], ((ynext >> (s & 3)) & 1u) ^ 1u, wlim);
+            return mbar_wait(&ybar[s % kYS2], ((ynext >> (s % kYS2)) & 1u) ^ 1u, wlim);
         };
-        auto wait_n = [&](int s) -> bool { return mbar_wait(&nbar[s & 1], ((nnext >> (s & 1)) & 1u) ^ 1u, wlim); };
+        auto wait_n = [&](int s) -> bool {
+            return mbar_wait(&nbar[s % kNS2], ((nnext >> (s % kNS2)) & 1u) ^ 1u, wlim);
+        };
 
+        // the segment's first copies: the y rows row ja needs and the rows
+        // behind them up to ja + kYS2 - 3, the plane rows ja .. ja + kNS2 - 2
         const int pre_lo = need_lo(ja, ny), pre_hi = need_hi(ja, ny);
         const int seg_hi = need_hi(jb - 1, ny) > pre_hi ? need_hi(jb - 1, ny) : pre_hi;
-        for (int s = pre_lo; s <= pre_hi; ++s) issue_y(s);
-        issue_n(ja);
-        int yissued = pre_hi;
+        const int y0 = min(seg_hi, max(pre_hi, ja + kYS2 - 3));
+        for (int s = pre_lo; s <= y0; ++s) issue_y(s);
+        const int n0 = min(jb - 1, ja + kNS2 - 2);
+        for (int s = ja; s <= n0; ++s) issue_n(s);
+        int yissued = y0, nissued = n0;
 
         const int i = i0 + tx;
         const bool active = i < G.nx;
@@ -813,11 +834,11 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             }
         }
         for (int j = ja; j < jb; ++j) {
-            if (yissued < seg_hi && j + 2 <= seg_hi && j + 2 > yissued) {
-                issue_y(j + 2);
-                yissued = j + 2;
-            }
-            if (j + 1 < jb) issue_n(j + 1);
+            // refill the slots of rows every warp has finished (the barrier
+            // that ended row j-1): y rows up to j + kYS2 - 2, plane rows up to
+            // j + kNS2 - 1
+            for (const int yt = min(seg_hi, j + kYS2 - 2); yissued < yt;) issue_y(++yissued);
+            for (const int nt = min(jb - 1, j + kNS2 - 1); nissued < nt;) issue_n(++nissued);
             bool ok = true;
             for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
             ok = ok && wait_n(j);
@@ -835,8 +856,8 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         }
     }
     if (aborted && tid == 0) {
-        for (int s = 0; s < 4; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
-        for (int s = 0; s < 2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < kYS2; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < kNS2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
     }
 }
 

@@ -72,11 +72,14 @@ def library_plan(ntiles, nz, grid, kind):
     return [[tuple(segs[3 * i:3 * i + 3]) for i in range(off[b], off[b + 1])] for b in range(used.value)]
 
 
-def replay(n, total, plan, nodes_of_unit, check_node):
+def replay(n, total, plan, nodes_of_unit, check_node, ys=4, ns=2):
     """Replay the march schedule along an axis of n slices for the CTAs of
-    `plan` (per CTA, its segments).  The in-plane indices of a node do not
-    depend on the step, so each tile's nodes are checked once, at every step
-    kind (first, inner, last slice)."""
+    `plan` (per CTA, its segments), with a ring of `ys` slots for the planes
+    whose stencil reaches along the axis and `ns` slots for the others: at
+    step k the copies of slices up to k + ys - 2 and k + ns - 1 are issued
+    (the 3D kernel: 4 and 2; the 2D kernel: kYS2 and kNS2).  The in-plane
+    indices of a node do not depend on the step, so each tile's nodes are
+    checked once, at every step kind (first, inner, last slice)."""
     covered = [0] * total
     checked = set()
     for segs in plan:
@@ -90,30 +93,37 @@ def replay(n, total, plan, nodes_of_unit, check_node):
 
             def issue(s, k_now):
                 assert 0 <= s < n
-                old = slot.get(s & 3)
+                old = slot.get(s % ys)
                 if old is not None and old[0] == t:
                     # the slice being evicted must not be needed by this or a later step
                     for kk in range(k_now, kb):
                         assert not (need_lo(kk, n) <= old[1] <= need_hi(kk, n)), (old, kk)
-                slot[s & 3] = (t, s)
+                slot[s % ys] = (t, s)
                 inflight.add(s)
 
-            for s in range(pre_lo, pre_hi + 1):
+            def issue_n(s, k_now):
+                old = nslot.get(s % ns)
+                assert old is None or old[0] != t or old[1] < k_now, (old, s, k_now)
+                nslot[s % ns] = (t, s)
+
+            y0 = min(seg_hi, max(pre_hi, ka + ys - 3))
+            for s in range(pre_lo, y0 + 1):
                 issue(s, ka)
-            nslot[ka & 1] = (t, ka)
-            zissued = pre_hi
+            n0 = min(kb - 1, ka + ns - 2)
+            for s in range(ka, n0 + 1):
+                issue_n(s, ka)
+            zissued, nissued = y0, n0
             for k in range(ka, kb):
-                if zissued < seg_hi and k + 2 <= seg_hi and k + 2 > zissued:
-                    issue(k + 2, k)
-                    zissued = k + 2
-                if k + 1 < kb:
-                    old = nslot.get((k + 1) & 1)
-                    assert old is None or old[0] != t or old[1] < k
-                    nslot[(k + 1) & 1] = (t, k + 1)
+                while zissued < min(seg_hi, k + ys - 2):
+                    zissued += 1
+                    issue(zissued, k)
+                while nissued < min(kb - 1, k + ns - 1):
+                    nissued += 1
+                    issue_n(nissued, k)
                 for s in range(need_lo(k, n), need_hi(k, n) + 1):
-                    assert slot.get(s & 3) == (t, s), ("slice not resident", s, k)
+                    assert slot.get(s % ys) == (t, s), ("slice not resident", s, k)
                     inflight.discard(s)
-                assert nslot[k & 1] == (t, k)
+                assert nslot[k % ns] == (t, k)
                 kind = (t, 0 if k == 0 else (2 if k == n - 1 else 1))
                 if kind not in checked:
                     checked.add(kind)
@@ -170,7 +180,7 @@ def check_3d(nx, ny, nz, grid, es, TY3=8, kind=0):
     replay(nz, ntiles * nz, library_plan(ntiles, nz, grid, kind), nodes, check_node)
 
 
-def check_2d(nx, ny, grid, es, TX=128):
+def check_2d(nx, ny, grid, es, TX=128, ys=4, ns=2):
     HX = 16 // es
     bx = lambda c: TX + (2 * HX if c else 0)  # noqa: E731
     ntx = -(-nx // TX)
@@ -196,7 +206,7 @@ def check_2d(nx, ny, grid, es, TX=128):
         for s in (j + off_a(j, ny), j, j + off_b(j, ny)):
             assert need_lo(j, ny) <= s <= need_hi(j, ny)
 
-    replay(ny, ntx * ny, contiguous_plan(ny, ntx * ny, grid), nodes, check_node)
+    replay(ny, ntx * ny, contiguous_plan(ny, ntx * ny, grid), nodes, check_node, ys, ns)
 
 
 @pytest.mark.parametrize("shape", [(128, 128, 128), (20, 16, 16), (33, 18, 7), (64, 24, 3), (40, 10, 5), (16, 16, 16),
@@ -230,12 +240,22 @@ def test_march3d_plan_balances_the_sms(ntiles, nz, grid):
         assert len(plan) == grid and all(len(s) == 1 for s in plan)
 
 
+def ring2d():
+    """The 2D kernel's ring depths (kYS2, kNS2) as the library's source sets them."""
+    import re
+    src = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                            "mpi-multi-process-version_b200", "csrc", "lbm_march.cuh")).read()
+    return (int(re.search(r"#define LBM_YS2 (\d+)", src).group(1)), int(re.search(r"#define LBM_NS2 (\d+)", src).group(1)))
+
+
 @pytest.mark.parametrize("shape", [(2048, 64), (128, 128), (130, 9), (48, 48), (300, 3), (40, 24)])
 @pytest.mark.parametrize("es", [8, 4, 2])
 @pytest.mark.parametrize("tx", [32, 64, 128])
-def test_march2d_schedule_and_indices(shape, es, tx):
+@pytest.mark.parametrize("ring", ["library", (4, 2), (5, 3), (6, 4)])
+def test_march2d_schedule_and_indices(shape, es, tx, ring):
+    ys, ns = ring2d() if ring == "library" else ring
     nx, ny = shape
     total = -(-nx // tx) * ny
     for grid in sorted({1, 2, 5, 148, 592, total}):
         if grid <= total:
-            check_2d(nx, ny, grid, es, tx)
+            check_2d(nx, ny, grid, es, tx, ys, ns)

@@ -1236,7 +1236,7 @@ static cudaError_t prepare_march2d()
     static bool done = false;
     if (!done) {
         cudaError_t e = cudaFuncSetAttribute(k_march2d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             L2<ST>::smem());
+                                             L2s<ST>::smem());
         if (e != cudaSuccess) return e;
         done = true;
     }
@@ -1260,7 +1260,7 @@ static int mbps(const Geo &g, int ty)
     if (g.dim == 3) return ty == 4 ? mbps3<ST, 4>() : mbps3<ST, 8>();
     if (prepare_march2d<ST>() != cudaSuccess) return 0;
     int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2<ST>::NT, L2<ST>::smem()) ==
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2s<ST>::NT, L2s<ST>::smem()) ==
                    cudaSuccess
                ? n
                : 0;
@@ -1298,7 +1298,7 @@ static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin,
         e = ty == 4 ? launch_march3d<ST, 4>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s)
                     : launch_march3d<ST, 8>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s);
     } else {
-        using L = L2<ST>;
+        using L = L2s<ST>;
         e = prepare_march2d<ST>();
         if (e != cudaSuccess) return e;
         const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
@@ -1480,15 +1480,15 @@ MarchShape march_shape(int dim, int store, int tx, int ty)
             m.by[c] = m.TY + ((c & 2) ? 2 : 0);
         }
     } else {
-#define LBM_FILL2(TXV)                                                    \
+#define LBM_FILL2(...)                                                    \
         switch (store) {                                                  \
-        case kF64: fill(fast::L2<kF64, TXV>{}, 2); break;                 \
-        case kF32: fill(fast::L2<kF32, TXV>{}, 2); break;                 \
-        default: fill(fast::L2<kF32, TXV>{}, 2); break;                   \
+        case kF64: fill(fast::L2<kF64, __VA_ARGS__>{}, 2); break;         \
+        case kF32: fill(fast::L2<kF32, __VA_ARGS__>{}, 2); break;         \
+        default: fill(fast::L2<kF32, __VA_ARGS__>{}, 2); break;           \
         }
         if (tx == 32) { LBM_FILL2(32) }
         else if (tx == 64) { LBM_FILL2(64) }
-        else { LBM_FILL2(128) }
+        else { LBM_FILL2(128, 6, 4) }  // the single-cavity kernel's layout (L2s)
 #undef LBM_FILL2
         for (int c = 0; c < 4; ++c) {
             m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);

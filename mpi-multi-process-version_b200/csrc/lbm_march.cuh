@@ -551,23 +551,19 @@ k_march3d_batch(const BatchDev D, int cur, int write_macro, int *err)
 // ---------------------------------------------------------------------------
 // 2D layout: a tile is TX nodes of one row; the march runs along y
 // ---------------------------------------------------------------------------
-// 2D ring depths.  The y-ring holds kYS2 rows of the planes whose stencil
-// reaches along y, the plane ring kNS2 rows of the others; at row j the copies
-// of rows up to j + kYS2 - 2 (y-ring) and j + kNS2 - 1 (plane ring) are in
-// flight or landed, each refilling the slot of a row every warp has finished.
-#ifndef LBM_YS2
-#define LBM_YS2 4
-#endif
-#ifndef LBM_NS2
-#define LBM_NS2 2
-#endif
-constexpr int kYS2 = LBM_YS2, kNS2 = LBM_NS2;
-static_assert(kYS2 >= 4 && kNS2 >= 2 && kYS2 + kNS2 <= 30, "2D ring depths");
-// the barriers (kYS2 + kNS2) and the abort word, rounded up to 64 bytes
-constexpr int kBar2 = ((kYS2 + kNS2 + 1) * 8 + 63) / 64 * 64;
-
-template <int ST, int TX_ = 128>
+// 2D layout.  Ring depths: the y-ring holds YS rows of the planes whose
+// stencil reaches along y, the plane ring NS rows of the others; at row j the
+// copies of rows up to j + YS - 2 (y-ring) and j + NS - 1 (plane ring) are in
+// flight or landed, each refilling the slot of a row every thread has
+// finished.  The batch kernel keeps 4 / 2 (more blocks per SM pay more on its
+// short segments); the single-cavity kernel runs 6 / 4 (measured on B200 at
+// 2048^2 FP64: 23,200 against 21,693 MLUPS; the batch loses 6-26 % with it).
+template <int ST, int TX_ = 128, int YS_ = 4, int NS_ = 2>
 struct L2 {
+    static constexpr int YS = YS_, NS = NS_;
+    static_assert(YS >= 4 && NS >= 2 && YS + NS <= 30, "2D ring depths");
+    // the barriers (YS + NS) and the abort word, rounded up to 64 bytes
+    static constexpr int BAR = ((YS + NS + 1) * 8 + 63) / 64 * 64;
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     static constexpr int ES = sizeof(S);
@@ -617,12 +613,16 @@ struct L2 {
         for (int a = 0; a < 6; ++a) b += bytes(nc(a));
         return b + fbytes() + 48;
     }
-    __host__ __device__ static constexpr int smem() { return kYS2 * yslot() + kNS2 * nslot() + kBar2 + kGeoStage + 128; }
+    __host__ __device__ static constexpr int smem() { return YS * yslot() + NS * nslot() + BAR + kGeoStage + 128; }
 };
+
+// the single-cavity 2D kernel's layout: 128-node rows, 6 / 4 ring slots
+template <int ST>
+using L2s = L2<ST, 128, 6, 4>;
 
 // One node of the 2D march at row j, from the ring slots in shared memory:
 // interpolation, walls, macro, collision, stores.
-template <int ST, int TX>
+template <int ST, class L>
 __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo &G, int tx, int i, int j, int xa,
                                              int xb, const typename Tr<ST>::C *xp, const typename Tr<ST>::C *xm,
                                              typename Tr<ST>::C Tcn, typename Tr<ST>::C sT,
@@ -631,13 +631,12 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    using L = L2<ST, TX>;
     constexpr int HX = L::HX;
     const int ny = G.ny;
     const int64_t P = G.plane;
     const int64_t id = (int64_t)j * G.pitch + i;
     const int ja_ = j + off_a(j, ny), jb_ = j + off_b(j, ny);
-    const unsigned char *nslot_j = sm + kYS2 * L::yslot() + (j % kNS2) * L::nslot();
+    const unsigned char *nslot_j = sm + L::YS * L::yslot() + (j % L::NS) * L::nslot();
     const C Fy0 = ((const C *)(nslot_j + L::fo()))[tx];
     const double *wy = (const double *)(nslot_j + L::wo());
     const C yp[3] = {C(wy[0]), C(wy[1]), C(wy[2])}, ym[3] = {C(wy[3]), C(wy[4]), C(wy[5])};
@@ -645,7 +644,7 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
         (void)q;
         return tocomp(((const S *)box)[idx]);
     };
-    auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s % kYS2) * L::yslot() + L::yoff(yi); };
+    auto YB = [&](int yi, int s) -> const unsigned char * { return sm + (s % L::YS) * L::yslot() + L::yoff(yi); };
     auto NB = [&](int ni) -> const unsigned char * { return nslot_j + L::noff(ni); };
     auto ix = [&](int c, int dx) -> int { return tx + (c ? HX : 0) + dx; };
     // y-interpolation of a y-ring plane at x-offset dx
@@ -726,25 +725,25 @@ __device__ __forceinline__ void march2d_node(const unsigned char *sm, const Geo 
 // x-offset i0, rows [ja, jb)).  `seg(k, cav, i0, ja, jb)` yields the block's
 // k-th segment; `cavity(cav, G, maps, dst, Fout, B)` yields the cavity's
 // geometry, the TMA descriptors of its source buffer and its outputs.
-template <int ST, int TX, bool kStage, class SegFn, class CavFn>
+template <int ST, class L, bool kStage, class SegFn, class CavFn>
 __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, int write_macro, int *err)
 {
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    using L = L2<ST, TX>;
+    constexpr int TX = L::TX;
     constexpr int HX = L::HX;
     extern __shared__ unsigned char sm_raw[];
     unsigned char *sm = sm_raw + ((128u - (saddr(sm_raw) & 127u)) & 127u);
-    uint64_t *ybar = (uint64_t *)(sm + kYS2 * L::yslot() + kNS2 * L::nslot());
-    uint64_t *nbar = ybar + kYS2;
-    volatile int &s_abort = *(volatile int *)(nbar + kNS2);
-    Geo *sgeo = (Geo *)(sm + kYS2 * L::yslot() + kNS2 * L::nslot() + kBar2);
+    uint64_t *ybar = (uint64_t *)(sm + L::YS * L::yslot() + L::NS * L::nslot());
+    uint64_t *nbar = ybar + L::YS;
+    volatile int &s_abort = *(volatile int *)(nbar + L::NS);
+    Geo *sgeo = (Geo *)(sm + L::YS * L::yslot() + L::NS * L::nslot() + L::BAR);
 
     const int tid = threadIdx.x;
     const int tx = tid;
     if (tid == 0) {
-        for (int s = 0; s < kYS2; ++s) mbar_init(&ybar[s], 1);
-        for (int s = 0; s < kNS2; ++s) mbar_init(&nbar[s], 1);
+        for (int s = 0; s < L::YS; ++s) mbar_init(&ybar[s], 1);
+        for (int s = 0; s < L::NS; ++s) mbar_init(&nbar[s], 1);
         fence_barrier_init();
         s_abort = 0;
     }
@@ -774,7 +773,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         const int ny = G.ny;
 
         auto issue_y = [&](int s) {
-            const int slot = s % kYS2;
+            const int slot = s % L::YS;
             if (tid == 0) {
                 uint64_t *bar = &ybar[slot];
                 mbar_arrive_tx(bar, L::ytx());
@@ -788,11 +787,11 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             ynext ^= 1u << slot;
         };
         auto issue_n = [&](int s) {
-            const int slot = s % kNS2;
+            const int slot = s % L::NS;
             if (tid == 0) {
                 uint64_t *bar = &nbar[slot];
                 mbar_arrive_tx(bar, L::ntx());
-                unsigned char *base = sm + kYS2 * L::yslot() + slot * L::nslot();
+                unsigned char *base = sm + L::YS * L::yslot() + slot * L::nslot();
 #pragma unroll
                 for (int ni = 0; ni < 6; ++ni) {
                     const int c = L::nc(ni);
@@ -804,19 +803,19 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
             nnext ^= 1u << slot;
         };
         auto wait_y = [&](int s) -> bool {
-            return mbar_wait(&ybar[s % kYS2], ((ynext >> (s % kYS2)) & 1u) ^ 1u, wlim);
+            return mbar_wait(&ybar[s % L::YS], ((ynext >> (s % L::YS)) & 1u) ^ 1u, wlim);
         };
         auto wait_n = [&](int s) -> bool {
-            return mbar_wait(&nbar[s % kNS2], ((nnext >> (s % kNS2)) & 1u) ^ 1u, wlim);
+            return mbar_wait(&nbar[s % L::NS], ((nnext >> (s % L::NS)) & 1u) ^ 1u, wlim);
         };
 
         // the segment's first copies: the y rows row ja needs and the rows
-        // behind them up to ja + kYS2 - 3, the plane rows ja .. ja + kNS2 - 2
+        // behind them up to ja + L::YS - 3, the plane rows ja .. ja + L::NS - 2
         const int pre_lo = need_lo(ja, ny), pre_hi = need_hi(ja, ny);
         const int seg_hi = need_hi(jb - 1, ny) > pre_hi ? need_hi(jb - 1, ny) : pre_hi;
-        const int y0 = min(seg_hi, max(pre_hi, ja + kYS2 - 3));
+        const int y0 = min(seg_hi, max(pre_hi, ja + L::YS - 3));
         for (int s = pre_lo; s <= y0; ++s) issue_y(s);
-        const int n0 = min(jb - 1, ja + kNS2 - 2);
+        const int n0 = min(jb - 1, ja + L::NS - 2);
         for (int s = ja; s <= n0; ++s) issue_n(s);
         int yissued = y0, nissued = n0;
 
@@ -835,10 +834,10 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         }
         for (int j = ja; j < jb; ++j) {
             // refill the slots of rows every warp has finished (the barrier
-            // that ended row j-1): y rows up to j + kYS2 - 2, plane rows up to
-            // j + kNS2 - 1
-            for (const int yt = min(seg_hi, j + kYS2 - 2); yissued < yt;) issue_y(++yissued);
-            for (const int nt = min(jb - 1, j + kNS2 - 1); nissued < nt;) issue_n(++nissued);
+            // that ended row j-1): y rows up to j + L::YS - 2, plane rows up to
+            // j + L::NS - 1
+            for (const int yt = min(seg_hi, j + L::YS - 2); yissued < yt;) issue_y(++yissued);
+            for (const int nt = min(jb - 1, j + L::NS - 1); nissued < nt;) issue_n(++nissued);
             bool ok = true;
             for (int s = need_lo(j, ny); s <= need_hi(j, ny); ++s) ok = ok && wait_y(s);
             ok = ok && wait_n(j);
@@ -847,7 +846,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
                 s_abort = 1;
             }
             if (active && ok)
-                march2d_node<ST, TX>(sm, G, tx, i, j, xa, xb, xp, xm, Tcn, sT, dst, Fout, *Bp, write_macro);
+                march2d_node<ST, L>(sm, G, tx, i, j, xa, xb, xp, xm, Tcn, sT, dst, Fout, *Bp, write_macro);
             __syncthreads();
             if (s_abort) {
                 aborted = true;
@@ -856,8 +855,8 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
         }
     }
     if (aborted && tid == 0) {
-        for (int s = 0; s < kYS2; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
-        for (int s = 0; s < kNS2; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < L::YS; ++s) mbar_wait(&ybar[s], ((ynext >> s) & 1u) ^ 1u);
+        for (int s = 0; s < L::NS; ++s) mbar_wait(&nbar[s], ((nnext >> s) & 1u) ^ 1u);
     }
 }
 
@@ -872,7 +871,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     (void)Fin;
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    constexpr int TX = L2<ST, 128>::TX;
+    constexpr int TX = L2s<ST>::TX;
     const int ny = G.ny;
     const int64_t G_ = gridDim.x;
     const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
@@ -895,7 +894,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
         Fo = Fout;
         Bp = &B;
     };
-    march2d_run<ST, TX, false>(nseg, seg, cavity, write_macro, err);
+    march2d_run<ST, L2s<ST>, false>(nseg, seg, cavity, write_macro, err);
 }
 
 // many cavities: block b runs segments seg_off[b] .. seg_off[b+1]-1; `cur`
@@ -923,5 +922,5 @@ k_march2d_batch(const BatchDev D, int cur, int write_macro, int *err)
         d = (S *)D.bufs[c].pop[1 - cur];
         Fo = (C *)D.bufs[c].F[1 - cur];
     };
-    march2d_run<ST, TX, true>(s1 - s0, seg, cavity, write_macro, err);
+    march2d_run<ST, L2<ST, TX>, true>(s1 - s0, seg, cavity, write_macro, err);
 }

@@ -77,7 +77,7 @@ def replay(n, total, plan, nodes_of_unit, check_node, ys=4, ns=2):
     `plan` (per CTA, its segments), with a ring of `ys` slots for the planes
     whose stencil reaches along the axis and `ns` slots for the others: at
     step k the copies of slices up to k + ys - 2 and k + ns - 1 are issued
-    (the 3D kernel: 4 and 2; the 2D kernel: kYS2 and kNS2).  The in-plane
+    (the 3D kernel: 4 and 2; the 2D kernels: their layout's YS and NS).  The in-plane
     indices of a node do not depend on the step, so each tile's nodes are
     checked once, at every step kind (first, inner, last slice)."""
     covered = [0] * total
@@ -240,20 +240,12 @@ def test_march3d_plan_balances_the_sms(ntiles, nz, grid):
         assert len(plan) == grid and all(len(s) == 1 for s in plan)
 
 
-def ring2d():
-    """The 2D kernel's ring depths (kYS2, kNS2) as the library's source sets them."""
-    import re
-    src = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
-                            "mpi-multi-process-version_b200", "csrc", "lbm_march.cuh")).read()
-    return (int(re.search(r"#define LBM_YS2 (\d+)", src).group(1)), int(re.search(r"#define LBM_NS2 (\d+)", src).group(1)))
-
-
 @pytest.mark.parametrize("shape", [(2048, 64), (128, 128), (130, 9), (48, 48), (300, 3), (40, 24)])
 @pytest.mark.parametrize("es", [8, 4, 2])
 @pytest.mark.parametrize("tx", [32, 64, 128])
-@pytest.mark.parametrize("ring", ["library", (4, 2), (5, 3), (6, 4)])
+@pytest.mark.parametrize("ring", [(4, 2), (5, 3), (6, 4)])  # batch kernel 4 / 2, single-cavity kernel 6 / 4
 def test_march2d_schedule_and_indices(shape, es, tx, ring):
-    ys, ns = ring2d() if ring == "library" else ring
+    ys, ns = ring
     nx, ny = shape
     total = -(-nx // tx) * ny
     for grid in sorted({1, 2, 5, 148, 592, total}):

@@ -1230,13 +1230,13 @@ static cudaError_t prepare_march3d()
     return cudaSuccess;
 }
 
-template <int ST>
+template <int ST, class L>
 static cudaError_t prepare_march2d()
 {
     static bool done = false;
     if (!done) {
-        cudaError_t e = cudaFuncSetAttribute(k_march2d<ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             L2s<ST>::smem());
+        cudaError_t e = cudaFuncSetAttribute(k_march2d<ST, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             L::smem());
         if (e != cudaSuccess) return e;
         done = true;
     }
@@ -1254,16 +1254,20 @@ static int mbps3(void)
                : 0;
 }
 
+template <int ST, class L>
+static int mbps2(void)
+{
+    if (prepare_march2d<ST, L>() != cudaSuccess) return 0;
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST, L>, L::NT, L::smem()) == cudaSuccess ? n
+                                                                                                             : 0;
+}
+
 template <int ST>
 static int mbps(const Geo &g, int ty)
 {
     if (g.dim == 3) return ty == 4 ? mbps3<ST, 4>() : mbps3<ST, 8>();
-    if (prepare_march2d<ST>() != cudaSuccess) return 0;
-    int n = 0;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_march2d<ST>, L2s<ST>::NT, L2s<ST>::smem()) ==
-                   cudaSuccess
-               ? n
-               : 0;
+    return g.nnode >= kDeepRingNodes ? mbps2<ST, L2d<ST>>() : mbps2<ST, L2s<ST>>();
 }
 
 int march_blocks_per_sm(const Geo &g, int store, int ty)
@@ -1286,6 +1290,20 @@ static cudaError_t launch_march3d(const Geo &g, const TmapSet &m, const void *Fi
                     (S *)pout, (C *)Fout, b, wm, segs, segoff, b.err);
 }
 
+template <int ST, class L>
+static cudaError_t launch_march2d(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
+                                  const Bufs &b, int wm, int nblocks, bool pdl, cudaStream_t s)
+{
+    using S = typename Tr<ST>::S;
+    using C = typename Tr<ST>::C;
+    cudaError_t e = prepare_march2d<ST, L>();
+    if (e != cudaSuccess) return e;
+    const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
+    const int nb = int(nblocks < total ? nblocks : total);
+    return launch_k(k_march2d<ST, L>, nb, L::NT, L::smem(), s, pdl, m, g, (const C *)Fin, (S *)pout, (C *)Fout, b,
+                    wm, total, b.err);
+}
+
 template <int ST>
 static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin, void *pout, void *Fout,
                                 const Bufs &b, int wm, int nblocks, int ty, const int4 *segs, const int *segoff,
@@ -1298,13 +1316,8 @@ static cudaError_t launch_march(const Geo &g, const TmapSet &m, const void *Fin,
         e = ty == 4 ? launch_march3d<ST, 4>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s)
                     : launch_march3d<ST, 8>(g, m, Fin, pout, Fout, b, wm, segs, segoff, nblocks, pdl, s);
     } else {
-        using L = L2s<ST>;
-        e = prepare_march2d<ST>();
-        if (e != cudaSuccess) return e;
-        const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
-        const int nb = int(nblocks < total ? nblocks : total);
-        e = launch_k(k_march2d<ST>, nb, L::NT, L::smem(), s, pdl, m, g, (const C *)Fin, (S *)pout, (C *)Fout, b, wm,
-                     total, b.err);
+        e = g.nnode >= kDeepRingNodes ? launch_march2d<ST, L2d<ST>>(g, m, Fin, pout, Fout, b, wm, nblocks, pdl, s)
+                                      : launch_march2d<ST, L2s<ST>>(g, m, Fin, pout, Fout, b, wm, nblocks, pdl, s);
     }
     ++g_launches;
     return e;
@@ -1488,7 +1501,7 @@ MarchShape march_shape(int dim, int store, int tx, int ty)
         }
         if (tx == 32) { LBM_FILL2(32) }
         else if (tx == 64) { LBM_FILL2(64) }
-        else { LBM_FILL2(128, 6, 4) }  // the single-cavity kernel's layout (L2s)
+        else { LBM_FILL2(128) }
 #undef LBM_FILL2
         for (int c = 0; c < 4; ++c) {
             m.bx[c] = m.TX + ((c & 1) ? 2 * m.HX : 0);

@@ -616,9 +616,18 @@ struct L2 {
     __host__ __device__ static constexpr int smem() { return YS * yslot() + NS * nslot() + BAR + kGeoStage + 128; }
 };
 
-// the single-cavity 2D kernel's layout: 128-node rows, 6 / 4 ring slots
+// the single-cavity 2D kernel's layouts: 128-node rows with 4 / 2 ring slots
+// (four blocks per SM in FP64: lower latency per step, the faster choice up to
+// a few hundred thousand nodes) or 6 / 4 (two blocks per SM, more rows in
+// flight: the faster choice on large domains).  Measured on B200, FP64, per
+// step: 256^2 4.87 us (4 / 2) against 5.70 us (6 / 4); 2048^2 21,666 against
+// 23,400 MLUPS.
 template <int ST>
-using L2s = L2<ST, 128, 6, 4>;
+using L2s = L2<ST, 128, 4, 2>;
+template <int ST>
+using L2d = L2<ST, 128, 6, 4>;
+// nodes from which the single-cavity 2D kernel uses the deep ring
+constexpr int64_t kDeepRingNodes = int64_t(1) << 20;
 
 // One node of the 2D march at row j, from the ring slots in shared memory:
 // interpolation, walls, macro, collision, stores.
@@ -862,7 +871,7 @@ __device__ __forceinline__ void march2d_run(int nseg, SegFn seg, CavFn cavity, i
 
 // one cavity: each block takes an equal contiguous share of the
 // (strip-major, row-minor) work items
-template <int ST>
+template <int ST, class L>
 __global__ void __launch_bounds__(128, 4)
 k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<ST>::C *__restrict__ Fin,
           typename Tr<ST>::S *__restrict__ dst, typename Tr<ST>::C *__restrict__ Fout, const Bufs B,
@@ -871,7 +880,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     (void)Fin;
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
-    constexpr int TX = L2s<ST>::TX;
+    constexpr int TX = L::TX;
     const int ny = G.ny;
     const int64_t G_ = gridDim.x;
     const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
@@ -894,7 +903,7 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
         Fo = Fout;
         Bp = &B;
     };
-    march2d_run<ST, L2s<ST>, false>(nseg, seg, cavity, write_macro, err);
+    march2d_run<ST, L, false>(nseg, seg, cavity, write_macro, err);
 }
 
 // many cavities: block b runs segments seg_off[b] .. seg_off[b+1]-1; `cur`

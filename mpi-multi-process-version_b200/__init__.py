@@ -7,6 +7,7 @@ from .lbm import (EXPORTS, GRID, MODE, NOALLOC_MAX_NODES, STORE, Batch, Cavity, 
 
 from . import studies  # noqa: E402
 from . import sharding  # noqa: E402
+from . import slabs  # noqa: E402
 from . import surrogate  # noqa: E402
 from . import warmstart  # noqa: E402
 

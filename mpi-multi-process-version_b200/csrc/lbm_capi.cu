@@ -561,7 +561,8 @@ static int resolve_path(lbm_handle *h)
     // small 2D domains: every iteration of an lbm_step call in one resident
     // cooperative launch (the per-iteration launch gap dominates there)
     h->resident = 0;
-    if (!h->use_march && h->p.dim == 2 && h->resident_opt && h->owns_stream && h->d_bar) {
+    if (!h->use_march && h->p.dim == 2 && h->resident_opt && h->owns_stream && h->d_bar && h->geo.jlo == 0 &&
+        h->geo.jhi == h->geo.ny) {
         const int nb = h->p.mode == LBM_MODE_EXACT ? exact::resident_blocks(h->geo, h->p.storage, h->device)
                                                    : fast::resident_blocks(h->geo, h->p.storage, h->device);
         if (nb > 0 && (int64_t)nb * 256 >= h->geo.nnode) h->resident = nb;
@@ -613,6 +614,8 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
     memset(&g, 0, sizeof g);
     g.dim = p->dim;
     g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
+    g.jlo = 0;
+    g.jhi = g.ny;
     // rows padded to 16 bytes for every storage type (TMA stride rule)
     g.pitch = (g.nx + 7) / 8 * 8;
     g.slab = g.pitch * g.ny;
@@ -1095,6 +1098,84 @@ extern "C" int lbm_nusselt(lbm_handle *h, double *nu_hot, double *nu_cold)
     if (nu_cold) *nu_cold = s[1] / s[2];
     if (!isfinite(s[0]) || !isfinite(s[1])) return fail(LBM_ERR_NONFINITE, "nusselt: non-finite");
     return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// slabs: one 2D domain split along y over several handles (the reference's
+// row decomposition with its per-step ghost exchange, `update`, 2M:572-589)
+// ---------------------------------------------------------------------------
+extern "C" int lbm_create_slab(const lbm_params *p, const double *x, const double *y, int32_t y0, int32_t y1,
+                               lbm_handle **out)
+{
+    if (!out) return fail(LBM_ERR_PARAM, "out is NULL");
+    *out = nullptr;
+    if (!p) return fail(LBM_ERR_PARAM, "params NULL");
+    if (p->dim != 2) return fail(LBM_ERR_UNSUPPORTED, "slabs are 2D (rows of the y axis)");
+    int st = validate(p);
+    if (st) return st;
+    if (!x || !y) return fail(LBM_ERR_PARAM, "coordinates missing");
+    if (y0 < 0 || y1 > p->ny || y1 - y0 < 2) return fail(LBM_ERR_PARAM, "slab rows [%d, %d) of %d", y0, y1, p->ny);
+    // the slab's buffer: its rows plus one ghost row on each side that has a neighbour
+    const int b0 = y0 > 0 ? y0 - 1 : 0, b1 = y1 < p->ny ? y1 + 1 : p->ny;
+    lbm_params q = *p;
+    q.ny = b1 - b0;
+    st = lbm_create(&q, x, y + b0, nullptr, out);
+    if (st) return st;
+    lbm_handle *h = *out;
+    h->geo.jlo = y0 - b0;
+    h->geo.jhi = y1 - b0;
+    st = resolve_path(h);
+    if (st) {
+        lbm_destroy(h);
+        *out = nullptr;
+    }
+    return st;
+}
+
+// row `r` (local) of every population plane of the newest state <-> a packed
+// device buffer [Q + QT][nx] of the storage type, on the handle's stream
+static int halo_copy(lbm_handle *h, int32_t side, void *buf, bool pack)
+{
+    CHECK_H(h);
+    if (h->geo.dim != 2) return fail(LBM_ERR_UNSUPPORTED, "halo rows are 2D");
+    if (side != 0 && side != 1) return fail(LBM_ERR_PARAM, "side must be 0 (low y) or 1 (high y)");
+    if (!buf) return fail(LBM_ERR_PARAM, "buffer NULL");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "halo exchange before an init call");
+    const Geo &g = h->geo;
+    if (side == 0 ? g.jlo == 0 : g.jhi == g.ny) return fail(LBM_ERR_PARAM, "no neighbour on side %d (a wall)", side);
+    // pack: the slab's first / last own row; unpack: the ghost row below / above it
+    const int row = pack ? (side == 0 ? g.jlo : g.jhi - 1) : (side == 0 ? g.jlo - 1 : g.jhi);
+    const size_t es = (size_t)h->esize, w = (size_t)g.nx * es;
+    unsigned char *pop = (unsigned char *)h->bufs.pop[h->cur] + (size_t)row * g.pitch * es;
+    const size_t planes = (size_t)(h->Q + h->QT), pstride = (size_t)g.plane * es;
+    CU(pack ? cudaMemcpy2DAsync(buf, w, pop, pstride, w, planes, cudaMemcpyDeviceToDevice, h->stream)
+            : cudaMemcpy2DAsync(pop, pstride, buf, w, w, planes, cudaMemcpyDeviceToDevice, h->stream));
+    return LBM_OK;
+}
+
+extern "C" int lbm_halo_pack(lbm_handle *h, int32_t side, void *dev_buf) { return halo_copy(h, side, dev_buf, true); }
+
+extern "C" int lbm_halo_unpack(lbm_handle *h, int32_t side, const void *dev_buf)
+{
+    return halo_copy(h, side, const_cast<void *>(dev_buf), false);
+}
+
+extern "C" int lbm_check_sums(lbm_handle *h, double sums[4])
+{
+    CHECK_H(h);
+    if (!sums) return fail(LBM_ERR_PARAM, "sums NULL");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_check_sums before an init call");
+    CU(reduce_check(h->geo, h->bufs, h->stream));
+    return read_scal(h, 0, 4, sums);
+}
+
+extern "C" int lbm_nusselt_sums(lbm_handle *h, double sums[3])
+{
+    CHECK_H(h);
+    if (!sums) return fail(LBM_ERR_PARAM, "sums NULL");
+    if (h->phase == 0) return fail(LBM_ERR_STATE, "lbm_nusselt_sums before an init call");
+    CU(reduce_nusselt(h->geo, h->bufs, h->stream));
+    return read_scal(h, 4, 3, sums);
 }
 
 extern "C" int lbm_sums(lbm_handle *h, double *mass, double *energy)

@@ -12,6 +12,9 @@ namespace lbm {
 // Geometry and physics constants a kernel needs, passed by value.
 struct Geo {
     int dim, nx, ny, nz;
+    int jlo, jhi;    // 2D: the rows the step kernels compute and the reductions sum, [jlo, jhi):
+                     // 0, ny for a whole cavity; a slab (lbm_create_slab) leaves out its ghost rows
+    int pad_[2];
     int64_t pitch;   // elements between rows of a population plane
     int64_t slab;    // elements between z-planes (pitch * ny)
     int64_t plane;   // elements between population planes

@@ -334,7 +334,7 @@ k_step2d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     if (!B.ctl->active) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    if (i >= G.nx || j >= G.ny) return;
+    if (i >= G.nx || j < G.jlo || j >= G.jhi) return;  // a slab's ghost rows come from its neighbours
     step2d_node<ST, KIND>(G, src, Fin, dst, Fout, B, write_macro, i, j);
 }
 
@@ -1298,7 +1298,7 @@ static cudaError_t launch_march2d(const Geo &g, const TmapSet &m, const void *Fi
     using C = typename Tr<ST>::C;
     cudaError_t e = prepare_march2d<ST, L>();
     if (e != cudaSuccess) return e;
-    const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * g.ny;
+    const int64_t total = (int64_t)((g.nx + L::TX - 1) / L::TX) * (g.jhi - g.jlo);
     const int nb = int(nblocks < total ? nblocks : total);
     return launch_k(k_march2d<ST, L>, nb, L::NT, L::smem(), s, pdl, m, g, (const C *)Fin, (S *)pout, (C *)Fout, b,
                     wm, total, b.err);

@@ -881,19 +881,21 @@ k_march2d(const __grid_constant__ TmapSet maps, const Geo G, const typename Tr<S
     using S = typename Tr<ST>::S;
     using C = typename Tr<ST>::C;
     constexpr int TX = L::TX;
-    const int ny = G.ny;
+    // the rows the kernel computes, [jlo, jhi): all rows, or a slab's rows
+    // without its ghost rows
+    const int nr = G.jhi - G.jlo;
     const int64_t G_ = gridDim.x;
     const int64_t ubeg = total * blockIdx.x / G_, uend = total * (blockIdx.x + 1) / G_;
     // segments: the block's range split at strip boundaries
-    const int nseg = ubeg >= uend ? 0 : int((uend - 1) / ny - ubeg / ny + 1);
+    const int nseg = ubeg >= uend ? 0 : int((uend - 1) / nr - ubeg / nr + 1);
     auto seg = [&](int k, int &cav, int &i0, int &ja, int &jb) {
-        const int64_t t = ubeg / ny + k;
-        const int64_t lo = t * ny > ubeg ? t * ny : ubeg;
-        const int64_t hi = (t + 1) * ny < uend ? (t + 1) * ny : uend;
+        const int64_t t = ubeg / nr + k;
+        const int64_t lo = t * nr > ubeg ? t * nr : ubeg;
+        const int64_t hi = (t + 1) * nr < uend ? (t + 1) * nr : uend;
         cav = 0;
         i0 = int(t) * TX;
-        ja = int(lo - t * ny);
-        jb = int(hi - t * ny);
+        ja = G.jlo + int(lo - t * nr);
+        jb = G.jlo + int(hi - t * nr);
     };
     const CUtensorMap *mp = &maps.m[0];
     auto cavity = [&](int, const Geo *&Gp, const CUtensorMap *&m, S *&d, C *&Fo, const Bufs *&Bp) {

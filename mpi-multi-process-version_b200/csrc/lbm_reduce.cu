@@ -60,7 +60,12 @@ __device__ __forceinline__ void check_block(const Geo &G, const Bufs &B, int blk
 {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t stride = (int64_t)kRedBlocks * blockDim.x;
+    const bool rows = G.dim == 2 && (G.jlo > 0 || G.jhi < G.ny);  // a slab: its own rows only
     for (int64_t n = (int64_t)blk * blockDim.x + threadIdx.x; n < G.nnode; n += stride) {
+        if (rows) {
+            const int j = int(n / G.nx);
+            if (j < G.jlo || j >= G.jhi) continue;
+        }
         const double u = B.u[n], v = B.v[n], T = B.T[n];
         const double du = u - B.up[n], dv = v - B.vp[n], dT = T - B.Tp[n];
         if (G.dim == 2) {
@@ -220,7 +225,7 @@ __global__ void __launch_bounds__(kRedThreads) k_nusselt(const Geo G, const Bufs
         const double *x = G.coord[0];
         const int nx = G.nx;
         const double xlo = x[1] - 0.5 * G.dt, xhi = x[nx] + 0.5 * G.dt;
-        for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < G.ny; j += stride) {
+        for (int64_t j = G.jlo + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < G.jhi; j += stride) {
             const double *T = B.T + j * nx;
             const double gh = wall_gradient(xlo, G.Thot, x[1], T[0], x[2], T[1]);
             const double gc = wall_gradient(xhi, G.Tcold, x[nx], T[nx - 1], x[nx - 1], T[nx - 2]);
@@ -266,6 +271,7 @@ __global__ void __launch_bounds__(kRedThreads) k_sums(const Geo G, const Bufs B)
         const int i = int(n % G.nx);
         const int j = int((n / G.nx) % G.ny);
         const int k = int(n / ((int64_t)G.nx * G.ny));
+        if (G.dim == 2 && (j < G.jlo || j >= G.jhi)) continue;  // a slab's ghost rows
         const double vol = G.cellw[0][i] * G.cellw[1][j] * (G.dim == 3 ? G.cellw[2][k] : 1.0);
         acc[0] += B.rho[n] * vol;
         acc[1] += B.T[n] * vol;

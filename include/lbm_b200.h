@@ -206,36 +206,42 @@ int lbm_nusselt(lbm_handle *h, double *nu_hot, double *nu_cold);
 int lbm_sums(lbm_handle *h, double *mass, double *energy);
 
 /* ------------------------------------------------------------------------ */
-/* Slabs: one 2D domain split along y over several handles (on one GPU, on
- * several GPUs of a process, or one per rank).  Replaces the reference's row
- * decomposition (natural-convection_2dim_block.f90: StartEnd, the ghost rows
- * of f_post / g_post) and its per-step ghost exchange `update`
- * (natural-convection_2dim_mono.f90:572-589, 2dim_block.f90:602-658).
+/* Slabs: one domain split along its slowest axis (y in 2D, z in 3D) over
+ * several handles (on one GPU, on several GPUs of a process, or one per
+ * rank).  Replaces the reference's slab decomposition (the ghost rows / planes
+ * of f_post / g_post; natural-convection_2dim_mono.f90 and 3dim_mono.f90 split
+ * y and z over ranks, StartEnd) and its per-step ghost exchange `update`
+ * (natural-convection_2dim_mono.f90:572-589, 2dim_block.f90:602-658,
+ * 3dim_mono.f90:732-749).
  *
- * lbm_create_slab: p and the coordinate arrays x(0:nx+1), y(0:ny+1) describe
- * the WHOLE domain; the handle owns rows [y0, y1) (0-based, at least 2) plus
- * one ghost row on each side that has a neighbouring slab.  Every other call
- * works on the handle as on a cavity of the slab's rows plus ghosts (the
- * fields of lbm_get_macro / lbm_init_* are (nx, rows incl. ghosts)); its step
- * kernels compute only its own rows, lbm_check_sums / lbm_nusselt_sums sum
- * only them.  lbm_run and batches do not take slabs.
+ * lbm_create_slab: p and the coordinate arrays x(0:nx+1), y(0:ny+1) and, in
+ * 3D, z(0:nz+1) describe the WHOLE domain (z NULL in 2D); the handle owns
+ * layers [lo, hi) of the split axis (rows in 2D, z-slices in 3D; 0-based, at
+ * least 2) plus one ghost layer on each side that has a neighbouring slab.
+ * Every other call works on the handle as on a cavity of the slab's layers
+ * plus ghosts (the fields of lbm_get_macro / lbm_init_* are (nx, rows incl.
+ * ghosts) in 2D, (nx, ny, slices incl. ghosts) in 3D); its step kernels
+ * compute only its own layers, lbm_check_sums / lbm_nusselt_sums sum only
+ * them.  lbm_run and batches do not take slabs.
  *
  * After every lbm_step(h, 1) of all slabs, each interface is exchanged:
  * lbm_halo_pack(lower, 1, buf) and lbm_halo_pack(upper, 0, buf') copy the
- * slabs' boundary rows of every population plane into device buffers of
- * (Q+QT) x nx values of the storage type (14 x nx in 2D); once both copies
- * are complete (they run on each handle's stream), lbm_halo_unpack(upper, 0,
- * buf) and lbm_halo_unpack(lower, 1, buf') write them into the neighbours'
- * ghost rows.  The buffers may move between devices or ranks (peer copy,
- * NCCL) in between.  side 0 is the low-y side, 1 the high-y side; a side
+ * slabs' boundary layers of every population plane into device buffers of
+ * lbm_halo_size bytes (2D: (Q+QT) x nx values of the storage type, 14 x nx;
+ * 3D: (Q+QT) x (padded row pitch x ny), 26 slices); once both copies are
+ * complete (they run on each handle's stream), lbm_halo_unpack(upper, 0, buf)
+ * and lbm_halo_unpack(lower, 1, buf') write them into the neighbours' ghost
+ * layers.  The buffers may move between devices or ranks (peer copy, NCCL) in
+ * between.  side 0 is the low end of the split axis, 1 the high end; a side
  * without a neighbour (a wall) is an error. */
-int lbm_create_slab(const lbm_params *p, const double *x, const double *y, int32_t y0, int32_t y1,
+int lbm_create_slab(const lbm_params *p, const double *x, const double *y, const double *z, int32_t lo, int32_t hi,
                     lbm_handle **out);
+int lbm_halo_size(const lbm_handle *h, int64_t *bytes);
 int lbm_halo_pack(lbm_handle *h, int32_t side, void *dev_buf);
 int lbm_halo_unpack(lbm_handle *h, int32_t side, const void *dev_buf);
 
 /* The sums behind lbm_check (sum |du|^2, sum |u|^2, sum dT^2, sum T^2, over
- * the handle's own rows; the previous fields are updated as by lbm_check) and
+ * the handle's own layers; the previous fields are updated as by lbm_check) and
  * behind lbm_nusselt (sum Nu_hot w, sum Nu_cold w, sum w), so that slabs
  * combine them: errorU = sqrt(sum of the first) / sqrt(sum of the second)
  * (2M:784), Nu = sum / sum.  No counterpart beyond check() itself. */

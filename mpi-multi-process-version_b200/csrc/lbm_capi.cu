@@ -473,7 +473,12 @@ static int upload_plan3d(lbm_handle *h, int G)
     const int ntiles = ((h->geo.nx + ms.TX - 1) / ms.TX) * ((h->geo.ny + ms.TY - 1) / ms.TY);
     std::vector<int4> segs;
     std::vector<int> off;
-    const int nb = lbm::plan_march3d(ntiles, h->geo.nz, G, h->plan_opt, segs, off);
+    // the slices the handle computes: all of them, or a slab's own [klo, khi)
+    const int nb = lbm::plan_march3d(ntiles, h->geo.khi - h->geo.klo, G, h->plan_opt, segs, off);
+    for (int4 &s : segs) {
+        s.y += h->geo.klo;
+        s.z += h->geo.klo;
+    }
     if (segs.size() > h->msegs_cap) {
         if (h->d_msegs) cudaFree(h->d_msegs);
         h->d_msegs = nullptr;
@@ -616,6 +621,8 @@ extern "C" int lbm_create(const lbm_params *p, const double *x, const double *y,
     g.nx = h->p.nx; g.ny = h->p.ny; g.nz = h->p.nz;
     g.jlo = 0;
     g.jhi = g.ny;
+    g.klo = 0;
+    g.khi = g.nz;
     // rows padded to 16 bytes for every storage type (TMA stride rule)
     g.pitch = (g.nx + 7) / 8 * 8;
     g.slab = g.pitch * g.ny;
@@ -1101,29 +1108,36 @@ extern "C" int lbm_nusselt(lbm_handle *h, double *nu_hot, double *nu_cold)
 }
 
 // ---------------------------------------------------------------------------
-// slabs: one 2D domain split along y over several handles (the reference's
-// row decomposition with its per-step ghost exchange, `update`, 2M:572-589)
+// slabs: one domain split along its slowest axis (y in 2D, z in 3D) over
+// several handles: the reference's slab decomposition with its per-step ghost
+// exchange, `update` (2M:572-589 rows, 3M:732-749 z-planes)
 // ---------------------------------------------------------------------------
-extern "C" int lbm_create_slab(const lbm_params *p, const double *x, const double *y, int32_t y0, int32_t y1,
-                               lbm_handle **out)
+extern "C" int lbm_create_slab(const lbm_params *p, const double *x, const double *y, const double *z, int32_t lo,
+                               int32_t hi, lbm_handle **out)
 {
     if (!out) return fail(LBM_ERR_PARAM, "out is NULL");
     *out = nullptr;
     if (!p) return fail(LBM_ERR_PARAM, "params NULL");
-    if (p->dim != 2) return fail(LBM_ERR_UNSUPPORTED, "slabs are 2D (rows of the y axis)");
     int st = validate(p);
     if (st) return st;
-    if (!x || !y) return fail(LBM_ERR_PARAM, "coordinates missing");
-    if (y0 < 0 || y1 > p->ny || y1 - y0 < 2) return fail(LBM_ERR_PARAM, "slab rows [%d, %d) of %d", y0, y1, p->ny);
-    // the slab's buffer: its rows plus one ghost row on each side that has a neighbour
-    const int b0 = y0 > 0 ? y0 - 1 : 0, b1 = y1 < p->ny ? y1 + 1 : p->ny;
+    if (!x || !y || (p->dim == 3 && !z)) return fail(LBM_ERR_PARAM, "coordinates missing");
+    const int n = p->dim == 2 ? p->ny : p->nz;  // the split axis
+    if (lo < 0 || hi > n || hi - lo < 2) return fail(LBM_ERR_PARAM, "slab layers [%d, %d) of %d", lo, hi, n);
+    // the slab's buffer: its layers plus one ghost layer on each side that has a neighbour
+    const int b0 = lo > 0 ? lo - 1 : 0, b1 = hi < n ? hi + 1 : n;
     lbm_params q = *p;
-    q.ny = b1 - b0;
-    st = lbm_create(&q, x, y + b0, nullptr, out);
+    if (p->dim == 2) q.ny = b1 - b0;
+    else q.nz = b1 - b0;
+    st = p->dim == 2 ? lbm_create(&q, x, y + b0, nullptr, out) : lbm_create(&q, x, y, z + b0, out);
     if (st) return st;
     lbm_handle *h = *out;
-    h->geo.jlo = y0 - b0;
-    h->geo.jhi = y1 - b0;
+    if (p->dim == 2) {
+        h->geo.jlo = lo - b0;
+        h->geo.jhi = hi - b0;
+    } else {
+        h->geo.klo = lo - b0;
+        h->geo.khi = hi - b0;
+    }
     st = resolve_path(h);
     if (st) {
         lbm_destroy(h);
@@ -1132,21 +1146,34 @@ extern "C" int lbm_create_slab(const lbm_params *p, const double *x, const doubl
     return st;
 }
 
-// row `r` (local) of every population plane of the newest state <-> a packed
-// device buffer [Q + QT][nx] of the storage type, on the handle's stream
+// One layer of the newest state in every population plane: a row (2D) or a
+// z-slice of pitch x ny elements, padding columns included (3D).
+static size_t halo_layer(const Geo &g) { return g.dim == 2 ? (size_t)g.nx : (size_t)g.slab; }
+
+extern "C" int lbm_halo_size(const lbm_handle *h, int64_t *bytes)
+{
+    CHECK_H(h);
+    if (!bytes) return fail(LBM_ERR_PARAM, "bytes NULL");
+    *bytes = (int64_t)((size_t)(h->Q + h->QT) * halo_layer(h->geo) * (size_t)h->esize);
+    return LBM_OK;
+}
+
+// layer `r` (local) of every population plane of the newest state <-> a packed
+// device buffer [Q + QT][layer] of the storage type, on the handle's stream
 static int halo_copy(lbm_handle *h, int32_t side, void *buf, bool pack)
 {
     CHECK_H(h);
-    if (h->geo.dim != 2) return fail(LBM_ERR_UNSUPPORTED, "halo rows are 2D");
-    if (side != 0 && side != 1) return fail(LBM_ERR_PARAM, "side must be 0 (low y) or 1 (high y)");
+    if (side != 0 && side != 1) return fail(LBM_ERR_PARAM, "side must be 0 (low end) or 1 (high end)");
     if (!buf) return fail(LBM_ERR_PARAM, "buffer NULL");
     if (h->phase == 0) return fail(LBM_ERR_STATE, "halo exchange before an init call");
     const Geo &g = h->geo;
-    if (side == 0 ? g.jlo == 0 : g.jhi == g.ny) return fail(LBM_ERR_PARAM, "no neighbour on side %d (a wall)", side);
-    // pack: the slab's first / last own row; unpack: the ghost row below / above it
-    const int row = pack ? (side == 0 ? g.jlo : g.jhi - 1) : (side == 0 ? g.jlo - 1 : g.jhi);
-    const size_t es = (size_t)h->esize, w = (size_t)g.nx * es;
-    unsigned char *pop = (unsigned char *)h->bufs.pop[h->cur] + (size_t)row * g.pitch * es;
+    const bool d2 = g.dim == 2;
+    const int lo = d2 ? g.jlo : g.klo, hi = d2 ? g.jhi : g.khi, n = d2 ? g.ny : g.nz;
+    if (side == 0 ? lo == 0 : hi == n) return fail(LBM_ERR_PARAM, "no neighbour on side %d (a wall)", side);
+    // pack: the slab's first / last own layer; unpack: the ghost layer below / above it
+    const int r = pack ? (side == 0 ? lo : hi - 1) : (side == 0 ? lo - 1 : hi);
+    const size_t es = (size_t)h->esize, w = halo_layer(g) * es;
+    unsigned char *pop = (unsigned char *)h->bufs.pop[h->cur] + (size_t)r * (size_t)(d2 ? g.pitch : g.slab) * es;
     const size_t planes = (size_t)(h->Q + h->QT), pstride = (size_t)g.plane * es;
     CU(pack ? cudaMemcpy2DAsync(buf, w, pop, pstride, w, planes, cudaMemcpyDeviceToDevice, h->stream)
             : cudaMemcpy2DAsync(pop, pstride, buf, w, w, planes, cudaMemcpyDeviceToDevice, h->stream));

@@ -14,7 +14,8 @@ struct Geo {
     int dim, nx, ny, nz;
     int jlo, jhi;    // 2D: the rows the step kernels compute and the reductions sum, [jlo, jhi):
                      // 0, ny for a whole cavity; a slab (lbm_create_slab) leaves out its ghost rows
-    int pad_[2];
+    int klo, khi;    // 3D: the z-slices the step kernels compute and the reductions sum, [klo, khi):
+                     // 0, nz for a whole cavity; a 3D slab leaves out its ghost slices
     int64_t pitch;   // elements between rows of a population plane
     int64_t slab;    // elements between z-planes (pitch * ny)
     int64_t plane;   // elements between population planes

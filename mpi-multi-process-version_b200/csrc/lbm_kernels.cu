@@ -773,7 +773,7 @@ k_step3d(const Geo G, const typename Tr<ST>::S *__restrict__ src, const typename
     if (!B.ctl->active) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
+    const int k = G.klo + blockIdx.z;  // a slab's ghost slices come from its neighbours
     if (i >= G.nx || j >= G.ny) return;
     const int64_t P = G.plane;
     const int64_t id = (int64_t)k * G.slab + (int64_t)j * G.pitch + i;
@@ -1077,7 +1077,7 @@ static cudaError_t launch_step(const Geo &g, const void *pin, const void *Fin, v
         else
             k_step2d<ST, 1><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
     } else {
-        dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.nz);
+        dim3 grd((g.nx + 31) / 32, (g.ny + 7) / 8, g.khi - g.klo);
         if (kind == 0)
             k_step3d<ST, 0><<<grd, blk, 0, s>>>(g, (const S *)pin, (const C *)Fin, (S *)pout, (C *)Fout, b, wm);
         else

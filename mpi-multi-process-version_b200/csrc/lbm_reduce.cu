@@ -60,11 +60,15 @@ __device__ __forceinline__ void check_block(const Geo &G, const Bufs &B, int blk
 {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t stride = (int64_t)kRedBlocks * blockDim.x;
-    const bool rows = G.dim == 2 && (G.jlo > 0 || G.jhi < G.ny);  // a slab: its own rows only
+    // a slab: its own rows (2D) or z-slices (3D) only
+    const bool d2 = G.dim == 2;
+    const int lo = d2 ? G.jlo : G.klo, hi = d2 ? G.jhi : G.khi;
+    const bool part = lo > 0 || hi < (d2 ? G.ny : G.nz);
+    const int64_t layer = d2 ? (int64_t)G.nx : (int64_t)G.nx * G.ny;
     for (int64_t n = (int64_t)blk * blockDim.x + threadIdx.x; n < G.nnode; n += stride) {
-        if (rows) {
-            const int j = int(n / G.nx);
-            if (j < G.jlo || j >= G.jhi) continue;
+        if (part) {
+            const int64_t l = n / layer;
+            if (l < lo || l >= hi) continue;
         }
         const double u = B.u[n], v = B.v[n], T = B.T[n];
         const double du = u - B.up[n], dv = v - B.vp[n], dT = T - B.Tp[n];
@@ -238,9 +242,9 @@ __global__ void __launch_bounds__(kRedThreads) k_nusselt(const Geo G, const Bufs
         const double *y = G.coord[1];
         const int nx = G.nx, ny = G.ny;
         const double ylo = y[1] - 0.5 * G.dt, yhi = y[ny] + 0.5 * G.dt;
-        const int64_t nwall = (int64_t)nx * G.nz;
+        const int64_t nwall = (int64_t)nx * (G.khi - G.klo);  // a slab's own z-slices
         for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nwall; t += stride) {
-            const int i = int(t % nx), k = int(t / nx);
+            const int i = int(t % nx), k = G.klo + int(t / nx);
             const double *T = B.T + (int64_t)k * nx * ny + i;
             const double gh = wall_gradient(ylo, G.Thot, y[1], T[0], y[2], T[nx]);
             const double gc = wall_gradient(yhi, G.Tcold, y[ny], T[(int64_t)(ny - 1) * nx],
@@ -271,7 +275,7 @@ __global__ void __launch_bounds__(kRedThreads) k_sums(const Geo G, const Bufs B)
         const int i = int(n % G.nx);
         const int j = int((n / G.nx) % G.ny);
         const int k = int(n / ((int64_t)G.nx * G.ny));
-        if (G.dim == 2 && (j < G.jlo || j >= G.jhi)) continue;  // a slab's ghost rows
+        if (G.dim == 2 ? (j < G.jlo || j >= G.jhi) : (k < G.klo || k >= G.khi)) continue;  // a slab's ghosts
         const double vol = G.cellw[0][i] * G.cellw[1][j] * (G.dim == 3 ? G.cellw[2][k] : 1.0);
         acc[0] += B.rho[n] * vol;
         acc[1] += B.T[n] * vol;

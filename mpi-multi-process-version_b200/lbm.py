@@ -37,7 +37,7 @@ EXPORTS = [
     "lbm_batch_step", "lbm_batch_check", "lbm_batch_nusselt", "lbm_batch_run", "lbm_batch_run_masked", "lbm_batch_tune",
     "lbm_batch_set_option", "lbm_batch_get_option", "lbm_batch_synchronize", "lbm_batch_stream",
     "lbm_batch_set_storage", "lbm_batch_run_mixed",
-    "lbm_create_slab", "lbm_halo_pack", "lbm_halo_unpack", "lbm_check_sums", "lbm_nusselt_sums",
+    "lbm_create_slab", "lbm_halo_size", "lbm_halo_pack", "lbm_halo_unpack", "lbm_check_sums", "lbm_nusselt_sums",
 ]
 BATCH_OPT = {"tile": 1, "nblocks": 2, "persistent": 3, "graphs": 4, "growth": 5, "storages": 6, "storage": 7,
              "pdl": 8}
@@ -82,8 +82,9 @@ def lib():
                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp]
         L.lbm_derived_params.argtypes = [ctypes.POINTER(lbm_params), _dp]
         L.lbm_create.argtypes = [ctypes.POINTER(lbm_params), _dp, _dp, _dp, ctypes.POINTER(ctypes.c_void_p)]
-        L.lbm_create_slab.argtypes = [ctypes.POINTER(lbm_params), _dp, _dp, ctypes.c_int32, ctypes.c_int32,
+        L.lbm_create_slab.argtypes = [ctypes.POINTER(lbm_params), _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.POINTER(ctypes.c_void_p)]
+        L.lbm_halo_size.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64)]
         L.lbm_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
         L.lbm_halo_unpack.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
         L.lbm_check_sums.argtypes = [ctypes.c_void_p, _dp]

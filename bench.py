@@ -442,7 +442,13 @@ def steady_cold_arm(pkg, cases, max_steps, device):
     return steps, nu, t
 
 
-def time_to_steady(pkg, ncases, max_steps, device):
+def _tau_delta(text):
+    """'TAU,DELTA' -> (float, int)."""
+    tau, delta = text.split(",")
+    return float(tau), int(delta)
+
+
+def time_to_steady(pkg, ncases, max_steps, device, extrapolate=None):
     """Both arms of the time-to-steady comparison on the first `ncases`
     held-out cavities, timed here: FP64 cold one cavity at a time against
     mixed precision (member by member, FP32 to 1e-5 then FP64) + one batch +
@@ -451,7 +457,8 @@ def time_to_steady(pkg, ncases, max_steps, device):
     model = W.WarmStart.load(MODEL_PATH, device=device)
     cases = W.sample_cases(200, seed=2000)[:ncases]
     steps_cold, nu_cold, t_cold = steady_cold_arm(pkg, cases, max_steps, device)
-    r = W.solve(cases, init="warm", model=model, storage="auto", max_steps=max_steps, device=device)
+    r = W.solve(cases, init="warm", model=model, storage="auto", max_steps=max_steps, device=device,
+                extrapolate=extrapolate)
     nu_cold = np.asarray(nu_cold)
     err = np.abs(np.asarray(r["nu_hot"]) - nu_cold) / np.abs(nu_cold)
     conv = np.asarray(r["status"]) == 1
@@ -463,6 +470,7 @@ def time_to_steady(pkg, ncases, max_steps, device):
             "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()), "max_nu_rel_err": float(err.max()),
             "fallbacks": int(np.sum(r["fallback"])), "storage_chosen": r["tuned"]["chosen"],
             "tuned_mlups": {k: r["tuned"][k]["mlups"] for k in ("f64", "f32")},
+            "extrapolate": None if extrapolate is None else {"tau": extrapolate[0], "delta": extrapolate[1]},
             "arms": "FP64 from the conduction state, one cavity per launch vs. one persistent batch + learned "
                     "warm start + storage chosen by the autotuner (mixed precision member by member if FP32 "
                     "stepping pays for its hand-over, else FP64); prediction, tuning and initialisation timed"}
@@ -560,7 +568,8 @@ def run_steady(args, world, rank, local):
         time.sleep(0.3)
     l0 = pkg.kernel_launches()
     _barrier(world)
-    r = W.solve(cases, init="warm", model=model, storage=args.steady_storage, max_steps=max_steps, device=local)
+    r = W.solve(cases, init="warm", model=model, storage=args.steady_storage, max_steps=max_steps, device=local,
+                extrapolate=args.steady_extrapolate)
     launches = pkg.kernel_launches() - l0
     clocks = sampler.stop() if sampler else None
     t_mixed = _reduce(r["seconds"], world, "max")  # prediction and initialisation included
@@ -600,7 +609,8 @@ def run_steady(args, world, rank, local):
                                "converged_warm_batched": int(conv.sum()),
                                "storage_chosen": (r["tuned"] or {}).get("chosen", args.steady_storage),
                                "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()),
-                               "max_nu_rel_err": float(err.max()), "fallbacks": int(np.sum(r["fallback"]))},
+                               "max_nu_rel_err": float(err.max()), "fallbacks": int(np.sum(r["fallback"])),
+                               "extrapolate": args.steady_extrapolate},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "bytes_per_lup": bpl,
                          "kernel": "k_march2d_batch, the warm arm's algorithmic bytes (240 B per FP64 update, "
@@ -633,6 +643,9 @@ def main():
                     help="cavity workloads: held-out cavities of the time_to_steady object (0: leave it out)")
     ap.add_argument("--steady-storage", default="auto", choices=["auto", "mixed", "f64", "f32"],
                     help="steady workload: storage policy of the warm-started batch")
+    ap.add_argument("--steady-extrapolate", type=_tau_delta, default=None, metavar="TAU,DELTA",
+                    help="steady workload and time_to_steady: one extrapolation of each member's slowest mode at "
+                         "residual TAU from states DELTA iterations apart (e.g. 3e-5,10000); off by default")
     ap.add_argument("--steady-max-steps", type=int, default=3_000_000,
                     help="time_to_steady: iteration cap per cavity, high enough for every case of both arms")
     ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")
@@ -776,7 +789,7 @@ def main():
     # steady state on the first held-out cavities, both arms timed here
     tts = None
     if rank == 0 and world == 1 and args.steady_cases > 0:
-        tts = time_to_steady(pkg, args.steady_cases, args.steady_max_steps, local)
+        tts = time_to_steady(pkg, args.steady_cases, args.steady_max_steps, local, args.steady_extrapolate)
 
     if rank == 0:
         line = {

@@ -309,8 +309,93 @@ def _run(b, eps, max_steps, check_every, mask=None, switch_eps=None):
     return status, steps, fallback, (low if switch_eps is not None else None)
 
 
+# ---------------------------------------------------------------------------
+# extrapolation of the slowest mode (no reference counterpart)
+# ---------------------------------------------------------------------------
+# Near the steady state a run converges geometrically, s_k = s* + c r^k v,
+# and in slowly converging cavities one real mode dominates (successive
+# changes d1 = s1 - s0, d2 = s2 - s1 a fixed number of iterations apart are
+# nearly parallel).  Lyusternik's (Aitken's) extrapolation then removes that
+# mode: s* = s2 + r / (1 - r) d2 with r = <d2, d1> / <d1, d1>.  The solver
+# still judges the result by the reference's criterion afterwards.
+EXTRAP_MAX_FACTOR = 50.0
+
+
+def lyusternik_factor(s0, s1, s2, fmax=EXTRAP_MAX_FACTOR):
+    """(factor, r) of the extrapolation s2 + factor * (s2 - s1) from three
+    states an equal number of iterations apart; factor 0 unless 0 < r < 1,
+    and at most fmax."""
+    d1 = np.asarray(s1, np.float64) - np.asarray(s0, np.float64)
+    d2 = np.asarray(s2, np.float64) - np.asarray(s1, np.float64)
+    den = float(d1.ravel() @ d1.ravel())
+    if not den > 0.0:
+        return 0.0, 0.0
+    r = float(d2.ravel() @ d1.ravel()) / den
+    if not 0.0 < r < 1.0:
+        return 0.0, r
+    return min(r / (1.0 - r), float(fmax)), r
+
+
+def _state(m):
+    """A member's populations and macroscopic fields (host copies)."""
+    f, g = m.populations()
+    mac = {k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "w", "T")}
+    return f, g, mac
+
+
+def _load_extrapolated(m, a, b, fac):
+    """Load b + fac * (b - a) (populations and fields) into member m: an exact
+    restart of b when fac is 0 (set_populations + set_macro)."""
+    f = b[0] + fac * (b[0] - a[0])
+    g = b[1] + fac * (b[1] - a[1])
+    mac = {k: b[2][k] + fac * (b[2][k] - a[2][k]) for k in b[2]}
+    m.set_populations(f, g)
+    m.set_macro(mac["rho"], mac["u"], mac["v"], mac.get("w"), mac["T"])
+
+
+def _run_extrapolated(b, eps, max_steps, check_every, tau, delta):
+    """_run with one extrapolation of the slowest mode per member: every
+    member runs to the residual tau, then `delta` and again `delta` more
+    iterations (three states); each member that has the budget is loaded with
+    its extrapolated state and all of them run on to eps.  Every member that
+    continues is loaded (unchanged ones with their own state, an exact
+    restart), so they stay in step.  Returns _run's tuple and the factors."""
+    limit = np.broadcast_to(np.asarray(max_steps, dtype=np.int64), (b.n,)).copy()
+    status, steps, fallback, _ = _run(b, tau, limit, check_every)
+    cont = (status == 1) & (steps < limit)
+    go = cont & (limit - steps > 2 * delta)
+    facs = np.zeros(b.n)
+    if go.any():
+        idx = np.nonzero(go)[0]
+        snaps = [[_state(b.members[i]) for i in idx]]
+        ok = np.ones(len(idx), bool)
+        for _ in range(2):
+            st, n = b.run_masked(go, int(delta), check_every, 0.0)  # eps 0: exactly delta iterations
+            steps = np.where(go, steps + n, steps)
+            snaps.append([_state(b.members[i]) for i in idx])
+            ok &= st[idx] == 0  # stopped by the iteration count, not by a bad residual
+        for j, i in enumerate(idx):
+            s0, s1, s2 = (snaps[k][j] for k in range(3))
+            fac = 0.0
+            if ok[j]:
+                fac, _ = lyusternik_factor(np.concatenate([s0[0].ravel(), s0[1].ravel()]),
+                                           np.concatenate([s1[0].ravel(), s1[1].ravel()]),
+                                           np.concatenate([s2[0].ravel(), s2[1].ravel()]))
+            facs[i] = fac
+            _load_extrapolated(b.members[i], s1, s2, fac)
+    status = np.where(cont, 0, status)
+    for part in (go, cont & ~go):  # the loaded members together, then any others
+        if part.any():
+            st, n, fb, _ = _run(b, eps, np.where(part, limit - steps, 0), check_every, mask=part)
+            status = np.where(part, st, status)
+            steps = np.where(part, steps + n, steps)
+            fallback = fallback | (part & fb)
+    return status, steps, fallback, None, facs
+
+
 def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_every=2000, max_steps=1_000_000,
-          growth=100, want_fields=False, device=0, predictions=None, field_fn=None, switch_eps=1e-5):
+          growth=100, want_fields=False, device=0, predictions=None, field_fn=None, switch_eps=1e-5,
+          extrapolate=None):
     """Run every case to the reference's stop criterion (errorU, errorT <= eps
     at a check every `check_every` iterations) in one batch, with the stop
     test on the device.
@@ -326,6 +411,9 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
     (lbm_batch_tune) times FP32 and FP64 stepping on the batch and the run is
     "mixed" if FP32 is more than FP32_HANDOVER_COST times faster, else FP64.
     max_steps bounds each member's iterations over all phases.
+    extrapolate (tau, delta): one extrapolation of each member's slowest mode
+    (_run_extrapolated) at residual tau from states delta iterations apart;
+    ignored when the run is mixed.
     Returns a dict of per-case arrays and the wall time: `seconds` from the
     first initialisation to the result (prediction and lbm_init_warm included),
     of which `predict_seconds` was the network."""
@@ -352,15 +440,22 @@ def solve(cases, init="cold", model=None, storage="f64", eps=F32_EPS, check_ever
         tune_steps = b.members[0].itc - it0
         tuned = {"f64": t64, "f32": t32, "chosen": "mixed" if mixed else "f64"}
     b.synchronize()
-    status, steps, fallback, steps_low = _run(b, eps, max_steps - tune_steps, check_every,
-                                               switch_eps=switch_eps if mixed else None)
+    facs = None
+    if extrapolate is not None and not mixed:
+        tau, delta = extrapolate
+        status, steps, fallback, steps_low, facs = _run_extrapolated(b, eps, max_steps - tune_steps, check_every,
+                                                                     float(tau), int(delta))
+    else:
+        status, steps, fallback, steps_low = _run(b, eps, max_steps - tune_steps, check_every,
+                                                   switch_eps=switch_eps if mixed else None)
     steps = steps + tune_steps
     b.synchronize()
     seconds = time.perf_counter() - t0
     nu_hot, nu_cold = b.nusselt()
     out = {"status": status, "steps": steps, "fallback": fallback, "nu_hot": nu_hot, "nu_cold": nu_cold,
            "seconds": seconds, "predict_seconds": t_pred, "nodes": np.array([m.nnode for m in b.members]),
-           "storage": storage, "init": init, "steps_low_precision": steps_low, "tuned": tuned}
+           "storage": storage, "init": init, "steps_low_precision": steps_low, "tuned": tuned,
+           "extrapolation_factors": facs}
     if want_fields:
         out["fields"] = [{k: v for k, v in m.macro().items() if k in ("rho", "u", "v", "T")} for m in b.members]
     if field_fn is not None:

@@ -67,6 +67,20 @@ def test_mixed_precision_reaches_fp64_nusselt(pkg, model):
     assert err.max() <= 1e-4, err
 
 
+def test_extrapolated_warm_start_reaches_the_fp64_fixed_point(pkg, model):
+    # one extrapolation of each member's slowest mode at residual 3e-5 from
+    # states 10,000 iterations apart; the solver's criterion judges the result
+    W = pkg.warmstart
+    cases = _cases(pkg, 2)
+    ref = W.solve(cases, init="cold", storage="f64", eps=EPS, max_steps=1500000)
+    ex = W.solve(cases, init="warm", model=model, storage="f64", eps=EPS, max_steps=1500000,
+                 extrapolate=(3e-5, 10000))
+    assert (ex["status"] == 1).all() and not ex["fallback"].any()
+    assert ex["extrapolation_factors"] is not None and (ex["extrapolation_factors"] >= 0).all()
+    err = np.abs(ex["nu_hot"] - ref["nu_hot"]) / ref["nu_hot"]
+    assert err.max() <= 1e-4, err
+
+
 def test_diverging_warm_start_falls_back_to_cold(pkg):
     # a prediction far outside the low-Mach regime blows up; the member is
     # stopped (residual not finite or growing) and restarted from the

@@ -178,3 +178,114 @@ def test_auto_storage_weighs_the_fp32_handover(pkg, fake, rates, mixed):
         assert ("storage", "f64") in b.log and ("option", "tile", 64) in b.log
     # the tuner's steps count toward each member's iterations and budget
     assert r["steps"].tolist() == [5072, 7072]
+
+
+# ---------------------------------------------------------------------------
+# extrapolation of the slowest mode (warmstart.lyusternik_factor,
+# warmstart._run_extrapolated)
+# ---------------------------------------------------------------------------
+def test_lyusternik_factor_recovers_a_geometric_limit(pkg):
+    W = pkg.warmstart
+    rng = np.random.default_rng(3)
+    s_star, v = rng.normal(size=50), rng.normal(size=50)
+    for r in (0.3, 0.9, 0.97):
+        s = [s_star + 0.2 * r ** k * v for k in range(3)]
+        fac, rr = W.lyusternik_factor(*s)
+        assert rr == pytest.approx(r, rel=1e-12)
+        assert np.allclose(s[2] + fac * (s[2] - s[1]), s_star, rtol=0, atol=1e-12)
+    # an oscillating or growing sequence, or no change at all: no extrapolation
+    for r in (-0.5, 1.2):
+        s = [s_star + 0.2 * r ** k * v for k in range(3)]
+        assert W.lyusternik_factor(*s)[0] == 0.0
+    assert W.lyusternik_factor(s_star, s_star, s_star) == (0.0, 0.0)
+    # the factor is capped
+    s = [s_star + 0.2 * 0.999 ** k * v for k in range(3)]
+    assert W.lyusternik_factor(*s, fmax=50.0)[0] == 50.0
+
+
+class _GeoMember:
+    """A member whose state relaxes geometrically to a fixed point: every
+    iteration multiplies its deviation by rho_it.  Loading a state (as
+    set_populations does) flips its buffer parity, like a first collision."""
+
+    def __init__(self, rho_it, seed):
+        rng = np.random.default_rng(seed)
+        self.rho_it = rho_it
+        self.star = {"f": rng.normal(size=(4, 3, 9)), "g": rng.normal(size=(4, 3, 5)),
+                     "u": rng.normal(size=(4, 3)) + 2.0, "rho": np.ones((4, 3)), "v": rng.normal(size=(4, 3)),
+                     "T": rng.normal(size=(4, 3))}
+        self.v = {k: 1e-2 * rng.normal(size=a.shape) for k, a in self.star.items()}
+        self.t = 0.0            # "time" of the state: deviation = v * rho_it ** t
+        self.parity = 0
+        self.u_prev = np.zeros((4, 3))
+        self.loads = 0
+
+    def _get(self, k):
+        return self.star[k] + self.v[k] * self.rho_it ** self.t
+
+    def populations(self):
+        return self._get("f"), self._get("g")
+
+    def macro(self):
+        return {k: self._get(k) for k in ("rho", "u", "v", "T")}
+
+    def set_populations(self, f, g):
+        # the loaded deviation along v fixes the new time of the state
+        dev = (f - self.star["f"]).ravel() @ self.v["f"].ravel() / (self.v["f"].ravel() @ self.v["f"].ravel())
+        self.loaded_dev = dev
+        self.t = np.inf if dev <= 1e-300 else np.log(dev) / np.log(self.rho_it)
+        self.parity ^= 1
+        self.loads += 1
+
+    def set_macro(self, rho, u, v, w, T):
+        assert w is None
+
+    def initial(self):
+        raise AssertionError("no member diverges here")
+
+
+class _GeoBatch:
+    def __init__(self, members):
+        self.members = members
+        self.n = len(members)
+
+    def run_masked(self, mask, max_steps, check_every, eps):
+        on = np.ones(self.n, bool) if mask is None else np.asarray(mask, bool)
+        par = {self.members[i].parity for i in np.nonzero(on)[0]}
+        assert len(par) <= 1, "members on the mask out of step"
+        status = np.zeros(self.n, np.int32)
+        done = np.zeros(self.n, np.int64)
+        for i in np.nonzero(on)[0]:
+            m = self.members[i]
+            while done[i] < max_steps:
+                k = min(check_every, max_steps - done[i])
+                m.t += k
+                done[i] += k
+                if k == check_every:  # a check: the reference's relative change of u
+                    u = m._get("u")
+                    res = np.linalg.norm(u - m.u_prev) / np.linalg.norm(u)
+                    m.u_prev = u
+                    if res <= eps:
+                        status[i] = 1
+                        break
+        return status, done
+
+
+def test_extrapolated_run_jumps_to_the_fixed_point(pkg):
+    W = pkg.warmstart
+    # per-iteration contraction: slow (1e-4 per 2000-iteration check ~ 0.82)
+    # and slower; the last member has no budget left for the snapshots
+    members = [_GeoMember(1 - 1e-4, 0), _GeoMember(1 - 2e-5, 1), _GeoMember(1 - 5e-4, 2)]
+    limit = np.array([3_000_000, 3_000_000, 30_000])
+    plain = _GeoBatch([_GeoMember(m.rho_it, s) for m, s in zip(members, range(3))])
+    st0, n0, fb0, _ = W._run(plain, W.F32_EPS, limit, 2000)
+    b = _GeoBatch(members)
+    status, steps, fallback, low, facs = W._run_extrapolated(b, W.F32_EPS, limit, 2000, 3e-5, 10_000)
+    assert (status == 1).all() and not fallback.any() and low is None
+    assert facs[0] > 0 and facs[1] > 0 and facs[2] == 0.0
+    # a one-mode deviation is removed by the jump (to rounding; it started at 1)
+    assert abs(members[0].loaded_dev) < 1e-9 and abs(members[1].loaded_dev) < 1e-9
+    # every member that went on after the jump was loaded
+    assert [m.loads for m in members] == [1, 1, 0]
+    assert steps[1] < 0.5 * n0[1]
+    assert (steps <= limit).all()

@@ -443,7 +443,9 @@ def steady_cold_arm(pkg, cases, max_steps, device):
 
 
 def _tau_delta(text):
-    """'TAU,DELTA' -> (float, int)."""
+    """'TAU,DELTA' -> (float, int); 'off' -> None."""
+    if text.strip().lower() == "off":
+        return None
     tau, delta = text.split(",")
     return float(tau), int(delta)
 
@@ -473,7 +475,9 @@ def time_to_steady(pkg, ncases, max_steps, device, extrapolate=None):
             "extrapolate": None if extrapolate is None else {"tau": extrapolate[0], "delta": extrapolate[1]},
             "arms": "FP64 from the conduction state, one cavity per launch vs. one persistent batch + learned "
                     "warm start + storage chosen by the autotuner (mixed precision member by member if FP32 "
-                    "stepping pays for its hand-over, else FP64); prediction, tuning and initialisation timed"}
+                    "stepping pays for its hand-over, else FP64) + one extrapolation of each member's slowest "
+                    "mode (see `extrapolate`, null when off); prediction, tuning, initialisation and the "
+                    "extrapolation's host round trips timed"}
 
 
 def run_unet(args, world, rank, local):
@@ -643,9 +647,10 @@ def main():
                     help="cavity workloads: held-out cavities of the time_to_steady object (0: leave it out)")
     ap.add_argument("--steady-storage", default="auto", choices=["auto", "mixed", "f64", "f32"],
                     help="steady workload: storage policy of the warm-started batch")
-    ap.add_argument("--steady-extrapolate", type=_tau_delta, default=None, metavar="TAU,DELTA",
+    ap.add_argument("--steady-extrapolate", type=_tau_delta, default=(3e-5, 10000), metavar="TAU,DELTA|off",
                     help="steady workload and time_to_steady: one extrapolation of each member's slowest mode at "
-                         "residual TAU from states DELTA iterations apart (e.g. 3e-5,10000); off by default")
+                         "residual TAU from states DELTA iterations apart (default 3e-5,10000; 'off' to run "
+                         "without it)")
     ap.add_argument("--steady-max-steps", type=int, default=3_000_000,
                     help="time_to_steady: iteration cap per cavity, high enough for every case of both arms")
     ap.add_argument("--max-steps", type=int, default=1_500_000, help="steady: iteration cap per cavity")

@@ -362,7 +362,9 @@ def _run_extrapolated(b, eps, max_steps, check_every, tau, delta):
     restart), so they stay in step.  Returns _run's tuple and the factors."""
     limit = np.broadcast_to(np.asarray(max_steps, dtype=np.int64), (b.n,)).copy()
     status, steps, fallback, _ = _run(b, tau, limit, check_every)
-    cont = (status == 1) & (steps < limit)
+    reached = status == 1
+    status = np.where(reached, 0, status)  # tau is not the criterion: a member out of budget here is capped
+    cont = reached & (steps < limit)
     go = cont & (limit - steps > 2 * delta)
     facs = np.zeros(b.n)
     if go.any():
@@ -383,7 +385,6 @@ def _run_extrapolated(b, eps, max_steps, check_every, tau, delta):
                                            np.concatenate([s2[0].ravel(), s2[1].ravel()]))
             facs[i] = fac
             _load_extrapolated(b.members[i], s1, s2, fac)
-    status = np.where(cont, 0, status)
     for part in (go, cont & ~go):  # the loaded members together, then any others
         if part.any():
             st, n, fb, _ = _run(b, eps, np.where(part, limit - steps, 0), check_every, mask=part)

@@ -289,3 +289,15 @@ def test_extrapolated_run_jumps_to_the_fixed_point(pkg):
     assert [m.loads for m in members] == [1, 1, 0]
     assert steps[1] < 0.5 * n0[1]
     assert (steps <= limit).all()
+
+
+def test_extrapolated_run_reports_tau_as_not_converged(pkg):
+    W = pkg.warmstart
+    # the step count at which this member reaches tau, from a copy of it
+    probe = _GeoBatch([_GeoMember(1 - 5e-4, 7)])
+    st, n, _, _ = W._run(probe, 3e-5, 1_000_000, 2000)
+    assert st[0] == 1
+    # a budget that ends exactly there: the member met tau, not the criterion
+    b = _GeoBatch([_GeoMember(1 - 5e-4, 7)])
+    status, steps, fallback, _, facs = W._run_extrapolated(b, W.F32_EPS, n, 2000, 3e-5, 10_000)
+    assert status[0] == 0 and steps[0] == n[0] and facs[0] == 0.0 and b.members[0].loads == 0

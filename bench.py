@@ -472,7 +472,10 @@ def time_to_steady(pkg, ncases, max_steps, device, extrapolate=None):
             "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()), "max_nu_rel_err": float(err.max()),
             "fallbacks": int(np.sum(r["fallback"])), "storage_chosen": r["tuned"]["chosen"],
             "tuned_mlups": {k: r["tuned"][k]["mlups"] for k in ("f64", "f32")},
-            "extrapolate": None if extrapolate is None else {"tau": extrapolate[0], "delta": extrapolate[1]},
+            # what the run applied: null when off, or when the autotuner chose the mixed run (no extrapolation)
+            "extrapolate": None if r.get("extrapolation_factors") is None else
+            {"tau": extrapolate[0], "delta": extrapolate[1],
+             "members_extrapolated": int(np.sum(np.asarray(r["extrapolation_factors"]) > 0))},
             "arms": "FP64 from the conduction state, one cavity per launch vs. one persistent batch + learned "
                     "warm start + storage chosen by the autotuner (mixed precision member by member if FP32 "
                     "stepping pays for its hand-over, else FP64) + one extrapolation of each member's slowest "
@@ -614,7 +617,8 @@ def run_steady(args, world, rank, local):
                                "storage_chosen": (r["tuned"] or {}).get("chosen", args.steady_storage),
                                "nu_within_1e-4_of_fp64": int((conv & (err <= 1e-4)).sum()),
                                "max_nu_rel_err": float(err.max()), "fallbacks": int(np.sum(r["fallback"])),
-                               "extrapolate": args.steady_extrapolate},
+                               "extrapolate": (args.steady_extrapolate
+                                               if r.get("extrapolation_factors") is not None else None)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "bytes_per_lup": bpl,
                          "kernel": "k_march2d_batch, the warm arm's algorithmic bytes (240 B per FP64 update, "

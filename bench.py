@@ -160,6 +160,38 @@ def cpu_sample(wl, seconds: float = 12.0, max_steps: int = 200):
                       f"{oracle.get_threads()} OpenMP threads), {dt:.1f} s"}
 
 
+def cpu_sample_batch(seconds: float = 12.0, max_rounds: int = 200, warmup: int = 1):
+    """Time the oracle (C restatement of the reference, OpenMP) on the first 8
+    cavities of the seed-0 batch sweep, one iteration of each per round."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    oracle.set_threads(os.cpu_count() or 1)
+    specs = pkg.sweep_specs(256, seed=0)[:8]
+    orc = []
+    for sp in specs:
+        m = sp["coords"]
+        orc.append(oracle.Oracle(2, sp["nx"], sp["ny"], 1, x=m.x, y=m.y, dt=m.dt, length_LB=m.length_LB,
+                                 Ra=sp["Ra"], Pr=sp["Pr"]))
+    for _ in range(warmup):
+        for o in orc:
+            o.step(1)
+    rounds, t0 = 0, time.perf_counter()
+    while rounds < max_rounds:
+        for o in orc:
+            o.step(1)
+        rounds += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    dt = time.perf_counter() - t0
+    nodes = sum(sp["nx"] * sp["ny"] for sp in specs)
+    return {"value": nodes * rounds / dt / 1e6, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
+            "sample": f"{rounds} iterations of the first 8 sweep cavities ({nodes} nodes; FP64, C restatement, "
+                      f"{oracle.get_threads()} OpenMP threads), {dt:.1f} s", "rounds": rounds, "seconds": dt,
+            "nodes": nodes}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -176,34 +208,14 @@ def dist_setup():
 def run_reference_batch(args):
     """batch256 on the CPU: the C restatement advances the first cavities of
     the same seeded sweep, one iteration of each per step (a bounded sample)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from __graft_entry__ import load_package
-    pkg = load_package()
-    oracle.set_threads(os.cpu_count() or 1)
-    specs = pkg.sweep_specs(256, seed=0)[:8]
-    orc = []
-    for sp in specs:
-        m = sp["coords"]
-        o = oracle.Oracle(2, sp["nx"], sp["ny"], 1, x=m.x, y=m.y, dt=m.dt, length_LB=m.length_LB, Ra=sp["Ra"],
-                          Pr=sp["Pr"])
-        orc.append(o)
-    for _ in range(args.warmup):
-        for o in orc:
-            o.step(1)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for o in orc:
-            o.step(1)
-    dt = time.perf_counter() - t0
-    nodes = sum(sp["nx"] * sp["ny"] for sp in specs)
-    v = nodes * args.steps / dt / 1e6
+    c = cpu_sample_batch(seconds=float("inf"), max_rounds=args.steps, warmup=args.warmup)
+    nodes, dt, v = c["nodes"], c["seconds"], c["value"]
     line = {"impl": "reference", "metric": "MLUPS", "value": v, "unit": "MLUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "batch256", "sample": "first 8 cavities of the seed-0 sweep, one iteration each "
                                                          "per step", "nodes": nodes},
-            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": oracle.get_threads(), "kind": "port",
+            "cpu_baseline": {"value": v, "unit": "MLUPS", "cores": c["cores"], "kind": "port",
                              "sample": f"{args.steps} iterations of 8 sweep cavities ({nodes} nodes)"},
             "e2e": {"value": v, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -393,6 +405,8 @@ def run_batch(args, world, rank, local):
         # the one collective of the data path: every cavity's result to every rank
         got = pkg.sharding.gather_by_index(idx, {"nu_hot": nu_hot}, n_total)
         e2e["nusselt_gathered"] = int(np.isfinite(got["nu_hot"]).sum())
+    # the C restatement on this host's cores, after the GPU timing: the first 8 sweep cavities
+    cpu = cpu_sample_batch() if rank == 0 and world == 1 and not args.no_cpu else None
     if rank == 0:
         line = {
             "metric": "MLUPS", "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
@@ -408,7 +422,7 @@ def run_batch(args, world, rank, local):
                        "speedup_vs_one_launch_per_cavity": value / baseline if baseline else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind, "bytes_per_lup": bpl, "kernel": "k_march2d_batch"},
-            "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     b.close()
